@@ -1,0 +1,12 @@
+"""blockvecchia_b200 -- B200-native block-Vecchia Gaussian-process likelihood.
+
+The hot path (conditioning-set selection, Matern generation, batched
+Cholesky / solves / log-determinant) runs in libbv_b200.so, hand-written CUDA
+for sm_100a behind the C ABI of include/bv.h.
+"""
+from ._lib import BvError, lib  # noqa: F401
+from .vecchia import (Layout, LlhData, build_layout, generate_xy, kmeans, knn,  # noqa: F401
+                      layout_from_clusters, llh_Xvecchia_batch)
+
+__all__ = ["BvError", "Layout", "LlhData", "build_layout", "generate_xy", "kmeans", "knn",
+           "layout_from_clusters", "llh_Xvecchia_batch", "lib"]

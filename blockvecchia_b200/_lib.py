@@ -1,0 +1,110 @@
+"""ctypes binding of libbv_b200.so (include/bv.h).
+
+The library is built in-tree by blockvecchia_b200.build; importing this module
+never falls back to anything else: a missing or unloadable library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbv_b200.so")
+
+BV_OK = 0
+BV_E_INVALID = -1
+BV_E_CUDA = -2
+BV_E_NOMEM = -3
+BV_E_NODEVICE = -4
+BV_E_TOOLARGE = -5
+BV_E_TIMEOUT = -6
+BV_PREC_FP64 = 0
+BV_PREC_MIXED = 1
+BV_FAIL_NEGINF = 0
+BV_FAIL_CONTINUE = 1
+BV_ST_COND_FAIL = 1
+BV_ST_SCHUR_FAIL = 2
+BV_ST_FP32_FALLBACK = 4
+BV_ST_NONFINITE = 8
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+
+# Every function include/bv.h declares, with its ctypes signature.
+EXPORTS = {
+    "bv_default_opts": (None, [C.c_void_p]),
+    "bv_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "bv_destroy": (None, [C.c_void_p]),
+    "bv_llh": (C.c_double, [C.c_uint, _D, _D, C.c_void_p]),
+    "bv_llh_eval": (C.c_int, [C.c_void_p, _D, _D]),
+    "bv_block_llk": (C.c_int, [C.c_void_p, _D, C.c_int]),
+    "bv_get_status": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bv_iterations": (C.c_int, [C.c_void_p]),
+    "bv_last_error": (C.c_char_p, []),
+    "bv_llh_host": (C.c_int, [C.c_void_p, _D, _D, _D, _I, _D, _D]),
+    "bv_knn": (C.c_int, [_D, _D, C.c_int, C.c_int, C.c_int, _I, _D, _D, _I, C.c_int]),
+    "bv_layout_build": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                  _I, _I, _D, _D, _D, _D, _D, _I, _I]),
+    "bv_layout_from_clusters": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, _I, _D, _D, C.c_int,
+                                          _I, _I, _D, _D, _D, _D, _D, _I, _I]),
+    "bv_kmeans": (C.c_int, [_D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _I, _D, _D]),
+    "bv_generate_xy": (C.c_int, [C.c_int, C.c_int, _D, _D]),
+}
+
+
+class BvLayout(C.Structure):
+    _fields_ = [("n", C.c_int), ("bc", C.c_int), ("cs", C.c_int),
+                ("batchNum", _I), ("batchNumAccum", _I),
+                ("x", _D), ("y", _D), ("obs", _D), ("knn_idx", _I),
+                ("cx", _D), ("cy", _D)]
+
+
+class BvOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("kernel", C.c_int), ("dist_scale", C.c_double),
+                ("device", C.c_int), ("on_failure", C.c_int), ("print_iter", C.c_int),
+                ("use_graph", C.c_int), ("schedule", C.c_int), ("mixed_tol", C.c_double)]
+
+
+class BvStatus(C.Structure):
+    _fields_ = [("blocks", C.c_int), ("cond_fail", C.c_int), ("schur_fail", C.c_int),
+                ("fp32_fallback", C.c_int), ("nonfinite", C.c_int), ("flags_or", C.c_uint),
+                ("llk", C.c_double), ("device_ms", C.c_double)]
+
+
+class BvError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libbv_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libbv_b200.so (building it first if it is absent and nvcc exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build as _build
+            _build.build()
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in EXPORTS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != BV_OK:
+        msg = lib().bv_last_error()
+        raise BvError(rc, msg.decode() if msg else "")
+
+
+def dp(a):
+    return a.ctypes.data_as(_D)
+
+
+def ip(a):
+    return a.ctypes.data_as(_I)

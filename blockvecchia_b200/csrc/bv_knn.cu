@@ -1,0 +1,434 @@
+// bv_knn.cu -- conditioning-set selection on the device, one warp per block.
+//
+// Follows findNearestPoints (include/nearest_neighbor.h:76-148) as the
+// reference's driver calls it for blocks 1..bc-1 with l0 = 0 and
+// l1 = batchNumAccum[i] (src/test_Xvecchia_batch.cpp:368-390):
+//   key(p) = sqrt(fma(dx, dx, dy*dy)), dx = x[p] - cx, dy = y[p] - cy
+//   (calEucDistance :30-35 as the reference's -O3 -march=native build
+//   contracts it), then k = cs rounds of a selection sort with swaps and a
+//   strict '<' (:115-133), output in selection order.
+//
+// The warp streams the candidates once, keeping those whose squared distance
+// is within a few ulps of the running k-th smallest (a threshold that only
+// falls) in a shared-memory buffer, and shrinks the buffer by an exact radix
+// select whenever it fills.  The final set S = {p : key(p) <= key_k} (all
+// ties of the k-th key included) is then put through an exact replay of the
+// reference's selection sort: at step t the winner is the unselected member
+// of S with the smallest (key, current position), it moves to position t and
+// whatever S member occupied position t moves to the winner's old position.
+// Members outside S never win and never change the relative positions of S
+// members, so the replay reproduces the reference's output, ties included.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/bv.h"
+#include "bv_common.cuh"
+#include "bv_knn.cuh"
+
+namespace bv {
+
+constexpr int kKnnWarps = 4;
+constexpr int kKnnCap = 1024;  // candidate buffer per warp
+constexpr int kKnnMaxCs = kKnnCap / 2;
+
+struct KnnWarpSmem {
+    unsigned long long key[kKnnCap];  // squared distance bits, later distance bits
+    int idx[kKnnCap];
+    int pos[kKnnCap];
+    unsigned hist[256];
+};
+
+struct KnnArgs {
+    const double *x, *y;
+    const int *acc;
+    const double *cx, *cy;  // device copies
+    int bc, cs;
+    int *out;
+    unsigned *counter;
+    int *error;  // first failing block + 1, or 0
+};
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Exact k-th smallest (1-based) of the first n keys, MSB-first radix select
+// with 8-bit digits.
+__device__ unsigned long long warp_kth(KnnWarpSmem &w, int n, int k)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned long long prefix = 0ull, mask = 0ull;
+    int kk = k;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+#pragma unroll
+        for (int b = 0; b < 8; ++b) w.hist[lane * 8 + b] = 0u;
+        __syncwarp();
+        for (int j = lane; j < n; j += 32) {
+            const unsigned long long key = w.key[j];
+            if ((key & mask) == prefix) atomicAdd(&w.hist[(key >> shift) & 255ull], 1u);
+        }
+        __syncwarp();
+        unsigned loc[8];
+        unsigned tot = 0;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            loc[b] = w.hist[lane * 8 + b];
+            tot += loc[b];
+        }
+        unsigned incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const unsigned excl = incl - tot;
+        // The lane whose bin range holds the kk-th element.
+        const bool mine = (excl < (unsigned)kk) && ((unsigned)kk <= incl);
+        const unsigned who = __ballot_sync(0xffffffffu, mine);
+        const int src = who ? __ffs(who) - 1 : 31;  // who != 0 whenever n >= k
+        int bin = 0, before = 0;
+        if (lane == src) {
+            unsigned run = excl;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                if (run + loc[b] >= (unsigned)kk) {
+                    bin = lane * 8 + b;
+                    before = (int)run;
+                    break;
+                }
+                run += loc[b];
+            }
+        }
+        bin = __shfl_sync(0xffffffffu, bin, src);
+        before = __shfl_sync(0xffffffffu, before, src);
+        prefix |= (unsigned long long)bin << shift;
+        mask |= 255ull << shift;
+        kk -= before;
+        __syncwarp();
+    }
+    return prefix;
+}
+
+// Keep entries with key <= lim, in order; returns the new count.
+__device__ int warp_compact(KnnWarpSmem &w, int n, unsigned long long lim)
+{
+    const int lane = threadIdx.x & 31;
+    int count = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int j = base + lane;
+        unsigned long long key = 0ull;
+        int id = 0;
+        bool keep = false;
+        if (j < n) {
+            key = w.key[j];
+            id = w.idx[j];
+            keep = key <= lim;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        __syncwarp();
+        if (keep) {
+            const int p = count + __popc(bal & lanemask_lt());
+            w.key[p] = key;
+            w.idx[p] = id;
+        }
+        count += __popc(bal);
+        __syncwarp();
+    }
+    return count;
+}
+
+// Upper end of the squared-distance window whose square roots can equal
+// sqrt(s): sqrt halves relative spacing, so 2^-49 relative is ample.
+__device__ __forceinline__ unsigned long long window_hi(unsigned long long skey)
+{
+    const double s = __longlong_as_double((long long)skey);
+    const double hi = s * (1.0 + 0x1p-49) + 0x1p-1070;
+    return (unsigned long long)__double_as_longlong(hi);
+}
+
+__global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
+{
+    extern __shared__ __align__(16) unsigned char knn_smem[];
+    KnnWarpSmem &w = reinterpret_cast<KnnWarpSmem *>(knn_smem)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int k = a.cs;
+
+    for (;;) {
+        unsigned task = 0;
+        if (lane == 0) task = atomicAdd(a.counter, 1u);
+        task = __shfl_sync(0xffffffffu, task, 0);
+        // Largest prefixes first; block 0 is handled by the host (points 0..cs-1).
+        const int i = a.bc - 1 - (int)task;
+        if (i < 1) break;
+        const int P = a.acc[i];
+        const double cx = a.cx[i], cy = a.cy[i];
+        int *out = a.out + (size_t)i * k;
+        if (P < k) {
+            if (lane == 0) atomicCAS(a.error, 0, i + 1);
+            continue;
+        }
+
+        // 1. Stream candidates 0..P-1 through the falling threshold.
+        unsigned long long lim = ~0ull;
+        int count = 0;
+        bool overflow = false;
+        for (int base = 0; base < P; base += 128) {
+            unsigned long long key[4];
+            bool keep[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int p = base + 32 * u + lane;
+                keep[u] = false;
+                key[u] = 0ull;
+                if (p < P) {
+                    const double dx = __ldg(a.x + p) - cx;
+                    const double dy = __ldg(a.y + p) - cy;
+                    const double s = __fma_rn(dx, dx, __dmul_rn(dy, dy));
+                    key[u] = (unsigned long long)__double_as_longlong(s);
+                    keep[u] = key[u] <= lim;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const unsigned bal = __ballot_sync(0xffffffffu, keep[u]);
+                if (keep[u]) {
+                    const int p = count + __popc(bal & lanemask_lt());
+                    w.key[p] = key[u];
+                    w.idx[p] = base + 32 * u + lane;
+                }
+                count += __popc(bal);
+            }
+            if (count > kKnnCap - 128) {
+                __syncwarp();
+                const unsigned long long kth = warp_kth(w, count, k);
+                lim = window_hi(kth);
+                count = warp_compact(w, count, lim);
+                if (count > kKnnCap - 128) {
+                    overflow = true;
+                    break;
+                }
+            }
+        }
+        if (overflow) {
+            if (lane == 0) atomicCAS(a.error, 0, i + 1);
+            continue;
+        }
+        __syncwarp();
+
+        // 2. Exact k-th key; S = members whose distance equals or beats it.
+        const unsigned long long kth = warp_kth(w, count, k);
+        count = warp_compact(w, count, window_hi(kth));
+        const double dk = __dsqrt_rn(__longlong_as_double((long long)kth));
+        {
+            int m = 0;
+            for (int base = 0; base < count; base += 32) {
+                const int j = base + lane;
+                double d = 0.0;
+                int id = 0;
+                bool keep = false;
+                if (j < count) {
+                    d = __dsqrt_rn(__longlong_as_double((long long)w.key[j]));
+                    id = w.idx[j];
+                    keep = d <= dk;
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                __syncwarp();
+                if (keep) {
+                    const int p = m + __popc(bal & lanemask_lt());
+                    w.key[p] = (unsigned long long)__double_as_longlong(d);
+                    w.idx[p] = id;
+                    w.pos[p] = id;  // initial position = index
+                }
+                m += __popc(bal);
+                __syncwarp();
+            }
+            count = m;
+        }
+
+        // 3. Replay the selection sort on S.
+        for (int t = 0; t < k; ++t) {
+            unsigned long long bkey = ~0ull;
+            int bpos = 0x7fffffff, bslot = -1, occ = -1;
+            for (int j = lane; j < count; j += 32) {
+                const int pj = w.pos[j];
+                if (pj < 0) continue;  // already selected
+                const unsigned long long kj = w.key[j];
+                if (kj < bkey || (kj == bkey && pj < bpos)) {
+                    bkey = kj;
+                    bpos = pj;
+                    bslot = j;
+                }
+                if (pj == t) occ = j;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long ok = __shfl_xor_sync(0xffffffffu, bkey, o);
+                const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
+                const int os = __shfl_xor_sync(0xffffffffu, bslot, o);
+                if (ok < bkey || (ok == bkey && op < bpos)) {
+                    bkey = ok;
+                    bpos = op;
+                    bslot = os;
+                }
+            }
+            const unsigned ob = __ballot_sync(0xffffffffu, occ >= 0);
+            const int occ_slot = ob ? __shfl_sync(0xffffffffu, occ, __ffs(ob) - 1) : -1;
+            if (bslot < 0) break;  // |S| >= k makes this unreachable
+            if (lane == 0) {
+                out[t] = w.idx[bslot];
+                if (occ_slot >= 0 && occ_slot != bslot) w.pos[occ_slot] = bpos;
+                w.pos[bslot] = -1;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, const int *d_acc,
+               const double *cx, const double *cy, int *d_knn, cudaStream_t s)
+{
+    if (cs <= 0) return BV_OK;
+    if (cs > kKnnMaxCs) {
+        set_error("bv_knn: cs=%d exceeds the supported maximum %d", cs, kKnnMaxCs);
+        return BV_E_TOOLARGE;
+    }
+    std::vector<int> first(cs);
+    for (int t = 0; t < cs; ++t) first[t] = t;
+    double *d_c = nullptr;
+    unsigned *d_counter = nullptr;
+    int *d_err = nullptr;
+    int rc = BV_OK;
+    auto fail = [&](cudaError_t e, const char *what) {
+        set_error("bv_knn: %s: %s", what, cudaGetErrorString(e));
+        rc = BV_E_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&d_c, sizeof(double) * 2 * (size_t)bc)) != cudaSuccess) {
+        fail(e, "cudaMalloc");
+        return rc;
+    }
+    if ((e = cudaMalloc(&d_counter, sizeof(unsigned) + sizeof(int))) != cudaSuccess) {
+        cudaFree(d_c);
+        fail(e, "cudaMalloc");
+        return rc;
+    }
+    d_err = reinterpret_cast<int *>(d_counter + 1);
+    do {
+        if ((e = cudaMemcpyAsync(d_c, cx, sizeof(double) * bc, cudaMemcpyHostToDevice, s)) ||
+            (e = cudaMemcpyAsync(d_c + bc, cy, sizeof(double) * bc, cudaMemcpyHostToDevice, s)) ||
+            (e = cudaMemcpyAsync(d_knn, first.data(), sizeof(int) * cs, cudaMemcpyHostToDevice, s)) ||
+            (e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned) + sizeof(int), s))) {
+            fail(e, "copy");
+            break;
+        }
+        KnnArgs ka;
+        ka.x = d_x;
+        ka.y = d_y;
+        ka.acc = d_acc;
+        ka.cx = d_c;
+        ka.cy = d_c + bc;
+        ka.bc = bc;
+        ka.cs = cs;
+        ka.out = d_knn;
+        ka.counter = d_counter;
+        ka.error = d_err;
+        const size_t smem = sizeof(KnnWarpSmem) * kKnnWarps;
+        if ((e = cudaFuncSetAttribute(knn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem))) {
+            fail(e, "attribute");
+            break;
+        }
+        int dev = 0, sms = 0, occ = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, knn_kernel, kKnnWarps * 32, smem);
+        if (occ < 1) occ = 1;
+        int grid = sms * occ;
+        const int need = (bc + kKnnWarps - 1) / kKnnWarps;
+        if (grid > need) grid = need > 0 ? need : 1;
+        knn_kernel<<<grid, kKnnWarps * 32, smem, s>>>(ka);
+        if ((e = cudaGetLastError())) {
+            fail(e, "launch");
+            break;
+        }
+        int herr = 0;
+        if ((e = cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
+            (e = cudaStreamSynchronize(s))) {
+            fail(e, "sync");
+            break;
+        }
+        if (herr) {
+            set_error("bv_knn: block %d has fewer than cs=%d earlier points or more than %d "
+                      "candidates tie at its cs-th distance",
+                      herr - 1, cs, kKnnCap - 128);
+            rc = BV_E_TOOLARGE;
+        }
+    } while (0);
+    cudaFree(d_c);
+    cudaFree(d_counter);
+    return rc;
+}
+
+}  // namespace bv
+
+extern "C" int bv_knn(const double *x, const double *y, int n, int bc, int cs,
+                      const int *batchNumAccum, const double *cx, const double *cy, int *knn_idx,
+                      int device)
+{
+    using namespace bv;
+    if (!x || !y || !batchNumAccum || !cx || !cy || !knn_idx || n <= 0 || bc <= 0 || cs < 0) {
+        set_error("bv_knn: invalid argument");
+        return BV_E_INVALID;
+    }
+    if (batchNumAccum[0] != 0 || batchNumAccum[bc] > n) {
+        set_error("bv_knn: batchNumAccum must start at 0 and stay within n");
+        return BV_E_INVALID;
+    }
+    for (int i = 1; i < bc; ++i)
+        if (batchNumAccum[i] < cs) {
+            set_error("bv_knn: block %d has %d earlier points < cs=%d", i, batchNumAccum[i], cs);
+            return BV_E_INVALID;
+        }
+    if (cs == 0) return BV_OK;
+    BV_CUDA_TRY(cudaSetDevice(device));
+    cudaStream_t s;
+    BV_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    double *d_x = nullptr, *d_y = nullptr;
+    int *d_acc = nullptr, *d_knn = nullptr;
+    int rc = BV_OK;
+    cudaError_t e;
+    do {
+        if ((e = cudaMalloc(&d_x, sizeof(double) * n)) || (e = cudaMalloc(&d_y, sizeof(double) * n)) ||
+            (e = cudaMalloc(&d_acc, sizeof(int) * (bc + 1))) ||
+            (e = cudaMalloc(&d_knn, sizeof(int) * (size_t)bc * cs))) {
+            set_error("bv_knn: cudaMalloc: %s", cudaGetErrorString(e));
+            rc = (e == cudaErrorMemoryAllocation) ? BV_E_NOMEM : BV_E_CUDA;
+            break;
+        }
+        if ((e = cudaMemcpyAsync(d_x, x, sizeof(double) * n, cudaMemcpyHostToDevice, s)) ||
+            (e = cudaMemcpyAsync(d_y, y, sizeof(double) * n, cudaMemcpyHostToDevice, s)) ||
+            (e = cudaMemcpyAsync(d_acc, batchNumAccum, sizeof(int) * (bc + 1), cudaMemcpyHostToDevice, s))) {
+            set_error("bv_knn: copy: %s", cudaGetErrorString(e));
+            rc = BV_E_CUDA;
+            break;
+        }
+        rc = knn_device(d_x, d_y, n, bc, cs, d_acc, cx, cy, d_knn, s);
+        if (rc) break;
+        if ((e = cudaMemcpyAsync(knn_idx, d_knn, sizeof(int) * (size_t)bc * cs, cudaMemcpyDeviceToHost, s)) ||
+            (e = cudaStreamSynchronize(s))) {
+            set_error("bv_knn: copy back: %s", cudaGetErrorString(e));
+            rc = BV_E_CUDA;
+        }
+    } while (0);
+    cudaFree(d_x);
+    cudaFree(d_y);
+    cudaFree(d_acc);
+    cudaFree(d_knn);
+    cudaStreamDestroy(s);
+    return rc;
+}

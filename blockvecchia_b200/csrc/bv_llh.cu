@@ -1,0 +1,662 @@
+// bv_llh.cu -- handle, schedule and C ABI of the block-Vecchia likelihood.
+//
+// Replaces the device side of the reference's objective
+// llh_Xvecchia_batch<double> (include/llh_Xvecchia_batch.h:22-522) and the
+// device allocations of its driver (src/test_Xvecchia_batch.cpp:459-600).
+// Layout data (locations, observations, conditioning indices) is copied to
+// HBM once at bv_create; one evaluation moves 48 bytes of parameters in and
+// one result record out, and runs as a CUDA graph:
+//   H2D params -> zero work counter -> fused per-block kernel(s)
+//   -> deterministic reduction -> D2H result.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "../../include/bv.h"
+#include "bv_common.cuh"
+#include "bv_knn.cuh"
+#include "bv_llh_fp64.cuh"
+#include "bv_llh_mixed.cuh"
+
+namespace bv {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+const char *get_error() { return g_err; }
+
+// Result record of one evaluation (device, then pinned host).
+struct EvalResult {
+    double llk;
+    int blocks, cond_fail, schur_fail, fallback, nonfinite;
+    unsigned flags_or;
+    int pad;
+};
+
+constexpr int kReduceThreads = 1024;
+
+// Deterministic reduction of the per-block contributions: every thread sums
+// a contiguous chunk in block order with Neumaier compensation, then the
+// partial (sum, compensation) pairs are combined in a fixed tree order.
+__global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const double *v,
+                                                                const unsigned *st, int n,
+                                                                EvalResult *out)
+{
+    __shared__ double s_s[kReduceThreads], s_c[kReduceThreads];
+    __shared__ int s_cnt[5][kReduceThreads / 32];
+    __shared__ unsigned s_or[kReduceThreads / 32];
+    const int t = threadIdx.x;
+    const int chunk = (n + kReduceThreads - 1) / kReduceThreads;
+    const int b0 = t * chunk, b1 = min(n, b0 + chunk);
+    double s = 0.0, c = 0.0;
+    int cf = 0, sf = 0, fb = 0, nf = 0, nb = 0;
+    unsigned fo = 0;
+    for (int i = b0; i < b1; ++i) {
+        const double x = v[i];
+        const double tt = s + x;
+        if (fabs(s) >= fabs(x))
+            c += (s - tt) + x;
+        else
+            c += (x - tt) + s;
+        s = tt;
+        const unsigned f = st[i];
+        fo |= f;
+        cf += (f & BV_ST_COND_FAIL) ? 1 : 0;
+        sf += (f & BV_ST_SCHUR_FAIL) ? 1 : 0;
+        fb += (f & BV_ST_FP32_FALLBACK) ? 1 : 0;
+        nf += (f & BV_ST_NONFINITE) ? 1 : 0;
+        ++nb;
+    }
+    s_s[t] = s;
+    s_c[t] = c;
+    // counts: warp reduce
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        cf += __shfl_xor_sync(0xffffffffu, cf, o);
+        sf += __shfl_xor_sync(0xffffffffu, sf, o);
+        fb += __shfl_xor_sync(0xffffffffu, fb, o);
+        nf += __shfl_xor_sync(0xffffffffu, nf, o);
+        nb += __shfl_xor_sync(0xffffffffu, nb, o);
+        fo |= __shfl_xor_sync(0xffffffffu, fo, o);
+    }
+    if ((t & 31) == 0) {
+        s_cnt[0][t >> 5] = cf;
+        s_cnt[1][t >> 5] = sf;
+        s_cnt[2][t >> 5] = fb;
+        s_cnt[3][t >> 5] = nf;
+        s_cnt[4][t >> 5] = nb;
+        s_or[t >> 5] = fo;
+    }
+    __syncthreads();
+    for (int w = kReduceThreads / 2; w > 0; w >>= 1) {
+        if (t < w) {
+            const double a = s_s[t], b = s_s[t + w];
+            const double tt = a + b;
+            double cc = s_c[t] + s_c[t + w];
+            if (fabs(a) >= fabs(b))
+                cc += (a - tt) + b;
+            else
+                cc += (b - tt) + a;
+            s_s[t] = tt;
+            s_c[t] = cc;
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        EvalResult r;
+        r.llk = s_s[0] + s_c[0];
+        int c5[5] = {0, 0, 0, 0, 0};
+        unsigned o = 0;
+        for (int w = 0; w < kReduceThreads / 32; ++w) {
+            for (int q = 0; q < 5; ++q) c5[q] += s_cnt[q][w];
+            o |= s_or[w];
+        }
+        r.cond_fail = c5[0];
+        r.schur_fail = c5[1];
+        r.fallback = c5[2];
+        r.nonfinite = c5[3];
+        r.blocks = c5[4];
+        r.flags_or = o;
+        r.pad = 0;
+        *out = r;
+    }
+}
+
+}  // namespace bv
+
+using namespace bv;
+
+struct bv_handle {
+    std::mutex mu;
+    bv_opts opts;
+    int device = 0;
+    int n = 0, bc = 0, cs = 0;
+    int max_m = 0;
+    std::vector<int> batchNum, acc, order;
+    // device
+    double *d_x = nullptr, *d_y = nullptr, *d_obs = nullptr;
+    int *d_acc = nullptr, *d_knn = nullptr, *d_order = nullptr;
+    double *d_block_llk = nullptr;
+    unsigned *d_block_status = nullptr;
+    unsigned *d_counters = nullptr;  // one per launch
+    double *d_slab = nullptr;
+    size_t slab_stride = 0;
+    MaternParams *d_mp = nullptr;
+    EvalResult *d_res = nullptr;
+    MixedWork mixed;  // mixed-precision scratch (bv_llh_mixed.cuh)
+    // pinned host
+    MaternParams *h_mp = nullptr;
+    EvalResult *h_res = nullptr;
+    // launch plan
+    int smem_max_m = 0;
+    size_t smem_bytes = 0;
+    int grid = 0;
+    struct Launch {
+        int begin, end, grid;
+    };
+    std::vector<Launch> launches;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // status
+    bv_status status{};
+    int iterations = 0;
+};
+
+static void handle_free(bv_handle *h)
+{
+    if (!h) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(h->device);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    cudaFree(h->d_x);
+    cudaFree(h->d_y);
+    cudaFree(h->d_obs);
+    cudaFree(h->d_acc);
+    cudaFree(h->d_knn);
+    cudaFree(h->d_order);
+    cudaFree(h->d_block_llk);
+    cudaFree(h->d_block_status);
+    cudaFree(h->d_counters);
+    cudaFree(h->d_slab);
+    cudaFree(h->d_mp);
+    cudaFree(h->d_res);
+    mixed_free(h->mixed);
+    cudaFreeHost(h->h_mp);
+    cudaFreeHost(h->h_res);
+    cudaSetDevice(prev);
+    delete h;
+}
+
+extern "C" void bv_default_opts(bv_opts *o)
+{
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->precision = BV_PREC_FP64;
+    o->kernel = 1;
+    o->dist_scale = 1.0;
+    o->device = 0;
+    o->on_failure = BV_FAIL_NEGINF;
+    o->print_iter = 0;
+    o->use_graph = 1;
+    o->schedule = 0;
+    o->mixed_tol = 1e-11;
+}
+
+extern "C" const char *bv_last_error(void) { return get_error(); }
+
+static int validate_layout(const bv_layout *L)
+{
+    if (!L || L->n <= 0 || L->bc <= 0 || L->cs < 0 || !L->batchNum || !L->batchNumAccum ||
+        !L->x || !L->y || !L->obs) {
+        set_error("bv_create: null or non-positive layout field");
+        return BV_E_INVALID;
+    }
+    if (L->batchNumAccum[0] != 0 || L->batchNumAccum[L->bc] != L->n) {
+        set_error("bv_create: batchNumAccum must start at 0 and end at n (got %d, %d, n=%d)",
+                  L->batchNumAccum[0], L->batchNumAccum[L->bc], L->n);
+        return BV_E_INVALID;
+    }
+    for (int i = 0; i < L->bc; ++i) {
+        if (L->batchNum[i] < 0 || L->batchNumAccum[i + 1] - L->batchNumAccum[i] != L->batchNum[i]) {
+            set_error("bv_create: batchNum[%d] inconsistent with batchNumAccum", i);
+            return BV_E_INVALID;
+        }
+    }
+    if (L->cs > 0 && L->bc > 1 && L->batchNum[0] < L->cs) {
+        set_error("bv_create: block 0 has %d points < cs=%d (firstbatch merges clusters until "
+                  ">= cs)", L->batchNum[0], L->cs);
+        return BV_E_INVALID;
+    }
+    if (L->cs > 0 && L->knn_idx) {
+        for (int i = 1; i < L->bc; ++i) {
+            const int lim = L->batchNumAccum[i];
+            const int *k = L->knn_idx + (size_t)i * L->cs;
+            for (int t = 0; t < L->cs; ++t)
+                if (k[t] < 0 || k[t] >= lim) {
+                    set_error("bv_create: knn_idx[%d*cs+%d]=%d outside the earlier blocks [0,%d)",
+                              i, t, k[t], lim);
+                    return BV_E_INVALID;
+                }
+        }
+        for (int t = 0; t < L->cs; ++t)
+            if (L->knn_idx[t] < 0 || L->knn_idx[t] >= L->n) {
+                set_error("bv_create: knn_idx[%d]=%d outside [0,n)", t, L->knn_idx[t]);
+                return BV_E_INVALID;
+            }
+    }
+    if (L->cs > 0 && !L->knn_idx && (!L->cx || !L->cy)) {
+        set_error("bv_create: knn_idx is NULL and no block centroids were given");
+        return BV_E_INVALID;
+    }
+    return BV_OK;
+}
+
+// Largest M whose block fits in `bytes` of dynamic shared memory.
+static int max_m_for_bytes(size_t bytes, size_t per_double)
+{
+    int lo = 1, hi = 4096;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) / 2;
+        if (block_doubles(mid) * per_double <= bytes)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+static int plan_launches(bv_handle *h)
+{
+    cudaDeviceProp prop;
+    BV_CUDA_TRY(cudaGetDeviceProperties(&prop, h->device));
+    int optin = 0;
+    BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    const size_t static_smem = 2048;  // the kernel's static shared arrays, rounded up
+    const size_t avail = (size_t)optin - static_smem;
+    const int cap_m = max_m_for_bytes(avail, sizeof(double));
+    h->smem_max_m = std::min(cap_m, h->max_m);
+    h->smem_bytes = block_doubles(h->smem_max_m) * sizeof(double);
+    BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)h->smem_bytes));
+    int occ = 0;
+    BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, llh_fp64_kernel, kThreads,
+                                                              h->smem_bytes));
+    if (occ < 1) {
+        set_error("plan: fused kernel cannot be resident (smem %zu B)", h->smem_bytes);
+        return BV_E_TOOLARGE;
+    }
+    h->grid = prop.multiProcessorCount * occ;
+    if (h->max_m > h->smem_max_m) {
+        h->slab_stride = (block_doubles(h->max_m) + 31) & ~(size_t)31;
+        const size_t bytes = h->slab_stride * sizeof(double) * (size_t)h->grid;
+        if (cudaMalloc(&h->d_slab, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("plan: cannot allocate %zu B of block slabs", bytes);
+            return BV_E_NOMEM;
+        }
+    }
+    h->launches.clear();
+    if (h->opts.schedule == 0) {
+        h->launches.push_back({0, h->bc, h->grid});
+    } else {
+        // One launch per size bucket of M (width 8), largest first.
+        int b = 0;
+        while (b < h->bc) {
+            const int mb = h->batchNum[h->order[b]] + (h->order[b] == 0 ? 0 : h->cs);
+            const int bucket = mb / 8;
+            int e = b;
+            while (e < h->bc) {
+                const int me = h->batchNum[h->order[e]] + (h->order[e] == 0 ? 0 : h->cs);
+                if (me / 8 != bucket) break;
+                ++e;
+            }
+            h->launches.push_back({b, e, std::min(h->grid, e - b)});
+            b = e;
+        }
+    }
+    BV_CUDA_TRY(cudaMalloc(&h->d_counters, sizeof(unsigned) * h->launches.size()));
+    return BV_OK;
+}
+
+static int enqueue_eval(bv_handle *h, cudaStream_t s)
+{
+    BV_CUDA_TRY(cudaMemcpyAsync(h->d_mp, h->h_mp, sizeof(MaternParams), cudaMemcpyHostToDevice, s));
+    BV_CUDA_TRY(cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned) * h->launches.size(), s));
+    if (h->opts.precision == BV_PREC_MIXED) {
+        int rc = mixed_enqueue(h->mixed, s);
+        if (rc) return rc;
+    } else {
+        for (size_t l = 0; l < h->launches.size(); ++l) {
+            LlhArgs a;
+            a.x = h->d_x;
+            a.y = h->d_y;
+            a.obs = h->d_obs;
+            a.acc = h->d_acc;
+            a.knn = h->d_knn;
+            a.order = h->d_order;
+            a.bc = h->bc;
+            a.cs = h->cs;
+            a.smem_max_m = h->smem_max_m;
+            a.slab_max_m = h->max_m;
+            a.block_llk = h->d_block_llk;
+            a.block_status = h->d_block_status;
+            a.work_counter = h->d_counters + l;
+            a.gslab = h->d_slab;
+            a.gslab_stride = h->slab_stride;
+            a.log2pi = std::log(2 * 3.141592653589793);
+            a.mp = h->d_mp;
+            a.task_begin = h->launches[l].begin;
+            a.task_end = h->launches[l].end;
+            llh_fp64_kernel<<<h->launches[l].grid, kThreads, h->smem_bytes, s>>>(a);
+            BV_CUDA_TRY(cudaGetLastError());
+        }
+    }
+    reduce_kernel<<<1, kReduceThreads, 0, s>>>(h->d_block_llk, h->d_block_status, h->bc, h->d_res);
+    BV_CUDA_TRY(cudaGetLastError());
+    BV_CUDA_TRY(cudaMemcpyAsync(h->h_res, h->d_res, sizeof(EvalResult), cudaMemcpyDeviceToHost, s));
+    return BV_OK;
+}
+
+extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **out)
+{
+    if (!out) {
+        set_error("bv_create: out is NULL");
+        return BV_E_INVALID;
+    }
+    *out = nullptr;
+    int rc = validate_layout(L);
+    if (rc) return rc;
+    bv_handle *h = new (std::nothrow) bv_handle();
+    if (!h) return BV_E_NOMEM;
+    if (opts)
+        h->opts = *opts;
+    else
+        bv_default_opts(&h->opts);
+    if (!(h->opts.dist_scale > 0)) h->opts.dist_scale = 1.0;
+    h->device = h->opts.device;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= h->device) {
+        cudaGetLastError();
+        set_error("bv_create: no CUDA device %d", h->device);
+        delete h;
+        return BV_E_NODEVICE;
+    }
+#define BV_TRY_H(expr)            \
+    do {                          \
+        int _rc = (expr);         \
+        if (_rc) {                \
+            handle_free(h);       \
+            return _rc;           \
+        }                         \
+    } while (0)
+#define BV_CUDA_H(expr)                                                                  \
+    do {                                                                                 \
+        cudaError_t _e = (expr);                                                         \
+        if (_e != cudaSuccess) {                                                         \
+            set_error("%s: %s", #expr, cudaGetErrorString(_e));                          \
+            handle_free(h);                                                              \
+            return (_e == cudaErrorMemoryAllocation) ? BV_E_NOMEM : BV_E_CUDA;           \
+        }                                                                                \
+    } while (0)
+    BV_CUDA_H(cudaSetDevice(h->device));
+    cudaDeviceProp prop;
+    BV_CUDA_H(cudaGetDeviceProperties(&prop, h->device));
+    if (prop.major < 10) {
+        set_error("bv_create: device %d is sm_%d%d; this library is built for sm_100a", h->device,
+                  prop.major, prop.minor);
+        handle_free(h);
+        return BV_E_NODEVICE;
+    }
+    h->n = L->n;
+    h->bc = L->bc;
+    h->cs = L->cs;
+    h->batchNum.assign(L->batchNum, L->batchNum + L->bc);
+    h->acc.assign(L->batchNumAccum, L->batchNumAccum + L->bc + 1);
+    h->max_m = 1;
+    for (int b = 0; b < h->bc; ++b)
+        h->max_m = std::max(h->max_m, h->batchNum[b] + (b == 0 ? 0 : h->cs));
+    // Largest blocks first (longest-processing-time order), ties by index.
+    h->order.resize(h->bc);
+    std::iota(h->order.begin(), h->order.end(), 0);
+    std::stable_sort(h->order.begin(), h->order.end(), [&](int a, int b) {
+        const int ma = h->batchNum[a] + (a == 0 ? 0 : h->cs);
+        const int mb = h->batchNum[b] + (b == 0 ? 0 : h->cs);
+        return ma > mb;
+    });
+
+    BV_CUDA_H(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    BV_CUDA_H(cudaEventCreate(&h->ev0));
+    BV_CUDA_H(cudaEventCreate(&h->ev1));
+    const size_t n = h->n, bc = h->bc, cs = h->cs;
+    BV_CUDA_H(cudaMalloc(&h->d_x, n * sizeof(double)));
+    BV_CUDA_H(cudaMalloc(&h->d_y, n * sizeof(double)));
+    BV_CUDA_H(cudaMalloc(&h->d_obs, n * sizeof(double)));
+    BV_CUDA_H(cudaMalloc(&h->d_acc, (bc + 1) * sizeof(int)));
+    BV_CUDA_H(cudaMalloc(&h->d_knn, std::max<size_t>(1, bc * cs) * sizeof(int)));
+    BV_CUDA_H(cudaMalloc(&h->d_order, bc * sizeof(int)));
+    BV_CUDA_H(cudaMalloc(&h->d_block_llk, bc * sizeof(double)));
+    BV_CUDA_H(cudaMalloc(&h->d_block_status, bc * sizeof(unsigned)));
+    BV_CUDA_H(cudaMalloc(&h->d_mp, sizeof(MaternParams)));
+    BV_CUDA_H(cudaMalloc(&h->d_res, sizeof(EvalResult)));
+    BV_CUDA_H(cudaMallocHost(&h->h_mp, sizeof(MaternParams)));
+    BV_CUDA_H(cudaMallocHost(&h->h_res, sizeof(EvalResult)));
+    BV_CUDA_H(cudaMemcpy(h->d_x, L->x, n * sizeof(double), cudaMemcpyHostToDevice));
+    BV_CUDA_H(cudaMemcpy(h->d_y, L->y, n * sizeof(double), cudaMemcpyHostToDevice));
+    BV_CUDA_H(cudaMemcpy(h->d_obs, L->obs, n * sizeof(double), cudaMemcpyHostToDevice));
+    BV_CUDA_H(cudaMemcpy(h->d_acc, L->batchNumAccum, (bc + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    BV_CUDA_H(cudaMemcpy(h->d_order, h->order.data(), bc * sizeof(int), cudaMemcpyHostToDevice));
+    if (cs > 0) {
+        if (L->knn_idx) {
+            BV_CUDA_H(cudaMemcpy(h->d_knn, L->knn_idx, bc * cs * sizeof(int), cudaMemcpyHostToDevice));
+        } else {
+            BV_TRY_H(knn_device(h->d_x, h->d_y, h->n, h->bc, h->cs, h->d_acc, L->cx, L->cy,
+                                h->d_knn, h->stream));
+            BV_CUDA_H(cudaStreamSynchronize(h->stream));
+        }
+    }
+    BV_TRY_H(plan_launches(h));
+    if (h->opts.precision == BV_PREC_MIXED) {
+        MixedSetup ms;
+        ms.x = h->d_x;
+        ms.y = h->d_y;
+        ms.obs = h->d_obs;
+        ms.acc = h->d_acc;
+        ms.knn = h->d_knn;
+        ms.order = h->d_order;
+        ms.bc = h->bc;
+        ms.cs = h->cs;
+        ms.max_m = h->max_m;
+        ms.block_llk = h->d_block_llk;
+        ms.block_status = h->d_block_status;
+        ms.mp = h->d_mp;
+        ms.tol = h->opts.mixed_tol;
+        ms.fp64_smem_max_m = h->smem_max_m;
+        ms.fp64_smem_bytes = h->smem_bytes;
+        ms.fp64_grid = h->grid;
+        ms.fp64_slab = h->d_slab;
+        ms.fp64_slab_stride = h->slab_stride;
+        BV_TRY_H(mixed_create(h->mixed, ms));
+    }
+    if (h->opts.use_graph) {
+        BV_CUDA_H(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int erc = enqueue_eval(h, h->stream);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+        if (erc || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            if (!erc) set_error("graph capture: %s", cudaGetErrorString(ce));
+            handle_free(h);
+            return erc ? erc : BV_E_CUDA;
+        }
+        h->graph = g;
+        BV_CUDA_H(cudaGraphInstantiate(&h->gexec, h->graph, 0));
+    }
+#undef BV_TRY_H
+#undef BV_CUDA_H
+    *out = h;
+    return BV_OK;
+}
+
+extern "C" void bv_destroy(bv_handle *h) { handle_free(h); }
+
+static int fill_params(bv_handle *h, const double *theta)
+{
+    const double sigma2 = theta[0], range = theta[1], nu = theta[2];
+    if (!std::isfinite(sigma2) || !(range > 0) || !(nu > 0) || !std::isfinite(range) ||
+        !std::isfinite(nu)) {
+        set_error("bv_llh: invalid theta (%g, %g, %g)", sigma2, range, nu);
+        return BV_E_INVALID;
+    }
+    MaternParams &p = *h->h_mp;
+    p.sigma2 = sigma2;
+    p.range = range;
+    p.nu = nu;
+    // src/ckernel.cpp:1072-1075, evaluated on the host as the reference does.
+    double con = std::pow(2.0, nu - 1.0) * std::tgamma(nu);
+    con = 1.0 / con;
+    con = sigma2 * con;
+    p.con = con;
+    p.dist_scale = h->opts.dist_scale;
+    p.scale_is_one = (h->opts.dist_scale == 1.0) ? 1 : 0;
+    p.nu_kind = (nu == 0.5) ? kNuHalf : (nu == 1.5) ? kNuThreeHalves : (nu == 2.5) ? kNuFiveHalves
+                                                                                  : kNuGeneral;
+    return BV_OK;
+}
+
+static int eval_locked(bv_handle *h, const double *theta, double *llk)
+{
+    int rc = fill_params(h, theta);
+    if (rc) return rc;
+    BV_CUDA_TRY(cudaSetDevice(h->device));
+    BV_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+    if (h->gexec) {
+        BV_CUDA_TRY(cudaGraphLaunch(h->gexec, h->stream));
+    } else {
+        rc = enqueue_eval(h, h->stream);
+        if (rc) return rc;
+    }
+    BV_CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
+    BV_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    const EvalResult r = *h->h_res;
+    bv_status &s = h->status;
+    s.blocks = r.blocks;
+    s.cond_fail = r.cond_fail;
+    s.schur_fail = r.schur_fail;
+    s.fp32_fallback = r.fallback;
+    s.nonfinite = r.nonfinite;
+    s.flags_or = r.flags_or;
+    s.llk = r.llk;
+    s.device_ms = ms;
+    double v = r.llk;
+    const bool failed = (r.cond_fail + r.schur_fail + r.nonfinite) > 0 || !std::isfinite(v);
+    if (failed && h->opts.on_failure == BV_FAIL_NEGINF) v = -HUGE_VAL;
+    *llk = v;
+    return BV_OK;
+}
+
+static void print_iteration(bv_handle *h, const double *theta, double llk)
+{
+    // include/llh_Xvecchia_batch.h:500-511
+    if (h->opts.kernel == 3)
+        printf("%dth Model Parameters (Variance, range, smoothness, nugget): (%1.8lf, %1.8lf, "
+               "%1.8lf, %1.8lf) -> Loglik: %.18lf \n",
+               h->iterations, theta[0], theta[1], theta[2], theta[3], llk);
+    else
+        printf("%dth Model Parameters (Variance, range, smoothness): (%1.8lf, %1.8lf, %1.8lf) -> "
+               "Loglik: %.18lf \n",
+               h->iterations, theta[0], theta[1], theta[2], llk);
+}
+
+extern "C" int bv_llh_eval(bv_handle *h, const double *theta, double *llk)
+{
+    if (!h || !theta || !llk) {
+        set_error("bv_llh_eval: null argument");
+        return BV_E_INVALID;
+    }
+    std::lock_guard<std::mutex> lk(h->mu);
+    int rc = eval_locked(h, theta, llk);
+    if (rc == BV_OK) {
+        if (h->opts.print_iter) print_iteration(h, theta, *llk);
+        h->iterations += 1;
+    }
+    return rc;
+}
+
+extern "C" double bv_llh(unsigned n, const double *theta, double *grad, void *f_data)
+{
+    (void)grad;
+    bv_handle *h = static_cast<bv_handle *>(f_data);
+    if (!h || !theta || n < 3) {
+        set_error("bv_llh: need a handle and at least 3 parameters");
+        return -HUGE_VAL;
+    }
+    double v = -HUGE_VAL;
+    if (bv_llh_eval(h, theta, &v) != BV_OK) return -HUGE_VAL;
+    return v;
+}
+
+extern "C" int bv_llh_host(bv_handle *h, const double *x, const double *y, const double *obs,
+                           const int *knn_idx, const double *theta, double *llk)
+{
+    if (!h || !obs || !theta || !llk) {
+        set_error("bv_llh_host: null argument");
+        return BV_E_INVALID;
+    }
+    std::lock_guard<std::mutex> lk(h->mu);
+    BV_CUDA_TRY(cudaSetDevice(h->device));
+    const size_t n = h->n;
+    if (x) BV_CUDA_TRY(cudaMemcpyAsync(h->d_x, x, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (y) BV_CUDA_TRY(cudaMemcpyAsync(h->d_y, y, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    BV_CUDA_TRY(cudaMemcpyAsync(h->d_obs, obs, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (knn_idx && h->cs > 0)
+        BV_CUDA_TRY(cudaMemcpyAsync(h->d_knn, knn_idx, (size_t)h->bc * h->cs * sizeof(int),
+                                    cudaMemcpyHostToDevice, h->stream));
+    int rc = eval_locked(h, theta, llk);
+    if (rc == BV_OK) h->iterations += 1;
+    return rc;
+}
+
+extern "C" int bv_block_llk(bv_handle *h, double *out, int count)
+{
+    if (!h || !out || count < h->bc) {
+        set_error("bv_block_llk: need room for %d values", h ? h->bc : 0);
+        return BV_E_INVALID;
+    }
+    std::lock_guard<std::mutex> lk(h->mu);
+    BV_CUDA_TRY(cudaSetDevice(h->device));
+    BV_CUDA_TRY(cudaMemcpy(out, h->d_block_llk, sizeof(double) * h->bc, cudaMemcpyDeviceToHost));
+    return BV_OK;
+}
+
+extern "C" int bv_get_status(bv_handle *h, bv_status *st)
+{
+    if (!h || !st) return BV_E_INVALID;
+    std::lock_guard<std::mutex> lk(h->mu);
+    *st = h->status;
+    return BV_OK;
+}
+
+extern "C" int bv_iterations(bv_handle *h) { return h ? h->iterations : 0; }

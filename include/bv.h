@@ -1,0 +1,178 @@
+/*
+ * bv.h -- C ABI of libbv_b200.so, the B200-native block-Vecchia
+ * log-likelihood library.
+ *
+ * Plain pointers and sizes only.  Host pointers unless a name says "_dev".
+ * Every entry point returns 0 on success or a negative BV_E* code; the
+ * library never exits the process.  bv_llh keeps the NLopt objective
+ * signature of the reference's llh_Xvecchia_batch so it drops into
+ * nlopt_set_max_objective unchanged.
+ */
+#ifndef BV_H
+#define BV_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------- codes */
+#define BV_OK 0
+#define BV_E_INVALID (-1)   /* bad argument                                  */
+#define BV_E_CUDA (-2)      /* CUDA runtime error (message: bv_last_error)   */
+#define BV_E_NOMEM (-3)     /* device allocation failed                      */
+#define BV_E_NODEVICE (-4)  /* no usable sm_100 device                       */
+#define BV_E_TOOLARGE (-5)  /* a size exceeds a documented maximum           */
+#define BV_E_TIMEOUT (-6)   /* a bounded device wait gave up                 */
+
+#define BV_PREC_FP64 0  /* plain FP64 method (reference semantics)           */
+#define BV_PREC_MIXED 1 /* FP32 factor + FP64 refinement, FP64 fallback      */
+
+#define BV_FAIL_NEGINF 0   /* a failed block makes bv_llh return -HUGE_VAL  */
+#define BV_FAIL_CONTINUE 1 /* keep going like the reference: a non-positive
+                              pivot is skipped in the log-determinant        */
+
+/* Per-evaluation block status bits (bv_status.flags_or). */
+#define BV_ST_COND_FAIL 1u   /* non-positive / NaN pivot in Sigma22          */
+#define BV_ST_SCHUR_FAIL 2u  /* non-positive / NaN pivot in Sigma11'         */
+#define BV_ST_FP32_FALLBACK 4u /* mixed path redid the block in FP64         */
+#define BV_ST_NONFINITE 8u   /* a block's contribution was not finite        */
+
+/* ---------------------------------------------------------------- layout */
+/*
+ * The block layout the reference's driver builds before the optimizer runs
+ * (src/test_Xvecchia_batch.cpp:240-404): blocks in random centroid order,
+ * block 0 = the first clusters merged until >= cs points, points of a block
+ * in ascending original index, conditioning sets of cs points per block.
+ */
+typedef struct {
+    int n;                     /* number of locations                        */
+    int bc;                    /* number of blocks (batchCount)              */
+    int cs;                    /* conditioning size (vecchia_cs)             */
+    const int *batchNum;       /* [bc]   points per block                    */
+    const int *batchNumAccum;  /* [bc+1] block offsets, [bc] == n            */
+    const double *x;           /* [n]    block-ordered locations_new->x      */
+    const double *y;           /* [n]    block-ordered locations_new->y      */
+    const double *obs;         /* [n]    block-ordered h_obs_new             */
+    const int *knn_idx;        /* [bc*cs] conditioning indices into x/y/obs;
+                                  NULL: computed on the device by bv_knn
+                                  from cx/cy                                 */
+    const double *cx;          /* [bc]   block centroids (locsCentroid[i +
+                                  firstClusterCount - 1]); used if knn_idx
+                                  is NULL                                    */
+    const double *cy;
+} bv_layout;
+
+typedef struct {
+    int precision;     /* BV_PREC_FP64 | BV_PREC_MIXED                        */
+    int kernel;        /* 1,2,3: Matern (the reference's llh evaluates Matern
+                          for all three, include/llh_Xvecchia_batch.h:126-144) */
+    double dist_scale; /* --dist_scale, default 1.0                           */
+    int device;        /* CUDA device ordinal                                 */
+    int on_failure;    /* BV_FAIL_NEGINF | BV_FAIL_CONTINUE                   */
+    int print_iter;    /* print the reference's per-evaluation line           */
+    int use_graph;     /* capture one evaluation in a CUDA graph (default 1)  */
+    int schedule;      /* 0 persistent work queue (default), 1 one launch per
+                          size bucket (the comparison baseline)               */
+    double mixed_tol;  /* mixed path: refinement residual tolerance           */
+} bv_opts;
+
+typedef struct {
+    int blocks;          /* blocks evaluated                                 */
+    int cond_fail;       /* blocks with a failed Sigma22 pivot               */
+    int schur_fail;      /* blocks with a failed Sigma11' pivot              */
+    int fp32_fallback;   /* mixed path: blocks redone in FP64                */
+    int nonfinite;       /* blocks whose contribution was not finite         */
+    unsigned flags_or;   /* OR of BV_ST_* over all blocks                    */
+    double llk;          /* last log-likelihood (before the failure policy)  */
+    double device_ms;    /* device time of the last evaluation               */
+} bv_status;
+
+typedef struct bv_handle bv_handle;
+
+/* Fill *o with the defaults (FP64, Matern, dist_scale 1, device 0,
+ * BV_FAIL_NEGINF, no printing, graphs on, persistent schedule). */
+void bv_default_opts(bv_opts *o);
+
+/* Create a handle: validates the layout, copies it to the device once
+ * (replaces the device allocations and copies of
+ * src/test_Xvecchia_batch.cpp:459-600), computes the conditioning sets on the
+ * device when layout->knn_idx is NULL, and plans the block schedule.
+ * The caller keeps ownership of its arrays. */
+int bv_create(const bv_layout *layout, const bv_opts *opts, bv_handle **out);
+void bv_destroy(bv_handle *h);
+
+/* NLopt objective (replaces llh_Xvecchia_batch<double>,
+ * include/llh_Xvecchia_batch.h:24): n = number of parameters (3 for Matern),
+ * theta = {sigma2, range, nu}, grad ignored (derivative-free optimizer),
+ * f_data = bv_handle*.  Returns the block-Vecchia log-likelihood; on a block
+ * failure under BV_FAIL_NEGINF, or on an error, returns -HUGE_VAL and records
+ * the reason in bv_get_status / bv_last_error. */
+double bv_llh(unsigned n, const double *theta, double *grad, void *f_data);
+
+/* Same evaluation with an explicit status code. */
+int bv_llh_eval(bv_handle *h, const double *theta, double *llk);
+
+/* Per-block contributions of the last evaluation, copied to host [bc]. */
+int bv_block_llk(bv_handle *h, double *out, int count);
+
+int bv_get_status(bv_handle *h, bv_status *st);
+int bv_iterations(bv_handle *h);
+const char *bv_last_error(void);
+
+/* End-to-end evaluation from host buffers: copies obs[n] (and, when not
+ * NULL, x/y[n] and knn_idx[bc*cs]) of a layout with the handle's shapes to
+ * the device, evaluates, and returns the log-likelihood.  Used when the
+ * observations change between calls (simulation studies, serving). */
+int bv_llh_host(bv_handle *h, const double *x, const double *y,
+                const double *obs, const int *knn_idx, const double *theta,
+                double *llk);
+
+/* ---------------------------------------------------- conditioning sets */
+/* Conditioning sets on the device (replaces findNearestPoints,
+ * include/nearest_neighbor.h:76-148, over blocks 1..bc-1 as called at
+ * src/test_Xvecchia_batch.cpp:368-390): block i >= 1 takes the cs points of
+ * blocks 0..i-1 nearest to (cx[i], cy[i]), in the reference's selection
+ * order including its tie order; block 0 takes points 0..cs-1.  Host
+ * buffers in and out. */
+int bv_knn(const double *x, const double *y, int n, int bc, int cs,
+           const int *batchNumAccum, const double *cx, const double *cy,
+           int *knn_idx, int device);
+
+/* ------------------------------------------------------- host layout */
+/* The driver's setup on the host (src/test_Xvecchia_batch.cpp:240-352):
+ * classic Vecchia when n < 2*bc, else k-means (random_initializer + Lloyd
+ * kmean_par with `epochs` epochs), random centroid order (srand(42)),
+ * reorderIndex, firstbatch, cluster_combine, cluster_to_batch.
+ * Outputs are caller-allocated with capacity nclusters (= n < 2*bc ? n : bc)
+ * for batchNum / cx / cy, nclusters+1 for batchNumAccum, n for
+ * x_new / y_new / obs_new.  *bc_out receives batchCount. */
+int bv_layout_build(const double *x, const double *y, const double *obs,
+                    int n, int bc, int cs, int seed, int epochs, int threads,
+                    int *batchNum, int *batchNumAccum, double *x_new,
+                    double *y_new, double *obs_new, double *cx, double *cy,
+                    int *bc_out, int *first_cluster_count);
+
+/* The same steps from a given clustering (labels[n], centroids cx/cy[k]). */
+int bv_layout_from_clusters(const double *x, const double *y,
+                            const double *obs, int n, int k,
+                            const int *labels, const double *ccx,
+                            const double *ccy, int cs, int *batchNum,
+                            int *batchNumAccum, double *x_new, double *y_new,
+                            double *obs_new, double *cx, double *cy,
+                            int *bc_out, int *first_cluster_count);
+
+/* k-means alone (random_initializer + kmean_par semantics, deterministic,
+ * exact nearest-centroid assignment through a uniform grid). */
+int bv_kmeans(const double *x, const double *y, int n, int k, int seed,
+              int epochs, int threads, int *labels, double *cx, double *cy);
+
+/* GenerateXYLoc (src/ckernel.cpp:43-76): n jittered grid points, glibc
+ * rand() seeded with `seed`, Morton-sorted and quantised to 1/65535. */
+int bv_generate_xy(int n, int seed, double *x, double *y);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BV_H */
