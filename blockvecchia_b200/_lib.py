@@ -49,6 +49,9 @@ EXPORTS = {
                                           _I, _I, _D, _D, _D, _D, _D, _I, _I]),
     "bv_kmeans": (C.c_int, [_D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _I, _D, _D]),
     "bv_generate_xy": (C.c_int, [C.c_int, C.c_int, _D, _D]),
+    "bv_shard_blocks": (C.c_int, [_I, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_ubyte)]),
+    "bv_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "bv_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
 }
 
 
@@ -62,13 +65,14 @@ class BvLayout(C.Structure):
 class BvOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("kernel", C.c_int), ("dist_scale", C.c_double),
                 ("device", C.c_int), ("on_failure", C.c_int), ("print_iter", C.c_int),
-                ("use_graph", C.c_int), ("schedule", C.c_int), ("mixed_tol", C.c_double)]
+                ("use_graph", C.c_int), ("schedule", C.c_int), ("mixed_tol", C.c_double),
+                ("shard_count", C.c_int), ("shard_index", C.c_int)]
 
 
 class BvStatus(C.Structure):
     _fields_ = [("blocks", C.c_int), ("cond_fail", C.c_int), ("schur_fail", C.c_int),
                 ("fp32_fallback", C.c_int), ("nonfinite", C.c_int), ("flags_or", C.c_uint),
-                ("llk", C.c_double), ("device_ms", C.c_double)]
+                ("llk", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double)]
 
 
 class BvError(RuntimeError):

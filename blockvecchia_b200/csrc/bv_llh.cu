@@ -147,6 +147,7 @@ struct bv_handle {
     int n = 0, bc = 0, cs = 0;
     int max_m = 0;
     std::vector<int> batchNum, acc, order;
+    int owned = 0;  // blocks this handle evaluates (all, or its shard)
     // device
     double *d_x = nullptr, *d_y = nullptr, *d_obs = nullptr;
     int *d_acc = nullptr, *d_knn = nullptr, *d_order = nullptr;
@@ -172,7 +173,8 @@ struct bv_handle {
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr;
+    cudaStream_t own_stream = nullptr;  // the handle's stream; `stream` may be a caller's
     // status
     bv_status status{};
     int iterations = 0;
@@ -188,7 +190,9 @@ static void handle_free(bv_handle *h)
     if (h->graph) cudaGraphDestroy(h->graph);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->evk0) cudaEventDestroy(h->evk0);
+    if (h->evk1) cudaEventDestroy(h->evk1);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
     cudaFree(h->d_x);
     cudaFree(h->d_y);
     cudaFree(h->d_obs);
@@ -221,6 +225,35 @@ extern "C" void bv_default_opts(bv_opts *o)
     o->use_graph = 1;
     o->schedule = 0;
     o->mixed_tol = 1e-11;
+    o->shard_count = 1;
+    o->shard_index = 0;
+}
+
+// Cost rank (largest first, ties by index) shared by the schedule and the
+// sharding rule.
+static std::vector<int> cost_order(const int *batchNum, int bc, int cs)
+{
+    std::vector<int> order(bc);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const int ma = batchNum[a] + (a == 0 ? 0 : cs);
+        const int mb = batchNum[b] + (b == 0 ? 0 : cs);
+        return ma > mb;
+    });
+    return order;
+}
+
+extern "C" int bv_shard_blocks(const int *batchNum, int bc, int cs, int shard_count,
+                               int shard_index, unsigned char *mask)
+{
+    if (!batchNum || !mask || bc <= 0 || cs < 0 || shard_count < 1 || shard_index < 0 ||
+        shard_index >= shard_count) {
+        set_error("bv_shard_blocks: invalid argument");
+        return BV_E_INVALID;
+    }
+    const std::vector<int> order = cost_order(batchNum, bc, cs);
+    for (int t = 0; t < bc; ++t) mask[order[t]] = (t % shard_count == shard_index) ? 1 : 0;
+    return BV_OK;
 }
 
 extern "C" const char *bv_last_error(void) { return get_error(); }
@@ -292,7 +325,7 @@ static int plan_launches(bv_handle *h)
     BV_CUDA_TRY(cudaGetDeviceProperties(&prop, h->device));
     int optin = 0;
     BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-    const size_t static_smem = 2048;  // the kernel's static shared arrays, rounded up
+    const size_t static_smem = 4096;  // the kernel's static shared arrays, rounded up
     const size_t avail = (size_t)optin - static_smem;
     const int cap_m = max_m_for_bytes(avail, sizeof(double));
     h->smem_max_m = std::min(cap_m, h->max_m);
@@ -318,15 +351,15 @@ static int plan_launches(bv_handle *h)
     }
     h->launches.clear();
     if (h->opts.schedule == 0) {
-        h->launches.push_back({0, h->bc, h->grid});
+        if (h->owned > 0) h->launches.push_back({0, h->owned, h->grid});
     } else {
         // One launch per size bucket of M (width 8), largest first.
         int b = 0;
-        while (b < h->bc) {
+        while (b < h->owned) {
             const int mb = h->batchNum[h->order[b]] + (h->order[b] == 0 ? 0 : h->cs);
             const int bucket = mb / 8;
             int e = b;
-            while (e < h->bc) {
+            while (e < h->owned) {
                 const int me = h->batchNum[h->order[e]] + (h->order[e] == 0 ? 0 : h->cs);
                 if (me / 8 != bucket) break;
                 ++e;
@@ -335,14 +368,15 @@ static int plan_launches(bv_handle *h)
             b = e;
         }
     }
-    BV_CUDA_TRY(cudaMalloc(&h->d_counters, sizeof(unsigned) * h->launches.size()));
+    BV_CUDA_TRY(cudaMalloc(&h->d_counters, sizeof(unsigned) * std::max<size_t>(1, h->launches.size())));
     return BV_OK;
 }
 
 static int enqueue_eval(bv_handle *h, cudaStream_t s)
 {
     BV_CUDA_TRY(cudaMemcpyAsync(h->d_mp, h->h_mp, sizeof(MaternParams), cudaMemcpyHostToDevice, s));
-    BV_CUDA_TRY(cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned) * h->launches.size(), s));
+    BV_CUDA_TRY(cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned) * std::max<size_t>(1, h->launches.size()), s));
+    BV_CUDA_TRY(cudaEventRecordWithFlags(h->evk0, s, cudaEventRecordExternal));
     if (h->opts.precision == BV_PREC_MIXED) {
         int rc = mixed_enqueue(h->mixed, s);
         if (rc) return rc;
@@ -372,6 +406,7 @@ static int enqueue_eval(bv_handle *h, cudaStream_t s)
             BV_CUDA_TRY(cudaGetLastError());
         }
     }
+    BV_CUDA_TRY(cudaEventRecordWithFlags(h->evk1, s, cudaEventRecordExternal));
     reduce_kernel<<<1, kReduceThreads, 0, s>>>(h->d_block_llk, h->d_block_status, h->bc, h->d_res);
     BV_CUDA_TRY(cudaGetLastError());
     BV_CUDA_TRY(cudaMemcpyAsync(h->h_res, h->d_res, sizeof(EvalResult), cudaMemcpyDeviceToHost, s));
@@ -436,18 +471,29 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
     h->max_m = 1;
     for (int b = 0; b < h->bc; ++b)
         h->max_m = std::max(h->max_m, h->batchNum[b] + (b == 0 ? 0 : h->cs));
-    // Largest blocks first (longest-processing-time order), ties by index.
-    h->order.resize(h->bc);
-    std::iota(h->order.begin(), h->order.end(), 0);
-    std::stable_sort(h->order.begin(), h->order.end(), [&](int a, int b) {
-        const int ma = h->batchNum[a] + (a == 0 ? 0 : h->cs);
-        const int mb = h->batchNum[b] + (b == 0 ? 0 : h->cs);
-        return ma > mb;
-    });
+    // Largest blocks first (longest-processing-time order), ties by index;
+    // with sharding, every shard_count-th block of that order.
+    if (h->opts.shard_count < 1 || h->opts.shard_index < 0 ||
+        h->opts.shard_index >= h->opts.shard_count) {
+        set_error("bv_create: shard_index %d outside [0, %d)", h->opts.shard_index,
+                  h->opts.shard_count);
+        handle_free(h);
+        return BV_E_INVALID;
+    }
+    {
+        const std::vector<int> all = cost_order(L->batchNum, L->bc, L->cs);
+        h->order.clear();
+        for (int t = 0; t < h->bc; ++t)
+            if (t % h->opts.shard_count == h->opts.shard_index) h->order.push_back(all[t]);
+    }
+    h->owned = (int)h->order.size();
 
-    BV_CUDA_H(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    BV_CUDA_H(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
     BV_CUDA_H(cudaEventCreate(&h->ev0));
     BV_CUDA_H(cudaEventCreate(&h->ev1));
+    BV_CUDA_H(cudaEventCreate(&h->evk0));
+    BV_CUDA_H(cudaEventCreate(&h->evk1));
     const size_t n = h->n, bc = h->bc, cs = h->cs;
     BV_CUDA_H(cudaMalloc(&h->d_x, n * sizeof(double)));
     BV_CUDA_H(cudaMalloc(&h->d_y, n * sizeof(double)));
@@ -465,7 +511,12 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
     BV_CUDA_H(cudaMemcpy(h->d_y, L->y, n * sizeof(double), cudaMemcpyHostToDevice));
     BV_CUDA_H(cudaMemcpy(h->d_obs, L->obs, n * sizeof(double), cudaMemcpyHostToDevice));
     BV_CUDA_H(cudaMemcpy(h->d_acc, L->batchNumAccum, (bc + 1) * sizeof(int), cudaMemcpyHostToDevice));
-    BV_CUDA_H(cudaMemcpy(h->d_order, h->order.data(), bc * sizeof(int), cudaMemcpyHostToDevice));
+    if (h->owned > 0)
+        BV_CUDA_H(cudaMemcpy(h->d_order, h->order.data(), h->owned * sizeof(int),
+                             cudaMemcpyHostToDevice));
+    // Blocks outside this handle's shard contribute exact zeros.
+    BV_CUDA_H(cudaMemset(h->d_block_llk, 0, bc * sizeof(double)));
+    BV_CUDA_H(cudaMemset(h->d_block_status, 0, bc * sizeof(unsigned)));
     if (cs > 0) {
         if (L->knn_idx) {
             BV_CUDA_H(cudaMemcpy(h->d_knn, L->knn_idx, bc * cs * sizeof(int), cudaMemcpyHostToDevice));
@@ -558,11 +609,12 @@ static int eval_locked(bv_handle *h, const double *theta, double *llk)
     }
     BV_CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
     BV_CUDA_TRY(cudaStreamSynchronize(h->stream));
-    float ms = 0.f;
+    float ms = 0.f, kms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    cudaEventElapsedTime(&kms, h->evk0, h->evk1);
     const EvalResult r = *h->h_res;
     bv_status &s = h->status;
-    s.blocks = r.blocks;
+    s.blocks = h->owned;
     s.cond_fail = r.cond_fail;
     s.schur_fail = r.schur_fail;
     s.fp32_fallback = r.fallback;
@@ -570,6 +622,7 @@ static int eval_locked(bv_handle *h, const double *theta, double *llk)
     s.flags_or = r.flags_or;
     s.llk = r.llk;
     s.device_ms = ms;
+    s.kernel_ms = kms;
     double v = r.llk;
     const bool failed = (r.cond_fail + r.schur_fail + r.nonfinite) > 0 || !std::isfinite(v);
     if (failed && h->opts.on_failure == BV_FAIL_NEGINF) v = -HUGE_VAL;
@@ -660,3 +713,18 @@ extern "C" int bv_get_status(bv_handle *h, bv_status *st)
 }
 
 extern "C" int bv_iterations(bv_handle *h) { return h ? h->iterations : 0; }
+
+extern "C" int bv_set_stream(bv_handle *h, void *stream)
+{
+    if (!h) return BV_E_INVALID;
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    return BV_OK;
+}
+
+extern "C" int bv_get_stream(bv_handle *h, void **stream)
+{
+    if (!h || !stream) return BV_E_INVALID;
+    *stream = (void *)h->stream;
+    return BV_OK;
+}

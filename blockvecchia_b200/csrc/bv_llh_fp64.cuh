@@ -22,13 +22,20 @@
 //
 // Packed storage: column j of the (M+1)-row lower triangle starts at
 // off(j) = j*Mp - j*(j+1)/2, Mp = M+1; element (i, j), i >= j, is at off(j)+i.
+//
+// Schedule (512 threads): Matern generation with four independent entries in
+// flight per lane; then per 16-wide panel p, warp 0 factors the diagonal
+// block while warps 1..15 apply panel p-1 to the columns beyond panel p
+// (one panel of look-ahead), all warps solve the panel rows, and all warps
+// bring panel p+1's columns up to date.  The rank-16 updates run on the FP64
+// tensor cores (mma.sync m8n8k4 f64).
 #pragma once
 
 #include "bv_matern.cuh"
 
 namespace bv {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kNB = 16;  // panel width of the blocked Cholesky
 
@@ -57,17 +64,80 @@ __host__ __device__ inline size_t block_doubles(int M) { return 2 * (size_t)M + 
 
 __device__ __forceinline__ int poff(int j, int Mp) { return j * Mp - ((j * (j + 1)) >> 1); }
 
+// Shared scratch of the kernel besides the block itself.
+struct alignas(16) BlockShared {
+    double L[kNB][kNB + 1];  // factored diagonal block of the current panel
+    double Lt[kNB][kNB];     // its transpose: Lt[q][c] = L_(c,q), column q contiguous
+    double inv[kNB];         // 1 / L_jj of the current panel (0: failed pivot)
+    double red[2][kWarps];
+    unsigned status;
+    int task;
+};
+
+// ---------------------------------------------------------------------------
+// Matern generation.
+// ---------------------------------------------------------------------------
+
+// Lower triangle of rows 0..M-1 with columns paired (q, M-1-q) so each pair
+// holds M+1 entries; warp w takes pairs w, w+16, ...; a lane computes four
+// entries of a pair at a time.
+__device__ __forceinline__ void generate(double *A, const double *X, const double *Y, int M,
+                                         const MaternParams &mp)
+{
+    const int Mp = M + 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int half = (M + 1) >> 1;
+    for (int q = warp; q < half; q += kWarps) {
+        const int jb = M - 1 - q;          // partner column
+        const int na = M - q;              // rows q..M-1 of column q
+        const int nt = (jb == q) ? na : M + 1;
+        const int oa = poff(q, Mp), ob = poff(jb, Mp);
+        const double xq = X[q], yq = Y[q], xb = X[jb], yb = Y[jb];
+        for (int r0 = lane; r0 < nt; r0 += 128) {
+            double v[4];
+            int dst[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int rr = r0 + 32 * u;
+                dst[u] = -1;
+                v[u] = 0.0;
+                if (rr < nt) {
+                    int i;
+                    double xj, yj;
+                    if (rr < na) {
+                        i = q + rr;
+                        xj = xq;
+                        yj = yq;
+                        dst[u] = oa + i;
+                    } else {
+                        i = jb + (rr - na);
+                        xj = xb;
+                        yj = yb;
+                        dst[u] = ob + i;
+                    }
+                    v[u] = matern(X[i], Y[i], xj, yj, mp);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (dst[u] >= 0) A[dst[u]] = v[u];
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Panel factorization pieces.
 // ---------------------------------------------------------------------------
 
 // Factor the kb x kb diagonal block at k0 with warp 0.  Lane r owns row k0+r.
-// A non-positive or NaN pivot is kept on the diagonal and its column is
-// zeroed below (the block is then reported; its log-determinant skips the
-// pivot, as core_Xlogdet does).  s_inv receives 1/L_jj (0 for a failed
-// pivot).  Returns a status mask in lane 0.
+// Per pivot: the owner's value is broadcast, every lane takes one rsqrt, the
+// pivot column is scaled and broadcast by shuffles, and the block's remaining
+// columns take a rank-1 update.  A non-positive or NaN pivot is kept on the
+// diagonal and its column is zeroed below (the block is then reported; its
+// log-determinant skips the pivot, as core_Xlogdet does).  The factor also
+// goes to sh.L and 1/L_jj to sh.inv (0 for a failed pivot).
 __device__ __forceinline__ unsigned factor_diag(double *A, int Mp, int k0, int kb, int mc,
-                                                double *s_inv)
+                                                BlockShared &sh)
 {
     const int lane = threadIdx.x & 31;
     double v[kNB];
@@ -79,39 +149,45 @@ __device__ __forceinline__ unsigned factor_diag(double *A, int Mp, int k0, int k
     for (int q = 0; q < kNB; ++q) {
         if (q < kb) {
             const double piv = __shfl_sync(0xffffffffu, v[q], q);
-            double d, inv;
-            if (piv > 0.0) {
-                d = sqrt(piv);
-                inv = 1.0 / d;
-            } else {
-                d = piv;
-                inv = 0.0;
-                st |= (k0 + q < mc) ? 1u : 2u;
-            }
+            const bool ok = piv > 0.0;
+            const double inv = ok ? rsqrt(piv) : 0.0;
+            if (!ok) st |= (k0 + q < mc) ? 1u : 2u;
             if (lane == q) {
-                v[q] = d;
-                s_inv[q] = inv;
+                v[q] = ok ? piv * inv : piv;
+                sh.inv[q] = inv;
             } else if (lane > q) {
                 v[q] *= inv;
             }
-            const double lq = v[q];
+            const double lq = (lane > q) ? v[q] : 0.0;
 #pragma unroll
             for (int c = q + 1; c < kNB; ++c) {
                 const double lc = __shfl_sync(0xffffffffu, lq, c);
-                if (c <= lane && c < kb) v[c] = fma(-lq, lc, v[c]);
+                if (c <= lane) v[c] = fma(-lq, lc, v[c]);
             }
         }
     }
     if (lane < kb) {
 #pragma unroll
-        for (int c = 0; c < kNB; ++c)
-            if (c <= lane && c < kb) A[poff(k0 + c, Mp) + k0 + lane] = v[c];
+        for (int c = 0; c < kNB; ++c) {
+            if (c <= lane && c < kb) {
+                A[poff(k0 + c, Mp) + k0 + lane] = v[c];
+                sh.L[lane][c] = v[c];
+            }
+        }
+    }
+    if (lane < kNB) {
+#pragma unroll
+        for (int c = 0; c < kNB; ++c) sh.Lt[c][lane] = (c < lane && lane < kb) ? v[c] : 0.0;
     }
     return st;
 }
 
-// Rows i in [k0+kb, Mp): A(i, k0:k0+kb) <- A(i, k0:k0+kb) L_kk^-T.
-__device__ __forceinline__ void panel_trsm(double *A, int Mp, int k0, int kb, const double *s_inv)
+// Rows i in [k0+kb, Mp): A(i, k0:k0+kb) <- A(i, k0:k0+kb) L_kk^-T
+// (forward substitution against the factored diagonal block).  Column q of
+// L_kk is read per stage as eight 16-byte broadcasts; a compiler fence keeps
+// the stages' loads from being hoisted into registers all at once.
+__device__ __forceinline__ void panel_trsm(double *A, int Mp, int k0, int kb,
+                                           const BlockShared &sh)
 {
     int cof[kNB];
 #pragma unroll
@@ -123,10 +199,17 @@ __device__ __forceinline__ void panel_trsm(double *A, int Mp, int k0, int kb, co
 #pragma unroll
         for (int q = 0; q < kNB; ++q) {
             if (q < kb) {
-                w[q] *= s_inv[q];
+                asm volatile("" ::: "memory");
+                double2 col[kNB / 2];
+                const double2 *src = reinterpret_cast<const double2 *>(sh.Lt[q]);
 #pragma unroll
-                for (int c = q + 1; c < kNB; ++c)
-                    if (c < kb) w[c] = fma(-w[q], A[cof[q] + k0 + c], w[c]);
+                for (int h = 0; h < kNB / 2; ++h) col[h] = src[h];
+                w[q] *= sh.inv[q];
+#pragma unroll
+                for (int c = q + 1; c < kNB; ++c) {
+                    const double l = (c & 1) ? col[c >> 1].y : col[c >> 1].x;
+                    w[c] = fma(-w[q], l, w[c]);
+                }
             }
         }
 #pragma unroll
@@ -135,64 +218,191 @@ __device__ __forceinline__ void panel_trsm(double *A, int Mp, int k0, int kb, co
     }
 }
 
-// Trailing update of rows [c0, Mp) x cols [c0, Mc), lower part, with the
-// panel columns k0..k0+kb-1.  Each warp owns 32 x 32 tiles; lane (lr, lc) =
-// (lane & 7, lane >> 3) holds rows i0 + lr + 8r (r < 4), cols j0 + lc + 4c
-// (c < 8), so every shared load is a broadcast over at most 8 consecutive
-// doubles.
-__device__ __forceinline__ void trailing_update(double *A, int Mp, int Mc, int k0, int kb)
+__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b)
 {
-    const int c0 = k0 + kb;
-    const int nrow = Mp - c0, ncol = Mc - c0;
-    if (nrow <= 0 || ncol <= 0) return;
-    const int TR = (nrow + 31) >> 5, TC = (ncol + 31) >> 5;
-    // Lower tiles: tr >= tc.  Count = sum_{tc < TC} (TR - tc).
-    const int ntiles = TC * TR - (TC * (TC - 1)) / 2;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int lr = lane & 7, lc = lane >> 3;
-    for (int t = warp; t < ntiles; t += kWarps) {
-        int tc = 0, rem = t;
-        while (rem >= TR - tc) {
-            rem -= TR - tc;
-            ++tc;
-        }
-        const int tr = tc + rem;
-        const int i0 = c0 + (tr << 5), j0 = c0 + (tc << 5);
-        double acc[4][8];
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(c0), "+d"(c1)
+        : "d"(a), "d"(b));
+}
+
+// One (8*NI) x (8*NJ) tile at (i0, j0) of A -= P_I P_J^T, P = panel columns
+// k0..k0+kb-1, rows limited to < Mp and columns to < ce, lower part only.
+// Fragments (m8n8k4, .row.col): lane l holds A[l>>2][l&3], B[l&3][l>>2] and
+// C[l>>2][2(l&3)+{0,1}].
+template <int NI, int NJ, int KB>
+__device__ __forceinline__ void mma_tile(double *A, int Mp, int k0, int kb_rt, int i0, int j0,
+                                         int ce)
+{
+    const int kb = KB > 0 ? KB : kb_rt;
+    const int lane = threadIdx.x & 31;
+    const int r8 = lane >> 2, c4 = lane & 3;
+    double acc[NI][NJ][2];
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+    for (int mi = 0; mi < NI; ++mi)
 #pragma unroll
-            for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
-        for (int kk = 0; kk < kb; ++kk) {
-            const int o = poff(k0 + kk, Mp);
-            double a[4], b[8];
+        for (int nj = 0; nj < NJ; ++nj) acc[mi][nj][0] = acc[mi][nj][1] = 0.0;
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int i = i0 + lr + 8 * r;
-                a[r] = (i < Mp) ? A[o + i] : 0.0;
-            }
+    for (int kk = 0; kk < (KB > 0 ? KB : kNB); kk += 4) {
+        if (KB == 0 && kk >= kb) break;
+        const bool kval = kk + c4 < kb;
+        const int o = poff(k0 + (kval ? kk + c4 : 0), Mp);
+        double a[NI], b[NJ];
 #pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const int j = j0 + lc + 4 * c;
-                b[c] = (j < Mc) ? A[o + j] : 0.0;
-            }
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int c = 0; c < 8; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        for (int mi = 0; mi < NI; ++mi) {
+            const int i = i0 + 8 * mi + r8;
+            a[mi] = (kval && i < Mp) ? A[o + i] : 0.0;
         }
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int j = j0 + lc + 4 * c;
-            if (j < Mc) {
+        for (int nj = 0; nj < NJ; ++nj) {
+            const int j = j0 + 8 * nj + r8;
+            b[nj] = (kval && j < ce) ? A[o + j] : 0.0;
+        }
+#pragma unroll
+        for (int mi = 0; mi < NI; ++mi)
+#pragma unroll
+            for (int nj = 0; nj < NJ; ++nj) dmma_8x8x4(acc[mi][nj][0], acc[mi][nj][1], a[mi], b[nj]);
+    }
+#pragma unroll
+    for (int nj = 0; nj < NJ; ++nj) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int j = j0 + 8 * nj + 2 * c4 + e;
+            if (j < ce) {
                 const int o = poff(j, Mp);
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int i = i0 + lr + 8 * r;
-                    if (i < Mp && i >= j) A[o + i] -= acc[r][c];
+                for (int mi = 0; mi < NI; ++mi) {
+                    const int i = i0 + 8 * mi + r8;
+                    if (i < Mp && i >= j) A[o + i] -= acc[mi][nj][e];
                 }
             }
         }
+    }
+}
+
+// Rows [cb, Mp) x cols [cb, ce) (lower part) with panel k0..k0+kb-1, by warps
+// [w0, w0+nw), in tiles of 32 rows x (8*NJ) columns.
+// skip_sp0: leave the warps of sub-partition 0 (ids = 0 mod 4) out, so warp
+// 0's diagonal factorization does not queue behind their tensor-core work.
+template <int NJ>
+__device__ __forceinline__ void update_cols(double *A, int Mp, int k0, int kb, int cb, int ce,
+                                            bool skip_sp0)
+{
+    constexpr int TW = 8 * NJ;
+    const int nrow = Mp - cb, ncol = ce - cb;
+    if (nrow <= 0 || ncol <= 0) return;
+    const int wid = threadIdx.x >> 5;
+    int warp, nw;
+    if (skip_sp0) {
+        if ((wid & 3) == 0) return;
+        warp = wid - (wid >> 2) - 1;
+        nw = kWarps - kWarps / 4;
+    } else {
+        warp = wid;
+        nw = kWarps;
+    }
+    const int TR = (nrow + 31) >> 5, TC = (ncol + TW - 1) / TW;
+    // Enumerate lower tiles (tc, tr >= first row tile reaching column tile tc).
+    int t = 0;
+    for (int tc = 0; tc < TC; ++tc) {
+        const int j0 = cb + tc * TW;
+        const int tr0 = (j0 - cb) >> 5;
+        for (int tr = tr0; tr < TR; ++tr, ++t) {
+            if (t % nw != warp) continue;
+            if (kb == kNB)
+                mma_tile<4, NJ, kNB>(A, Mp, k0, kb, cb + (tr << 5), j0, ce);
+            else
+                mma_tile<4, NJ, 0>(A, Mp, k0, kb, cb + (tr << 5), j0, ce);
+        }
+    }
+}
+
+// Blocked right-looking Cholesky of the first M columns of the packed
+// (M+1)-row system with one panel of look-ahead.
+__device__ __forceinline__ void cholesky_lookahead(double *A, int M, int mc, BlockShared &sh)
+{
+    const int Mp = M + 1;
+    const int P = (M + kNB - 1) / kNB;
+    const int tid = threadIdx.x;
+    for (int p = 0; p < P; ++p) {
+        const int k0 = p * kNB, kb = min(kNB, M - k0);
+        const int n0 = k0 + kb;           // first column after panel p
+        const int n1 = min(M, n0 + kNB);  // end of panel p+1
+        if (tid < 32) {
+            const unsigned st = factor_diag(A, Mp, k0, kb, mc, sh);
+            if (tid == 0 && st) sh.status |= st;
+        } else if (p > 0) {
+            // Deferred update with panel p-1 of the columns beyond panel p
+            // (warps outside sub-partition 0).
+            update_cols<2>(A, Mp, k0 - kNB, kNB, n0, M, true);
+        }
+        __syncthreads();
+        panel_trsm(A, Mp, k0, kb, sh);
+        __syncthreads();
+        if (n0 < M) {
+            // Look-ahead: panel p+1's columns with panel p.
+            update_cols<2>(A, Mp, k0, kb, n0, n1, false);
+            __syncthreads();
+        }
+    }
+}
+
+// One block, with its matrix at A (shared memory or the global slab).
+__device__ __forceinline__ void process_block(const LlhArgs &a, const MaternParams &mp, int b,
+                                              double *X, double *Y, double *A, BlockShared &sh)
+{
+    const int tid = threadIdx.x;
+    const int off = a.acc[b];
+    const int bs = a.acc[b + 1] - off;
+    const int mc = (b == 0) ? 0 : a.cs;
+    const int M = mc + bs, Mp = M + 1;
+
+    // Gather: conditioning points by index, then the block's own points;
+    // observations go to row M.
+    const int *kidx = a.knn + (size_t)b * a.cs;
+    for (int t = tid; t < M; t += kThreads) {
+        const int src = (t < mc) ? __ldg(kidx + t) : off + (t - mc);
+        X[t] = __ldg(a.x + src);
+        Y[t] = __ldg(a.y + src);
+        A[poff(t, Mp) + M] = __ldg(a.obs + src);
+    }
+    __syncthreads();
+    generate(A, X, Y, M, mp);
+    __syncthreads();
+
+    // Cholesky of the first M columns; row M rides along as the
+    // forward-substitution right-hand side.
+    cholesky_lookahead(A, M, mc, sh);
+
+    // log det of the conditional factor (positive pivots only, as
+    // core_Xlogdet) and |u|^2 from row M.
+    double ld = 0.0, qf = 0.0;
+    for (int j = mc + tid; j < M; j += kThreads) {
+        const double d = A[poff(j, Mp) + j];
+        if (d > 0) ld += log(d * d);
+        const double u = A[poff(j, Mp) + M];
+        qf = fma(u, u, qf);
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        ld += __shfl_xor_sync(0xffffffffu, ld, s);
+        qf += __shfl_xor_sync(0xffffffffu, qf, s);
+    }
+    if ((tid & 31) == 0) {
+        sh.red[0][tid >> 5] = ld;
+        sh.red[1][tid >> 5] = qf;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double Ls = 0.0, Qs = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            Ls += sh.red[0][w];
+            Qs += sh.red[1][w];
+        }
+        const double v = -(Qs + Ls + (double)bs * a.log2pi) * 0.5;
+        unsigned st = sh.status;
+        if (!isfinite(v)) st |= 8u;
+        a.block_llk[b] = v;
+        a.block_status[b] = st;
     }
 }
 
@@ -203,125 +413,31 @@ __device__ __forceinline__ void trailing_update(double *A, int Mp, int Mc, int k
 __global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel(LlhArgs a)
 {
     extern __shared__ __align__(16) double smem[];
-    __shared__ int s_task;
-    __shared__ double s_inv[kNB];
-    __shared__ unsigned s_status;
-    __shared__ double s_red[2][kWarps];
+    __shared__ BlockShared sh;
 
     const MaternParams mp = *a.mp;
     const int tid = threadIdx.x;
 
     for (;;) {
-        if (tid == 0) s_task = (int)atomicAdd(a.work_counter, 1u) + a.task_begin;
+        if (tid == 0) sh.task = (int)atomicAdd(a.work_counter, 1u) + a.task_begin;
         __syncthreads();
-        const int task = s_task;
+        const int task = sh.task;
         if (task >= a.task_end) break;
         const int b = a.order[task];
-        const int off = a.acc[b];
-        const int bs = a.acc[b + 1] - off;
-        const int mc = (b == 0) ? 0 : a.cs;
-        const int M = mc + bs, Mp = M + 1;
+        const int bs = a.acc[b + 1] - a.acc[b];
+        const int M = ((b == 0) ? 0 : a.cs) + bs;
+        if (tid == 0) sh.status = 0u;
 
         if (bs == 0) {  // empty block: contributes -(0 + 0 + 0) / 2
             if (tid == 0) {
                 a.block_llk[b] = -0.0;
                 a.block_status[b] = 0u;
             }
-            __syncthreads();
-            continue;
-        }
-
-        double *X, *Y, *A;
-        if (M <= a.smem_max_m) {
-            X = smem;
-            Y = smem + M;
-            A = smem + 2 * M;
+        } else if (M <= a.smem_max_m) {
+            process_block(a, mp, b, smem, smem + M, smem + 2 * M, sh);
         } else {
             double *slab = a.gslab + (size_t)blockIdx.x * a.gslab_stride;
-            X = slab;
-            Y = slab + M;
-            A = slab + 2 * M;
-        }
-        if (tid == 0) s_status = 0u;
-
-        // Gather: conditioning points by index, then the block's own points;
-        // observations go to row M.
-        const int *kidx = a.knn + (size_t)b * a.cs;
-        for (int t = tid; t < M; t += kThreads) {
-            const int src = (t < mc) ? __ldg(kidx + t) : off + (t - mc);
-            X[t] = __ldg(a.x + src);
-            Y[t] = __ldg(a.y + src);
-            A[poff(t, Mp) + M] = __ldg(a.obs + src);
-        }
-        __syncthreads();
-
-        // Matern lower triangle, columns paired (q, M-1-q) so every pair holds
-        // M+1 entries.
-        {
-            const int half = (M + 1) >> 1;
-            const int total = half * (M + 1);
-            for (int e = tid; e < total; e += kThreads) {
-                const int q = e / (M + 1);
-                const int rr = e - q * (M + 1);
-                int i, j;
-                if (rr < M - q) {
-                    j = q;
-                    i = q + rr;
-                } else {
-                    j = M - 1 - q;
-                    if (j == q) continue;  // odd M: middle column counted once
-                    i = j + (rr - (M - q));
-                }
-                A[poff(j, Mp) + i] = matern(X[i], Y[i], X[j], Y[j], mp);
-            }
-        }
-        __syncthreads();
-
-        // Blocked right-looking Cholesky of the first M columns; row M rides
-        // along as the forward-substitution right-hand side.
-        for (int k0 = 0; k0 < M; k0 += kNB) {
-            const int kb = min(kNB, M - k0);
-            if (tid < 32) {
-                const unsigned st = factor_diag(A, Mp, k0, kb, mc, s_inv);
-                if (tid == 0 && st) s_status |= st;
-            }
-            __syncthreads();
-            panel_trsm(A, Mp, k0, kb, s_inv);
-            __syncthreads();
-            trailing_update(A, Mp, M, k0, kb);
-            __syncthreads();
-        }
-
-        // log det of the conditional factor (positive pivots only, as
-        // core_Xlogdet) and |u|^2 from row M.
-        double ld = 0.0, qf = 0.0;
-        for (int j = mc + tid; j < M; j += kThreads) {
-            const double d = A[poff(j, Mp) + j];
-            if (d > 0) ld += log(d * d);
-            const double u = A[poff(j, Mp) + M];
-            qf = fma(u, u, qf);
-        }
-#pragma unroll
-        for (int s = 16; s > 0; s >>= 1) {
-            ld += __shfl_xor_sync(0xffffffffu, ld, s);
-            qf += __shfl_xor_sync(0xffffffffu, qf, s);
-        }
-        if ((tid & 31) == 0) {
-            s_red[0][tid >> 5] = ld;
-            s_red[1][tid >> 5] = qf;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            double L = 0.0, Q = 0.0;
-            for (int w = 0; w < kWarps; ++w) {
-                L += s_red[0][w];
-                Q += s_red[1][w];
-            }
-            const double v = -(Q + L + (double)bs * a.log2pi) * 0.5;
-            unsigned st = s_status;
-            if (!isfinite(v)) st |= 8u;
-            a.block_llk[b] = v;
-            a.block_status[b] = st;
+            process_block(a, mp, b, slab, slab + M, slab + 2 * M, sh);
         }
         __syncthreads();
     }

@@ -124,7 +124,7 @@ __device__ __forceinline__ double besselk_scaled_trap(double nu, double x)
     return h * sum;
 }
 
-__device__ __forceinline__ double besselk(double nu, double x)
+static __device__ __noinline__ double besselk(double nu, double x)
 {
     nu = fabs(nu);
     if (x > 2.0) return besselk_scaled_trap(nu, x) * exp(-x);
@@ -139,6 +139,12 @@ __device__ __forceinline__ double besselk(double nu, double x)
         k1 = k2;
     }
     return k0;
+}
+
+// General nu: con * r^nu * K_nu(r) (kept out of line; it is long and rare).
+static __device__ __noinline__ double matern_general(double r, double con, double nu)
+{
+    return con * pow(r, nu) * besselk(nu, r);
 }
 
 // Scaled distance r of core_dcmg for two points.
@@ -164,7 +170,7 @@ __device__ __forceinline__ double matern_from_r(double r, const MaternParams &p)
     case kNuFiveHalves:
         return p.sigma2 * (fma(r, r * (1.0 / 3.0), 1.0 + r) * exp(-r));
     default:
-        return p.con * pow(r, p.nu) * besselk(p.nu, r);
+        return matern_general(r, p.con, p.nu);
     }
 }
 

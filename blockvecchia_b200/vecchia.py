@@ -140,7 +140,7 @@ class LlhData:
     def __init__(self, layout: Layout, precision: str = "fp64", kernel: int = 1,
                  dist_scale: float = 1.0, device: int = 0, on_failure: str = "neginf",
                  print_iter: bool = False, use_graph: bool = True, schedule: str = "persistent",
-                 mixed_tol: float = 1e-11):
+                 mixed_tol: float = 1e-11, shard_count: int = 1, shard_index: int = 0):
         L = layout.normalized()
         self.layout = L
         o = _lib.BvOpts()
@@ -154,6 +154,8 @@ class LlhData:
         o.use_graph = int(bool(use_graph))
         o.schedule = _SCHED[schedule]
         o.mixed_tol = float(mixed_tol)
+        o.shard_count = int(shard_count)
+        o.shard_index = int(shard_index)
         null_i = C.POINTER(C.c_int)()
         null_d = C.POINTER(C.c_double)()
         self._l = _lib.BvLayout(L.n, L.bc, L.cs, ip(L.batchNum), ip(L.batchNumAccum), dp(L.x),
@@ -218,6 +220,27 @@ class LlhData:
     @property
     def iterations(self) -> int:
         return lib().bv_iterations(self._h)
+
+    def set_stream(self, stream: int) -> None:
+        """Launch subsequent evaluations on `stream` (a cudaStream_t as an
+        integer; 0 restores the handle's own stream)."""
+        check(lib().bv_set_stream(self._h, C.c_void_p(int(stream)) if stream else None))
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t (as an integer) the handle launches on."""
+        p = C.c_void_p()
+        check(lib().bv_get_stream(self._h, C.byref(p)))
+        return int(p.value or 0)
+
+
+def shard_blocks(batchNum, cs: int, shard_count: int, shard_index: int) -> np.ndarray:
+    """Boolean mask of the blocks one shard evaluates (bv_shard_blocks)."""
+    bn = np.ascontiguousarray(batchNum, dtype=np.int32)
+    mask = np.zeros(len(bn), dtype=np.uint8)
+    check(lib().bv_shard_blocks(ip(bn), len(bn), int(cs), int(shard_count), int(shard_index),
+                                mask.ctypes.data_as(C.POINTER(C.c_ubyte))))
+    return mask.astype(bool)
 
 
 def llh_Xvecchia_batch(n: int, localtheta, grad, data: LlhData) -> float:

@@ -76,6 +76,10 @@ typedef struct {
     int schedule;      /* 0 persistent work queue (default), 1 one launch per
                           size bucket (the comparison baseline)               */
     double mixed_tol;  /* mixed path: refinement residual tolerance           */
+    int shard_count;   /* > 1: this handle evaluates only its shard of the
+                          blocks (bv_shard_blocks); partial log-likelihoods of
+                          all shards sum to the full one                      */
+    int shard_index;   /* 0 .. shard_count-1                                  */
 } bv_opts;
 
 typedef struct {
@@ -87,6 +91,7 @@ typedef struct {
     unsigned flags_or;   /* OR of BV_ST_* over all blocks                    */
     double llk;          /* last log-likelihood (before the failure policy)  */
     double device_ms;    /* device time of the last evaluation               */
+    double kernel_ms;    /* of which the fused per-block kernel(s)            */
 } bv_status;
 
 typedef struct bv_handle bv_handle;
@@ -118,6 +123,14 @@ int bv_llh_eval(bv_handle *h, const double *theta, double *llk);
 int bv_block_llk(bv_handle *h, double *out, int count);
 
 int bv_get_status(bv_handle *h, bv_status *st);
+
+/* The CUDA stream (cudaStream_t) the handle launches on, for callers that
+ * time evaluations with their own events or order work after them. */
+int bv_get_stream(bv_handle *h, void **stream);
+
+/* Launch subsequent evaluations on `stream` (a cudaStream_t of the handle's
+ * device; NULL restores the handle's own stream). */
+int bv_set_stream(bv_handle *h, void *stream);
 int bv_iterations(bv_handle *h);
 const char *bv_last_error(void);
 
@@ -128,6 +141,14 @@ const char *bv_last_error(void);
 int bv_llh_host(bv_handle *h, const double *x, const double *y,
                 const double *obs, const int *knn_idx, const double *theta,
                 double *llk);
+
+/* Block sharding for multi-GPU evaluation (blocks are independent given
+ * theta; the reference runs them all on one GPU).  Blocks are ranked by cost
+ * (M^3 with M = cs + bs, block 0 unconditioned), largest first, ties by
+ * index, and dealt round-robin to shard_count shards.  mask[b] = 1 for the
+ * blocks of shard shard_index.  Host only. */
+int bv_shard_blocks(const int *batchNum, int bc, int cs, int shard_count,
+                    int shard_index, unsigned char *mask);
 
 /* ---------------------------------------------------- conditioning sets */
 /* Conditioning sets on the device (replaces findNearestPoints,

@@ -216,6 +216,70 @@ int bvo_knn_block(const double *x, const double *y, int prefix,
     return k;
 }
 
+static double bvo_select_kth(double *a, int n, int k) /* k-th smallest, 0-based */
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        double piv = a[lo + (hi - lo) / 2];
+        int i = lo, j = hi;
+        while (i <= j) {
+            while (a[i] < piv) ++i;
+            while (a[j] > piv) --j;
+            if (i <= j) {
+                double t = a[i]; a[i] = a[j]; a[j] = t;
+                ++i; --j;
+            }
+        }
+        if (k <= j) hi = j;
+        else if (k >= i) lo = i;
+        else return a[k];
+    }
+    return a[k];
+}
+
+int bvo_knn_block_fast(const double *x, const double *y, int prefix,
+                       double cx, double cy, int k, int *out_idx)
+{
+    if (prefix <= 0 || k <= 0) return 0;
+    if (k > prefix) k = prefix;
+    double *dist = (double *)malloc(sizeof(double) * (size_t)prefix);
+    double *tmp = (double *)malloc(sizeof(double) * (size_t)prefix);
+    for (int p = 0; p < prefix; ++p) {
+        double dx = x[p] - cx;
+        double dy = y[p] - cy;
+        dist[p] = sqrt(fma(dx, dx, dy * dy));
+        tmp[p] = dist[p];
+    }
+    double dk = bvo_select_kth(tmp, prefix, k - 1);
+    int m = 0;
+    for (int p = 0; p < prefix; ++p)
+        if (dist[p] <= dk) tmp[m++] = (double)p; /* S in index order */
+    int *sidx = (int *)malloc(sizeof(int) * (size_t)m);
+    int *pos = (int *)malloc(sizeof(int) * (size_t)m);
+    for (int e = 0; e < m; ++e) {
+        sidx[e] = (int)tmp[e];
+        pos[e] = sidx[e];
+    }
+    for (int t = 0; t < k; ++t) {
+        int best = -1, occ = -1;
+        for (int e = 0; e < m; ++e) {
+            if (pos[e] < 0) continue;
+            if (best < 0 || dist[sidx[e]] < dist[sidx[best]] ||
+                (dist[sidx[e]] == dist[sidx[best]] && pos[e] < pos[best]))
+                best = e;
+            if (pos[e] == t) occ = e;
+        }
+        out_idx[t] = sidx[best];
+        if (occ >= 0 && occ != best) pos[occ] = pos[best];
+        pos[best] = -1;
+    }
+    free(dist);
+    free(tmp);
+    free(sidx);
+    free(pos);
+    return k;
+}
+
 void bvo_knn_all(const double *x, const double *y, int bc, int cs,
                  const int *batchNumAccum, const double *cx, const double *cy,
                  int *knn_idx)

@@ -49,6 +49,14 @@ void bvo_matern(double *A, int m, int n,
 int bvo_knn_block(const double *x, const double *y, int prefix,
                   double cx, double cy, int k, int *out_idx);
 
+/* Same result as bvo_knn_block in O(prefix + k*|S|): the candidate set
+ * S = {p : key(p) <= k-th smallest key} is found by quickselect, then the
+ * reference's selection sort is replayed on S alone (members outside S
+ * never win a round and never change the relative positions of S members).
+ * Used to prepare conditioning sets for large CPU samples. */
+int bvo_knn_block_fast(const double *x, const double *y, int prefix,
+                       double cx, double cy, int k, int *out_idx);
+
 /* All conditioning sets: block 0 takes points 0..cs-1
  * (src/test_Xvecchia_batch.cpp:360-366), block i >= 1 calls bvo_knn_block
  * with prefix = batchNumAccum[i] and centroid (cx[i], cy[i])

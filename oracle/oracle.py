@@ -61,6 +61,8 @@ def lib():
         L.bvo_knn_block.restype = C.c_int
         L.bvo_knn_block.argtypes = [_D, _D, C.c_int, C.c_double, C.c_double, C.c_int, _I]
         L.bvo_knn_all.argtypes = [_D, _D, C.c_int, C.c_int, _I, _D, _D, _I]
+        L.bvo_knn_block_fast.restype = C.c_int
+        L.bvo_knn_block_fast.argtypes = [_D, _D, C.c_int, C.c_double, C.c_double, C.c_int, _I]
         L.bvo_llh.restype = C.c_double
         L.bvo_llh.argtypes = [C.POINTER(Problem), _D, C.POINTER(BlockResult), C.c_int]
         L.bvo_llh_blas.restype = C.c_double
@@ -115,6 +117,14 @@ def knn_block(x, y, prefix, cx, cy, k):
     y = np.ascontiguousarray(y, dtype=np.float64)
     out = np.zeros(max(k, 1), dtype=np.int32)
     got = lib().bvo_knn_block(_dp(x), _dp(y), int(prefix), float(cx), float(cy), int(k), _ip(out))
+    return out[:got]
+
+
+def knn_block_fast(x, y, prefix, cx, cy, k):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    out = np.zeros(max(k, 1), dtype=np.int32)
+    got = lib().bvo_knn_block_fast(_dp(x), _dp(y), int(prefix), float(cx), float(cy), int(k), _ip(out))
     return out[:got]
 
 

@@ -1,0 +1,60 @@
+"""Device conditioning sets (bv_knn) against findNearestPoints: indices and
+their order must be bit-exact, ties included."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def test_golden_layout_knn(bvlib, golden_layout):
+    g = golden_layout
+    L = bvlib.Layout(g["batchNum"], g["batchNumAccum"], g["x_new"], g["y_new"], g["obs_new"], 60,
+                     g["cx"], g["cy"])
+    assert np.array_equal(bvlib.knn(L), g["knn"])
+
+
+def test_ties_on_a_grid(bvlib):
+    """A regular grid has many exactly equal distances; the selection-sort
+    order of the reference must be reproduced."""
+    g = golden("knn_ties.npz")
+    X, Y = g["x"], g["y"]
+    for t in range(3):
+        c = g[f"c_{t}"]
+        # Two blocks: block 0 = all 900 grid points, block 1 = one extra point.
+        x = np.concatenate([X, [0.5]])
+        y = np.concatenate([Y, [0.5]])
+        L = bvlib.Layout(np.array([900, 1], np.int32), np.array([0, 900, 901], np.int32), x, y,
+                         np.zeros(901), 60, np.array([0.0, c[0]]), np.array([0.0, c[1]]))
+        got = bvlib.knn(L)[60:]
+        assert np.array_equal(got, g[f"idx_{t}"]), t
+
+
+@pytest.mark.parametrize("n,bc,cs,seed", [(4000, 300, 60, 0), (20000, 1500, 100, 1),
+                                          (6000, 400, 300, 2), (3000, 1600, 40, 3)])
+def test_generated_vs_oracle(bvlib, oracle, n, bc, cs, seed):
+    x, y = bvlib.generate_xy(n, seed)  # 16-bit quantised: exact ties occur
+    L = bvlib.build_layout(x, y, np.zeros(n), bc, cs, seed=seed, epochs=10)
+    got = bvlib.knn(L)
+    ref = oracle.knn_all(L.x, L.y, cs, L.batchNumAccum, L.cx, L.cy)
+    assert np.array_equal(got, ref)
+
+
+def test_duplicates_and_uniform(bvlib, oracle):
+    """Duplicated locations (exact ties on both coordinates) and plain uniform
+    points."""
+    rng = np.random.default_rng(7)
+    base = rng.random((1500, 2))
+    pts = np.concatenate([base, base[:700]])  # 700 exact duplicates
+    perm = rng.permutation(len(pts))
+    x, y = pts[perm, 0].copy(), pts[perm, 1].copy()
+    L = bvlib.build_layout(x, y, np.zeros(len(x)), 150, 50, seed=1, epochs=5)
+    assert np.array_equal(bvlib.knn(L), oracle.knn_all(L.x, L.y, 50, L.batchNumAccum, L.cx, L.cy))
+
+
+def test_knn_rejects_short_prefix(bvlib):
+    L = bvlib.Layout(np.array([5, 5], np.int32), np.array([0, 5, 10], np.int32), np.random.rand(10),
+                     np.random.rand(10), np.zeros(10), 8, np.zeros(2), np.zeros(2))
+    with pytest.raises(bvlib.BvError):
+        bvlib.knn(L)

@@ -1,0 +1,179 @@
+"""FP64 device log-likelihood (libbv_b200.so) against the CPU oracle.
+
+Tolerance: 1e-10 relative on the total log-likelihood (the FP64-path parity
+bound), and 1e-7 relative per block contribution (max(1, |value|)-scaled):
+a single block whose conditioning covariance has condition number ~1e13
+(smooth kernels, dense points) carries kappa * eps rounding in its
+conditional variance, while the total stays within 1e-10."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-10
+THETAS = [(1.5, 0.1, 0.5), (1.0, 0.08, 1.5), (1.0, 0.05, 2.5), (1.0, 0.1, 0.8), (0.7, 0.03, 1.2)]
+
+
+def _layout(bv, g):
+    return bv.Layout(g["batchNum"], g["batchNumAccum"], g["x_new"], g["y_new"], g["obs_new"], 60,
+                     g["cx"], g["cy"], g["knn"].copy())
+
+
+def _blocks(oracle, L, th):
+    P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, L.knn_idx, L.cs)
+    v, pb = oracle.llh(P, th, per_block=True)
+    per = -(pb[:, 1] ** 2 + pb[:, 0] + L.batchNum * np.log(2 * 3.141592653589793)) * 0.5
+    return v, per
+
+
+def _check(bv, oracle, L, thetas=THETAS, **kw):
+    with bv.LlhData(L, **kw) as D:
+        for th in thetas:
+            v = D(th)
+            ref, per = _blocks(oracle, L, th)
+            assert abs(v - ref) <= REL * abs(ref), (th, v, ref)
+            bl = D.block_llk()
+            assert np.all(np.abs(bl - per) <= 1e-7 * np.maximum(1.0, np.abs(per))), th
+            st = D.status()
+            assert st["cond_fail"] == 0 and st["schur_fail"] == 0
+
+
+def test_golden_layout(bvlib, oracle, golden_layout):
+    """The reference-built layout and conditioning sets, five smoothness values."""
+    L = _layout(bvlib, golden_layout)
+    g = golden("llh_2000_150_60.npz")
+    with bvlib.LlhData(L) as D:
+        for t in range(4):
+            v = D(g[f"theta_{t}"])
+            ref = float(g[f"llk_{t}"])
+            assert abs(v - ref) <= REL * abs(ref), t
+    _check(bvlib, oracle, L)
+
+
+def _gen(bv, n, bc, cs, seed=0, epochs=10):
+    x, y = bv.generate_xy(n, seed)
+    z = np.random.default_rng(seed).standard_normal(n)
+    L = bv.build_layout(x, y, z, bc, cs, seed=seed, epochs=epochs)
+    L.knn_idx = bv.knn(L)
+    return L
+
+
+@pytest.mark.parametrize("n,bc,cs", [(3000, 200, 100), (1500, 100, 300), (2000, 1200, 30)])
+def test_generated_layouts(bvlib, oracle, n, bc, cs):
+    """Shared-memory blocks, global-slab blocks (cs = 300) and classic Vecchia."""
+    _check(bvlib, oracle, _gen(bvlib, n, bc, cs), thetas=THETAS[:4])
+
+
+def test_dist_scale(bvlib, oracle, golden_layout):
+    L = _layout(bvlib, golden_layout)
+    P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, L.knn_idx, 60, 2.0)
+    with bvlib.LlhData(L, dist_scale=2.0) as D:
+        for th in THETAS[:3]:
+            ref = oracle.llh(P, th)
+            assert abs(D(th) - ref) <= REL * abs(ref)
+
+
+def test_no_conditioning_cs0(bvlib, oracle):
+    """cs = 0: every block independent (the reference skips the conditioning
+    step, include/llh_Xvecchia_batch.h:152,239,278)."""
+    rng = np.random.default_rng(5)
+    bn = np.array([7, 1, 4, 0, 12], dtype=np.int32)
+    acc = np.concatenate([[0], np.cumsum(bn)]).astype(np.int32)
+    n = int(acc[-1])
+    L = bvlib.Layout(bn, acc, rng.random(n), rng.random(n), rng.standard_normal(n), 0,
+                     knn_idx=np.zeros(0, dtype=np.int32))
+    _check(bvlib, oracle, L, thetas=THETAS[:2])
+
+
+def test_edge_blocks(bvlib, oracle):
+    """Empty blocks, one-point blocks, a single block (block 0 only)."""
+    rng = np.random.default_rng(11)
+    cs = 20
+    bn = np.array([25, 1, 0, 3, 1, 0, 9], dtype=np.int32)
+    acc = np.concatenate([[0], np.cumsum(bn)]).astype(np.int32)
+    n = int(acc[-1])
+    x, y, z = rng.random(n), rng.random(n), rng.standard_normal(n)
+    knn = np.zeros(len(bn) * cs, dtype=np.int32)
+    knn[:cs] = np.arange(cs)
+    for b in range(1, len(bn)):
+        knn[b * cs:(b + 1) * cs] = rng.choice(acc[b], cs, replace=False)
+    L = bvlib.Layout(bn, acc, x, y, z, cs, knn_idx=knn)
+    _check(bvlib, oracle, L, thetas=THETAS[:3])
+    L1 = bvlib.Layout(np.array([30], np.int32), np.array([0, 30], np.int32), x[:30], y[:30], z[:30],
+                      cs, knn_idx=np.arange(cs, dtype=np.int32))
+    _check(bvlib, oracle, L1, thetas=THETAS[:2])
+
+
+def test_graph_schedule_and_determinism(bvlib, golden_layout):
+    """Graph vs stream launch, persistent vs per-bucket launches: identical bits."""
+    L = _layout(bvlib, golden_layout)
+    th = (1.0, 0.08, 1.5)
+    vals = []
+    for kw in [dict(), dict(use_graph=False), dict(schedule="bucketed")]:
+        with bvlib.LlhData(L, **kw) as D:
+            a, b = D(th), D(th)
+            assert a == b
+            vals.append(a)
+    assert vals[0] == vals[1] == vals[2]
+
+
+def test_shards_sum_to_total(bvlib, golden_layout):
+    L = _layout(bvlib, golden_layout)
+    th = (1.0, 0.05, 2.5)
+    with bvlib.LlhData(L) as D:
+        full = D(th)
+    parts = []
+    for r in range(3):
+        with bvlib.LlhData(L, shard_count=3, shard_index=r) as D:
+            parts.append(D(th))
+    assert abs(sum(parts) - full) <= 1e-13 * abs(full)
+
+
+def test_failure_policy(bvlib):
+    """Duplicated locations make Sigma22 singular: the default policy returns
+    -inf and reports the block; 'continue' returns a finite value."""
+    rng = np.random.default_rng(2)
+    cs = 10
+    x = np.concatenate([np.repeat(rng.random(5), 2), rng.random(20)])
+    y = np.concatenate([np.repeat(rng.random(5), 2), rng.random(20)])
+    n = len(x)
+    bn = np.array([10, 10, 10], dtype=np.int32)
+    acc = np.array([0, 10, 20, 30], dtype=np.int32)
+    knn = np.concatenate([np.arange(10), np.arange(10), np.arange(10)]).astype(np.int32)
+    L = bvlib.Layout(bn, acc, x, y, rng.standard_normal(n), cs, knn_idx=knn)
+    with bvlib.LlhData(L) as D:
+        v = D((1.0, 0.1, 0.5))
+        st = D.status()
+    assert v == -np.inf and st["cond_fail"] >= 1
+    with bvlib.LlhData(L, on_failure="continue") as D:
+        v = D((1.0, 0.1, 0.5))
+    assert np.isfinite(v)
+
+
+def test_nlopt_signature_and_host_entry(bvlib, golden_layout):
+    L = _layout(bvlib, golden_layout)
+    th = np.array([1.0, 0.08, 1.5])
+    with bvlib.LlhData(L) as D:
+        a = bvlib.llh_Xvecchia_batch(3, th, None, D)
+        b = D.eval_host(L.obs, th, x=L.x, y=L.y, knn_idx=L.knn_idx)
+        c = D(th)
+        assert a == b == c
+        assert D.iterations == 3
+        z2 = L.obs * 0.5
+        d = D.eval_host(z2, th)
+        e = D(th)
+        assert d == e and d != c
+
+
+def test_invalid_inputs_rejected(bvlib, golden_layout):
+    L = _layout(bvlib, golden_layout)
+    bad = L.knn_idx.copy()
+    bad[60 * 5] = int(L.batchNumAccum[5])  # a point that is not earlier than block 5
+    Lb = bvlib.Layout(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, 60, knn_idx=bad)
+    with pytest.raises(bvlib.BvError):
+        bvlib.LlhData(Lb)
+    with bvlib.LlhData(L) as D:
+        with pytest.raises(bvlib.BvError):
+            D((1.0, -0.1, 0.5))

@@ -1,0 +1,139 @@
+"""The CPU oracle against mpmath and the reference's own code (golden
+fixtures made by tests/golden/make_golden.py, and oracle/_ref live when it is
+built)."""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+mpmath = pytest.importorskip("mpmath")
+
+
+NUS = [0.01, 0.1, 0.25, 1 / 3, 0.5, 0.5000001, 0.8, 1.0, 1.2, 1.5, 1.77, 2.0, 2.5, 2.99, 3.0]
+XS = [1e-8, 1e-4, 1e-2, 0.1, 0.5, 1.0, 1.5, 1.999, 2.0, 2.001, 2.5, 3, 5, 10, 30, 100, 300, 700]
+
+
+def test_besselk_vs_mpmath(oracle):
+    """K_nu(x) to 1e-13 relative over nu in [0.01, 3], x in [1e-8, 700]."""
+    mpmath.mp.dps = 40
+    worst = 0.0
+    for nu in NUS:
+        for x in XS:
+            t = float(mpmath.besselk(nu, x))
+            v = oracle.besselk(nu, x)
+            worst = max(worst, abs(v - t) / abs(t))
+    assert worst < 1e-13, worst
+
+
+def test_besselk_half_integer_closed_forms(oracle):
+    for x in [0.01, 0.3, 1.0, 1.9, 2.1, 7.0, 40.0]:
+        k12 = math.sqrt(math.pi / (2 * x)) * math.exp(-x)
+        assert abs(oracle.besselk(0.5, x) - k12) <= 1e-14 * k12
+        k32 = k12 * (1 + 1 / x)
+        assert abs(oracle.besselk(1.5, x) - k32) <= 1e-14 * k32
+        k52 = k12 * (1 + 3 / x + 3 / x ** 2)
+        assert abs(oracle.besselk(2.5, x) - k52) <= 1e-14 * k52
+
+
+def test_matern_golden_bitexact(oracle):
+    """bvo_matern == the reference's core_dcmg, bit for bit."""
+    g = golden("core_dcmg.npz")
+    x = golden("generate_xy.npz")["x_2000_0"]
+    y = golden("generate_xy.npz")["y_2000_0"]
+    for t in range(4):
+        i, j, th = g[f"i_{t}"], g[f"j_{t}"], g[f"theta_{t}"]
+        A = oracle.matern(x[i], y[i], x[j], y[j], th)
+        assert np.array_equal(A, g[f"A_{t}"]), t
+
+
+def test_knn_golden_bitexact(oracle, golden_layout):
+    """bvo_knn_block == findNearestPoints (selection order) for every block."""
+    g = golden_layout
+    knn = oracle.knn_all(g["x_new"], g["y_new"], 60, g["batchNumAccum"], g["cx"], g["cy"])
+    assert np.array_equal(knn, g["knn"])
+
+
+def test_knn_ties_golden(oracle):
+    g = golden("knn_ties.npz")
+    for t in range(3):
+        c = g[f"c_{t}"]
+        got = oracle.knn_block(g["x"], g["y"], 900, c[0], c[1], 60)
+        assert np.array_equal(got, g[f"idx_{t}"]), t
+
+
+def test_llh_golden(oracle, golden_layout):
+    g = golden_layout
+    L = golden("llh_2000_150_60.npz")
+    P = oracle.OracleProblem(g["batchNum"], g["batchNumAccum"], g["x_new"], g["y_new"],
+                             g["obs_new"], g["knn"], 60)
+    for t in range(4):
+        v = oracle.llh(P, L[f"theta_{t}"])
+        assert v == float(L[f"llk_{t}"]), t
+
+
+def test_llh_exact_two_blocks(oracle):
+    """Block 1 conditioning on every point of block 0 makes block Vecchia the
+    exact Gaussian log-density; check against a dense Cholesky (scipy)."""
+    scipy_stats = pytest.importorskip("scipy.stats")
+    rng = np.random.default_rng(3)
+    cs, bs1 = 40, 13
+    n = cs + bs1
+    x, y = rng.random(n), rng.random(n)
+    z = rng.standard_normal(n)
+    bn = np.array([cs, bs1], dtype=np.int32)
+    acc = np.array([0, cs, n], dtype=np.int32)
+    knn = np.concatenate([np.arange(cs), rng.permutation(cs)]).astype(np.int32)
+    P = oracle.OracleProblem(bn, acc, x, y, z, knn, cs)
+    for th in [(1.5, 0.3, 0.5), (0.9, 0.2, 1.5), (1.2, 0.15, 2.5), (1.0, 0.25, 0.8)]:
+        Sigma = oracle.matern(x, y, x, y, th)
+        exact = scipy_stats.multivariate_normal(mean=np.zeros(n), cov=Sigma).logpdf(z)
+        v = oracle.llh(P, th)
+        assert abs(v - exact) <= 1e-10 * abs(exact), (th, v, exact)
+
+
+def test_llh_matches_blas_variant(oracle, golden_layout):
+    """The OpenBLAS-backed CPU baseline computes the same quantity."""
+    g = golden_layout
+    P = oracle.OracleProblem(g["batchNum"], g["batchNumAccum"], g["x_new"], g["y_new"],
+                             g["obs_new"], g["knn"], 60)
+    th = (1.0, 0.08, 1.5)
+    a = oracle.llh(P, th)
+    try:
+        b = oracle.llh_blas(P, th)
+    except RuntimeError:
+        pytest.skip("scipy OpenBLAS not found")
+    assert abs(a - b) <= 1e-10 * abs(a)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_live_pins_against_reference(ref, seed):
+    """Random cases through the reference's own core_dcmg / findNearestPoints."""
+    rng = np.random.default_rng(100 + seed)
+    x, y = ref.ref_generate_xy(3000, seed)
+    th = [(1.5, 0.1, 0.5), (1.0, 0.07, 1.3), (0.5, 0.2, 2.7)][seed]
+    i = rng.choice(3000, 50, replace=False)
+    j = rng.choice(3000, 35, replace=False)
+    assert np.array_equal(ref.matern(x[i], y[i], x[j], y[j], th),
+                          ref.ref_core_dcmg(x[i], y[i], x[j], y[j], th))
+    for prefix, k in [(400, 100), (3000, 300), (1500, 37)]:
+        cx, cy = rng.random(2)
+        assert np.array_equal(ref.knn_block(x, y, prefix, cx, cy, k),
+                              ref.ref_find_nearest(x, y, prefix, cx, cy, k))
+
+
+def test_knn_fast_matches_selection_sort(oracle):
+    """The O(P + k|S|) replay gives the selection sort's output, ties included."""
+    g = golden("knn_ties.npz")
+    for t in range(3):
+        c = g[f"c_{t}"]
+        assert np.array_equal(oracle.knn_block_fast(g["x"], g["y"], 900, c[0], c[1], 60),
+                              g[f"idx_{t}"])
+    rng = np.random.default_rng(4)
+    x = np.round(rng.random(5000), 3)  # coarse grid: many ties
+    y = np.round(rng.random(5000), 3)
+    for prefix, k in [(5000, 200), (900, 300), (4000, 17)]:
+        cx, cy = np.round(rng.random(2), 3)
+        assert np.array_equal(oracle.knn_block_fast(x, y, prefix, cx, cy, k),
+                              oracle.knn_block(x, y, prefix, cx, cy, k))
