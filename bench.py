@@ -39,9 +39,18 @@ METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] \
     if os.path.exists(os.path.join(ROOT, "BASELINE.json")) else \
     "loglik evals/s n=1M cs=200, mixed vs FP64 at rel err<=1e-8; serve p50/p99 ms"
 
-WORKLOAD = dict(name="n=1M uniform, nu=2.5 sigma2=1 range=0.05, bc=100k, cs=200",
-                n=1_000_000, bc=100_000, cs=200, sigma2=1.0, range=0.05, nu=2.5, seed=0,
-                kmeans_epochs=50, rff_features=1024)
+WORKLOADS = {
+    # The headline configuration.
+    "c3": dict(name="n=1M uniform, nu=2.5 sigma2=1 range=0.05, bc=100k, cs=200",
+               n=1_000_000, bc=100_000, cs=200, sigma2=1.0, range=0.05, nu=2.5, seed=0,
+               kmeans_epochs=50, rff_features=1024),
+    # Same kernel shape (cs = 200, blocks of ~10 points) on 4,000 blocks: the
+    # case ncu captures with full sections.
+    "c3-small": dict(name="n=40k uniform, nu=2.5 sigma2=1 range=0.05, bc=4k, cs=200 (profiling case)",
+                     n=40_000, bc=4_000, cs=200, sigma2=1.0, range=0.05, nu=2.5, seed=0,
+                     kmeans_epochs=50, rff_features=1024),
+}
+WORKLOAD = WORKLOADS["c3"]
 
 
 # ----------------------------------------------------------------- workload
@@ -456,7 +465,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", choices=sorted(WORKLOADS), default="c3",
+                    help="c3: the headline workload (default); c3-small: profiling case")
     args = ap.parse_args()
+    global WORKLOAD
+    WORKLOAD = WORKLOADS[args.case]
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

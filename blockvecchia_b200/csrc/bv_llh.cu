@@ -372,11 +372,22 @@ static int plan_launches(bv_handle *h)
     return BV_OK;
 }
 
+// Timing events around the fused kernel: inside a captured graph they must be
+// external event-record nodes; on a plain stream, ordinary records.
+static cudaError_t record_timing(cudaEvent_t ev, cudaStream_t s)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cs);
+    if (e != cudaSuccess) return e;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal)
+                                               : cudaEventRecord(ev, s);
+}
+
 static int enqueue_eval(bv_handle *h, cudaStream_t s)
 {
     BV_CUDA_TRY(cudaMemcpyAsync(h->d_mp, h->h_mp, sizeof(MaternParams), cudaMemcpyHostToDevice, s));
     BV_CUDA_TRY(cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned) * std::max<size_t>(1, h->launches.size()), s));
-    BV_CUDA_TRY(cudaEventRecordWithFlags(h->evk0, s, cudaEventRecordExternal));
+    BV_CUDA_TRY(record_timing(h->evk0, s));
     if (h->opts.precision == BV_PREC_MIXED) {
         int rc = mixed_enqueue(h->mixed, s);
         if (rc) return rc;
@@ -406,7 +417,7 @@ static int enqueue_eval(bv_handle *h, cudaStream_t s)
             BV_CUDA_TRY(cudaGetLastError());
         }
     }
-    BV_CUDA_TRY(cudaEventRecordWithFlags(h->evk1, s, cudaEventRecordExternal));
+    BV_CUDA_TRY(record_timing(h->evk1, s));
     reduce_kernel<<<1, kReduceThreads, 0, s>>>(h->d_block_llk, h->d_block_status, h->bc, h->d_res);
     BV_CUDA_TRY(cudaGetLastError());
     BV_CUDA_TRY(cudaMemcpyAsync(h->h_res, h->d_res, sizeof(EvalResult), cudaMemcpyDeviceToHost, s));
