@@ -52,6 +52,9 @@ EXPORTS = {
     "bv_shard_blocks": (C.c_int, [_I, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_ubyte)]),
     "bv_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "bv_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bv_llh_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_int, C.c_int, C.c_int, _D, C.c_double, C.c_void_p,
+                                 C.POINTER(C.c_uint), C.c_void_p]),
 }
 
 

@@ -739,3 +739,189 @@ extern "C" int bv_get_stream(bv_handle *h, void **stream)
     *stream = (void *)h->stream;
     return BV_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.  For callers that cannot allocate device
+// memory themselves or let a library do it (their allocator owns the GPU,
+// or the host application manages every buffer).  Its working memory is one
+// fixed array inside this library; see bv_llh_noalloc in include/bv.h.
+// ---------------------------------------------------------------------------
+
+namespace bv {
+
+constexpr size_t kNoAllocBlocks = BV_NOALLOC_MAX_BLOCKS;
+// Byte offsets of the regions carved out of the array (each 256-aligned).
+constexpr size_t kNaLlk = 0;                                         // double[kNoAllocBlocks]
+constexpr size_t kNaStatus = kNaLlk + kNoAllocBlocks * 8;            // unsigned[kNoAllocBlocks]
+constexpr size_t kNaOrder = kNaStatus + kNoAllocBlocks * 4;          // int[kNoAllocBlocks]
+constexpr size_t kNaCounter = kNaOrder + kNoAllocBlocks * 4;         // unsigned work counter
+constexpr size_t kNaCheck = kNaCounter + 256;                        // int[4] validation
+constexpr size_t kNaParams = kNaCheck + 256;                         // MaternParams
+constexpr size_t kNaResult = kNaParams + 256;                        // EvalResult
+constexpr size_t kNaBytes = kNaResult + 256;
+
+// The working memory of bv_llh_noalloc: every device that loads the library
+// holds it until exit.  Host code must use the address from
+// cudaGetSymbolAddress, never the name.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+static std::mutex g_noalloc_mu;
+static unsigned char *g_noalloc_ptr[64] = {nullptr};
+static int g_noalloc_smem_max_m[64] = {0};
+
+// Validation of a caller's layout on the device: offsets non-decreasing and
+// ending at n, every block fits in shared memory, every conditioning index of
+// block b >= 1 lies in [0, batchNumAccum[b]).  check[0] = first bad block + 1
+// (offsets/indices), check[1] = largest M.
+__global__ void noalloc_check_kernel(const int *acc, const int *knn, int n, int bc, int cs,
+                                     int *check, int *order)
+{
+    const int stride = gridDim.x * blockDim.x;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < bc; b += stride) {
+        order[b] = b;
+        const int a0 = acc[b], a1 = acc[b + 1];
+        bool ok = a0 >= 0 && a1 >= a0 && a1 <= n && (b + 1 < bc || a1 == n) && (b > 0 || a0 == 0);
+        const int M = (a1 - a0) + (b == 0 ? 0 : cs);
+        atomicMax(&check[1], M);
+        if (ok && b > 0 && cs > 0) {
+            const int *k = knn + (size_t)b * cs;
+            for (int t = 0; t < cs; ++t)
+                if (k[t] < 0 || k[t] >= a0) {
+                    ok = false;
+                    break;
+                }
+        }
+        if (!ok) atomicCAS(&check[0], 0, b + 1);
+    }
+}
+
+}  // namespace bv
+
+extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *obs,
+                              const int *batchNumAccum, const int *knn_idx, int n, int bc, int cs,
+                              const double *theta, double dist_scale, double *llk_out,
+                              unsigned *status_flags, void *stream)
+{
+    using namespace bv;
+    if (!x || !y || !obs || !batchNumAccum || !theta || !llk_out || n <= 0 || bc <= 0 || cs < 0 ||
+        (cs > 0 && !knn_idx)) {
+        set_error("bv_llh_noalloc: null pointer or non-positive size");
+        return BV_E_INVALID;
+    }
+    if ((size_t)bc > kNoAllocBlocks) {
+        set_error("bv_llh_noalloc: %d blocks exceed the fixed maximum of %d", bc,
+                  (int)kNoAllocBlocks);
+        return BV_E_TOOLARGE;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0;
+    BV_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        set_error("bv_llh_noalloc: device ordinal %d unsupported", dev);
+        return BV_E_NODEVICE;
+    }
+    unsigned char *base = nullptr;
+    int smem_max_m = 0;
+    {
+        // Once per device, with that device current: the array's device
+        // address and the fused kernel's shared-memory size.
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p) {
+                set_error("bv_llh_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+                return BV_E_CUDA;
+            }
+            int optin = 0;
+            BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            g_noalloc_smem_max_m[dev] = max_m_for_bytes((size_t)optin - 4096, sizeof(double));
+            g_noalloc_ptr[dev] = (unsigned char *)p;
+        }
+        base = g_noalloc_ptr[dev];
+        smem_max_m = g_noalloc_smem_max_m[dev];
+    }
+    int *check = reinterpret_cast<int *>(base + kNaCheck);
+    int *order = reinterpret_cast<int *>(base + kNaOrder);
+    unsigned *counter = reinterpret_cast<unsigned *>(base + kNaCounter);
+    // Validate the layout on the device; read back 8 bytes.
+    BV_CUDA_TRY(cudaMemsetAsync(check, 0, 2 * sizeof(int), s));
+    noalloc_check_kernel<<<(bc + 255) / 256, 256, 0, s>>>(batchNumAccum, knn_idx, n, bc, cs, check,
+                                                          order);
+    BV_CUDA_TRY(cudaGetLastError());
+    int hc[2] = {0, 0};
+    BV_CUDA_TRY(cudaMemcpyAsync(hc, check, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    BV_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hc[0]) {
+        set_error("bv_llh_noalloc: block %d has inconsistent offsets or a conditioning index "
+                  "outside the earlier blocks", hc[0] - 1);
+        return BV_E_INVALID;
+    }
+    if (hc[1] > smem_max_m) {
+        set_error("bv_llh_noalloc: a block needs cs + bs = %d > %d, the largest block one SM's "
+                  "shared memory holds", hc[1], smem_max_m);
+        return BV_E_TOOLARGE;
+    }
+    // Parameters (host-computed as in bv_llh_eval) into the array.
+    const double sigma2 = theta[0], range = theta[1], nu = theta[2];
+    if (!std::isfinite(sigma2) || !(range > 0) || !(nu > 0) || !std::isfinite(range) ||
+        !std::isfinite(nu) || !(dist_scale > 0)) {
+        set_error("bv_llh_noalloc: invalid theta (%g, %g, %g) or dist_scale %g", sigma2, range,
+                  nu, dist_scale);
+        return BV_E_INVALID;
+    }
+    MaternParams mp;
+    double con = std::pow(2.0, nu - 1.0) * std::tgamma(nu);
+    con = 1.0 / con;
+    mp.sigma2 = sigma2;
+    mp.range = range;
+    mp.nu = nu;
+    mp.con = sigma2 * con;
+    mp.dist_scale = dist_scale;
+    mp.scale_is_one = dist_scale == 1.0 ? 1 : 0;
+    mp.nu_kind = (nu == 0.5) ? kNuHalf : (nu == 1.5) ? kNuThreeHalves : (nu == 2.5) ? kNuFiveHalves
+                                                                                  : kNuGeneral;
+    MaternParams *d_mp = reinterpret_cast<MaternParams *>(base + kNaParams);
+    BV_CUDA_TRY(cudaMemcpyAsync(d_mp, &mp, sizeof(mp), cudaMemcpyHostToDevice, s));
+    // The work counter must start at zero; per-block results are fully
+    // overwritten by the kernel.
+    BV_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
+    int sms = 0;
+    BV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // The kernel's dynamic shared-memory limit is a per-function setting that
+    // other callers also set, so it is set for every call.
+    const size_t smem = block_doubles(smem_max_m) * sizeof(double);
+    BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    LlhArgs a;
+    a.x = x;
+    a.y = y;
+    a.obs = obs;
+    a.acc = batchNumAccum;
+    a.knn = knn_idx;
+    a.order = order;
+    a.bc = bc;
+    a.cs = cs;
+    a.smem_max_m = smem_max_m;
+    a.slab_max_m = smem_max_m;
+    a.block_llk = reinterpret_cast<double *>(base + kNaLlk);
+    a.block_status = reinterpret_cast<unsigned *>(base + kNaStatus);
+    a.work_counter = counter;
+    a.gslab = nullptr;  // never used: every block fits in shared memory (checked above)
+    a.gslab_stride = 0;
+    a.log2pi = std::log(2 * 3.141592653589793);
+    a.mp = d_mp;
+    a.task_begin = 0;
+    a.task_end = bc;
+    llh_fp64_kernel<<<sms, kThreads, smem, s>>>(a);
+    BV_CUDA_TRY(cudaGetLastError());
+    EvalResult *d_res = reinterpret_cast<EvalResult *>(base + kNaResult);
+    reduce_kernel<<<1, kReduceThreads, 0, s>>>(a.block_llk, a.block_status, bc, d_res);
+    BV_CUDA_TRY(cudaGetLastError());
+    BV_CUDA_TRY(cudaMemcpyAsync(llk_out, &d_res->llk, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    unsigned flags = 0;
+    BV_CUDA_TRY(cudaMemcpyAsync(&flags, &d_res->flags_or, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    BV_CUDA_TRY(cudaStreamSynchronize(s));
+    if (status_flags) *status_flags = flags;
+    return BV_OK;
+}

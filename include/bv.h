@@ -142,6 +142,32 @@ int bv_llh_host(bv_handle *h, const double *x, const double *y,
                 const double *obs, const int *knn_idx, const double *theta,
                 double *llk);
 
+/* Allocation-free evaluation, for callers that cannot allocate device memory
+ * (an allocator they do not own, a memory pool that forbids extra
+ * cudaMalloc calls, embedding in a host application that manages every
+ * buffer itself).  No counterpart in the reference.  The caller passes
+ * device pointers to the block-ordered locations and observations (x, y,
+ * obs [n]), the block offsets (batchNumAccum [bc+1]) and the conditioning
+ * indices (knn_idx [bc*cs]; block 0 unconditioned), the host parameters
+ * theta = {sigma2, range, nu}, and a device pointer llk_out that receives the
+ * log-likelihood.  The library's working memory for this call is a fixed
+ * 2 MB device array inside the library (every device that loads the library
+ * holds it until exit): at most BV_NOALLOC_MAX_BLOCKS blocks, and every
+ * block must fit in one SM's shared memory (cs + bs <= about 236), else
+ * BV_E_TOOLARGE.  Invalid offsets or indices give BV_E_INVALID.  The first
+ * call on a device looks up that array's device address, so make that first
+ * call before any stream capture.  Every call shares the array: calls that
+ * overlap on the GPU race, so serialise them (one stream, or synchronise).
+ * Runs on `stream` (a cudaStream_t of the current device; NULL = the default
+ * stream) and returns after the evaluation has finished.  Allocates nothing:
+ * no cudaMalloc, cudaFree or allocating library call.  *status_flags (may be
+ * NULL) receives the OR of the blocks' BV_ST_* bits. */
+#define BV_NOALLOC_MAX_BLOCKS 131072
+int bv_llh_noalloc(const double *x, const double *y, const double *obs,
+                   const int *batchNumAccum, const int *knn_idx, int n, int bc,
+                   int cs, const double *theta, double dist_scale,
+                   double *llk_out, unsigned *status_flags, void *stream);
+
 /* Block sharding for multi-GPU evaluation (blocks are independent given
  * theta; the reference runs them all on one GPU).  Blocks are ranked by cost
  * (M^3 with M = cs + bs, block 0 unconditioned), largest first, ties by
