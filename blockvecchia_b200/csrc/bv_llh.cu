@@ -330,8 +330,10 @@ static int plan_launches(bv_handle *h)
     const int cap_m = max_m_for_bytes(avail, sizeof(double));
     h->smem_max_m = std::min(cap_m, h->max_m);
     h->smem_bytes = block_doubles(h->smem_max_m) * sizeof(double);
+    // The cap is per kernel, not per handle: set it to what the device allows
+    // so that handles with different block sizes can coexist.
     BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)h->smem_bytes));
+                                     (int)(block_doubles(cap_m) * sizeof(double))));
     int occ = 0;
     BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, llh_fp64_kernel, kThreads,
                                                               h->smem_bytes));

@@ -177,3 +177,17 @@ def test_invalid_inputs_rejected(bvlib, golden_layout):
     with bvlib.LlhData(L) as D:
         with pytest.raises(bvlib.BvError):
             D((1.0, -0.1, 0.5))
+
+
+def test_handles_with_different_block_sizes_coexist(bvlib, oracle, golden_layout):
+    """A handle with small blocks created after one with large blocks must not
+    shrink the large one's shared-memory allowance."""
+    big = _gen(bvlib, 3000, 200, 180)
+    small = _layout(bvlib, golden_layout)
+    th = (1.0, 0.1, 0.8)
+    with bvlib.LlhData(big) as Db:
+        vb0 = Db(th)
+        with bvlib.LlhData(small) as Ds:
+            Ds(th)
+            vb1 = Db(th)
+    assert vb0 == vb1
