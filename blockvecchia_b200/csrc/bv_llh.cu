@@ -305,6 +305,18 @@ static int validate_layout(const bv_layout *L)
     return BV_OK;
 }
 
+// Static shared memory of the fused kernel plus a margin; the dynamic part
+// gets the rest of the per-block opt-in limit.
+static size_t fused_static_smem()
+{
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, llh_fp64_kernel) != cudaSuccess) {
+        cudaGetLastError();
+        return 16384;
+    }
+    return fa.sharedSizeBytes + 1024;
+}
+
 // Largest M whose block fits in `bytes` of dynamic shared memory.
 static int max_m_for_bytes(size_t bytes, size_t per_double)
 {
@@ -325,8 +337,7 @@ static int plan_launches(bv_handle *h)
     BV_CUDA_TRY(cudaGetDeviceProperties(&prop, h->device));
     int optin = 0;
     BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-    const size_t static_smem = 4096;  // the kernel's static shared arrays, rounded up
-    const size_t avail = (size_t)optin - static_smem;
+    const size_t avail = (size_t)optin - fused_static_smem();
     const int cap_m = max_m_for_bytes(avail, sizeof(double));
     h->smem_max_m = std::min(cap_m, h->max_m);
     h->smem_bytes = block_doubles(h->smem_max_m) * sizeof(double);
@@ -603,6 +614,8 @@ static int fill_params(bv_handle *h, const double *theta)
     p.con = con;
     p.dist_scale = h->opts.dist_scale;
     p.scale_is_one = (h->opts.dist_scale == 1.0) ? 1 : 0;
+    p.inv_range = 1.0 / range;
+    p.inv_ds = 1.0 / h->opts.dist_scale;
     p.nu_kind = (nu == 0.5) ? kNuHalf : (nu == 1.5) ? kNuThreeHalves : (nu == 2.5) ? kNuFiveHalves
                                                                                   : kNuGeneral;
     return BV_OK;
@@ -837,7 +850,7 @@ extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *ob
             }
             int optin = 0;
             BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-            g_noalloc_smem_max_m[dev] = max_m_for_bytes((size_t)optin - 4096, sizeof(double));
+            g_noalloc_smem_max_m[dev] = max_m_for_bytes((size_t)optin - fused_static_smem(), sizeof(double));
             g_noalloc_ptr[dev] = (unsigned char *)p;
         }
         base = g_noalloc_ptr[dev];
@@ -881,6 +894,8 @@ extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *ob
     mp.con = sigma2 * con;
     mp.dist_scale = dist_scale;
     mp.scale_is_one = dist_scale == 1.0 ? 1 : 0;
+    mp.inv_range = 1.0 / range;
+    mp.inv_ds = 1.0 / dist_scale;
     mp.nu_kind = (nu == 0.5) ? kNuHalf : (nu == 1.5) ? kNuThreeHalves : (nu == 2.5) ? kNuFiveHalves
                                                                                   : kNuGeneral;
     MaternParams *d_mp = reinterpret_cast<MaternParams *>(base + kNaParams);

@@ -66,9 +66,10 @@ __device__ __forceinline__ int poff(int j, int Mp) { return j * Mp - ((j * (j + 
 
 // Shared scratch of the kernel besides the block itself.
 struct alignas(16) BlockShared {
-    double L[kNB][kNB + 1];  // factored diagonal block of the current panel
-    double Lt[kNB][kNB];     // its transpose: Lt[q][c] = L_(c,q), column q contiguous
-    double inv[kNB];         // 1 / L_jj of the current panel (0: failed pivot)
+    double L[kNB][kNB];         // factored diagonal block of panel p, L[r][c], 0 above
+    double Lt[kNB][kNB];        // its transpose, Lt[c][r] = L[r][c]: column c contiguous
+    double Lnx[kNB][kNB + 2];   // L(rows of panel p+1, columns of panel p)
+    double inv[kNB];            // 1 / L_jj of panel p (0: failed pivot)
     double red[2][kWarps];
     unsigned status;
     int task;
@@ -129,93 +130,69 @@ __device__ __forceinline__ void generate(double *A, const double *X, const doubl
 // Panel factorization pieces.
 // ---------------------------------------------------------------------------
 
-// Factor the kb x kb diagonal block at k0 with warp 0.  Lane r owns row k0+r.
-// Per pivot: the owner's value is broadcast, every lane takes one rsqrt, the
-// pivot column is scaled and broadcast by shuffles, and the block's remaining
-// columns take a rank-1 update.  A non-positive or NaN pivot is kept on the
-// diagonal and its column is zeroed below (the block is then reported; its
-// log-determinant skips the pivot, as core_Xlogdet does).  The factor also
-// goes to sh.L and 1/L_jj to sh.inv (0 for a failed pivot).
-__device__ __forceinline__ unsigned factor_diag(double *A, int Mp, int k0, int kb, int mc,
-                                                BlockShared &sh)
+// Warp 0: left-looking (Crout) factorization of the kb x kb diagonal block
+// of panel p, with the kb1 rows of panel p+1 solved in the same pass.  Lane r
+// < 16 owns row k0+r of the diagonal block, lane 16+r owns row n0+r (panel
+// p+1); at pivot q every lane forms a_rq - sum_{k<q} L_rk L_qk (row q comes
+// by shuffles from lane q), lane q's value is the pivot, and one rsqrt scales
+// the column.  A non-positive or NaN pivot is kept on the diagonal and its
+// column is zeroed below (the block is reported; its log-determinant skips
+// the pivot, as core_Xlogdet does).  Results: L to A, sh.L (diagonal block)
+// and sh.Lnx (panel p+1 rows), 1/L_jj to sh.inv (0 for a failed pivot).
+__device__ __forceinline__ unsigned factor_diag(double *A, int Mp, int k0, int kb, int n0, int kb1,
+                                                int mc, BlockShared &sh)
 {
     const int lane = threadIdx.x & 31;
+    const bool low = lane < kNB;
+    const int r = low ? lane : lane - kNB;  // row within its 16-row group
+    const bool valid = low ? (r < kb) : (r < kb1);
+    const int row = low ? k0 + r : n0 + r;
     double v[kNB];
 #pragma unroll
     for (int c = 0; c < kNB; ++c)
-        v[c] = (lane < kb && c <= lane && c < kb) ? A[poff(k0 + c, Mp) + k0 + lane] : 0.0;
+        v[c] = (valid && c < kb && (!low || c <= r)) ? A[poff(k0 + c, Mp) + row] : 0.0;
     unsigned st = 0;
 #pragma unroll
     for (int q = 0; q < kNB; ++q) {
         if (q < kb) {
-            const double piv = __shfl_sync(0xffffffffu, v[q], q);
+            // Four independent partial sums keep the dependent chain short.
+            double s4[4] = {v[q], 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < q; ++k) {
+                const double lqk = __shfl_sync(0xffffffffu, v[k], q);
+                s4[k & 3] = fma(-v[k], lqk, s4[k & 3]);
+            }
+            const double s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+            const double piv = __shfl_sync(0xffffffffu, s, q);
             const bool ok = piv > 0.0;
             const double inv = ok ? rsqrt(piv) : 0.0;
             if (!ok) st |= (k0 + q < mc) ? 1u : 2u;
-            if (lane == q) {
+            if (low && r == q) {
                 v[q] = ok ? piv * inv : piv;
                 sh.inv[q] = inv;
-            } else if (lane > q) {
-                v[q] *= inv;
-            }
-            const double lq = (lane > q) ? v[q] : 0.0;
-#pragma unroll
-            for (int c = q + 1; c < kNB; ++c) {
-                const double lc = __shfl_sync(0xffffffffu, lq, c);
-                if (c <= lane) v[c] = fma(-lq, lc, v[c]);
+            } else if (!low || r > q) {
+                v[q] = s * inv;
             }
         }
     }
-    if (lane < kb) {
-#pragma unroll
-        for (int c = 0; c < kNB; ++c) {
-            if (c <= lane && c < kb) {
-                A[poff(k0 + c, Mp) + k0 + lane] = v[c];
-                sh.L[lane][c] = v[c];
-            }
-        }
-    }
-    if (lane < kNB) {
-#pragma unroll
-        for (int c = 0; c < kNB; ++c) sh.Lt[c][lane] = (c < lane && lane < kb) ? v[c] : 0.0;
-    }
-    return st;
-}
-
-// Rows i in [k0+kb, Mp): A(i, k0:k0+kb) <- A(i, k0:k0+kb) L_kk^-T
-// (forward substitution against the factored diagonal block).  Column q of
-// L_kk is read per stage as eight 16-byte broadcasts; a compiler fence keeps
-// the stages' loads from being hoisted into registers all at once.
-__device__ __forceinline__ void panel_trsm(double *A, int Mp, int k0, int kb,
-                                           const BlockShared &sh)
-{
-    int cof[kNB];
-#pragma unroll
-    for (int c = 0; c < kNB; ++c) cof[c] = poff(k0 + (c < kb ? c : 0), Mp);
-    for (int i = k0 + kb + threadIdx.x; i < Mp; i += kThreads) {
-        double w[kNB];
-#pragma unroll
-        for (int c = 0; c < kNB; ++c) w[c] = (c < kb) ? A[cof[c] + i] : 0.0;
-#pragma unroll
-        for (int q = 0; q < kNB; ++q) {
-            if (q < kb) {
-                asm volatile("" ::: "memory");
-                double2 col[kNB / 2];
-                const double2 *src = reinterpret_cast<const double2 *>(sh.Lt[q]);
-#pragma unroll
-                for (int h = 0; h < kNB / 2; ++h) col[h] = src[h];
-                w[q] *= sh.inv[q];
-#pragma unroll
-                for (int c = q + 1; c < kNB; ++c) {
-                    const double l = (c & 1) ? col[c >> 1].y : col[c >> 1].x;
-                    w[c] = fma(-w[q], l, w[c]);
-                }
-            }
-        }
+    if (valid) {
 #pragma unroll
         for (int c = 0; c < kNB; ++c)
-            if (c < kb) A[cof[c] + i] = w[c];
+            if (c < kb && (!low || c <= r)) A[poff(k0 + c, Mp) + row] = v[c];
     }
+    if (low) {
+#pragma unroll
+        for (int c = 0; c < kNB; ++c) {
+            const double l = (c <= r && r < kb) ? v[c] : 0.0;
+            sh.L[r][c] = l;
+            sh.Lt[c][r] = l;
+        }
+        if (r >= kb) sh.inv[r] = 0.0;
+    } else {
+#pragma unroll
+        for (int c = 0; c < kNB; ++c) sh.Lnx[r][c] = (valid && c < kb) ? v[c] : 0.0;
+    }
+    return st;
 }
 
 __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b)
@@ -231,7 +208,7 @@ __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, dou
 // C[l>>2][2(l&3)+{0,1}].
 template <int NI, int NJ, int KB>
 __device__ __forceinline__ void mma_tile(double *A, int Mp, int k0, int kb_rt, int i0, int j0,
-                                         int ce)
+                                         int ce, int excl)
 {
     const int kb = KB > 0 ? KB : kb_rt;
     const int lane = threadIdx.x & 31;
@@ -272,7 +249,7 @@ __device__ __forceinline__ void mma_tile(double *A, int Mp, int k0, int kb_rt, i
 #pragma unroll
                 for (int mi = 0; mi < NI; ++mi) {
                     const int i = i0 + 8 * mi + r8;
-                    if (i < Mp && i >= j) A[o + i] -= acc[mi][nj][e];
+                    if (i < Mp && i >= j && !(i < excl && j < excl)) A[o + i] -= acc[mi][nj][e];
                 }
             }
         }
@@ -283,9 +260,11 @@ __device__ __forceinline__ void mma_tile(double *A, int Mp, int k0, int kb_rt, i
 // [w0, w0+nw), in tiles of 32 rows x (8*NJ) columns.
 // skip_sp0: leave the warps of sub-partition 0 (ids = 0 mod 4) out, so warp
 // 0's diagonal factorization does not queue behind their tensor-core work.
+// Elements with both indices below `excl` are left alone (a diagonal block
+// another warp updates).
 template <int NJ>
 __device__ __forceinline__ void update_cols(double *A, int Mp, int k0, int kb, int cb, int ce,
-                                            bool skip_sp0)
+                                            bool skip_sp0, int excl)
 {
     constexpr int TW = 8 * NJ;
     const int nrow = Mp - cb, ncol = ce - cb;
@@ -309,40 +288,160 @@ __device__ __forceinline__ void update_cols(double *A, int Mp, int k0, int kb, i
         for (int tr = tr0; tr < TR; ++tr, ++t) {
             if (t % nw != warp) continue;
             if (kb == kNB)
-                mma_tile<4, NJ, kNB>(A, Mp, k0, kb, cb + (tr << 5), j0, ce);
+                mma_tile<4, NJ, kNB>(A, Mp, k0, kb, cb + (tr << 5), j0, ce, excl);
             else
-                mma_tile<4, NJ, 0>(A, Mp, k0, kb, cb + (tr << 5), j0, ce);
+                mma_tile<4, NJ, 0>(A, Mp, k0, kb, cb + (tr << 5), j0, ce, excl);
+        }
+    }
+}
+
+// Warp 0: the diagonal block of panel p (rows/cols k0..k0+kb-1, lower part)
+// takes the updates of panels p-2 and p-1, which the bulk updates leave to
+// it (FP64 tensor cores, three 8x8 sub-tiles).
+__device__ __forceinline__ void update_diag_block(double *A, int Mp, int k0, int kb, int p)
+{
+    const int lane = threadIdx.x & 31;
+    const int r8 = lane >> 2, c4 = lane & 3;
+    double acc[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};  // (0,0), (1,0), (1,1)
+    const int qb = p >= 2 ? p - 2 : 0;
+    for (int q = qb; q < p; ++q) {
+#pragma unroll
+        for (int kk = 0; kk < kNB; kk += 4) {
+            const int o = poff(q * kNB + kk + c4, Mp);
+            const int i0 = k0 + r8, i1 = k0 + 8 + r8;
+            const double a0 = (r8 < kb) ? A[o + i0] : 0.0;
+            const double a1 = (8 + r8 < kb) ? A[o + i1] : 0.0;
+            dmma_8x8x4(acc[0][0], acc[0][1], a0, a0);
+            dmma_8x8x4(acc[1][0], acc[1][1], a1, a0);
+            dmma_8x8x4(acc[2][0], acc[2][1], a1, a1);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        const int mi = (t == 0) ? 0 : 1, nj = (t == 2) ? 1 : 0;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int ii = 8 * mi + r8, jj = 8 * nj + 2 * c4 + e;
+            if (ii < kb && jj < kb && ii >= jj) A[poff(k0 + jj, Mp) + k0 + ii] -= acc[t][e];
+        }
+    }
+}
+
+// All warps, 32-row groups of rows [rb, Mp): each lane solves its row of
+// X L_kk^T = A(row, panel p) by forward substitution (backward stable; column
+// q of L_kk read per stage as eight 16-byte broadcasts behind a compiler
+// fence so the 120 factor values are not all hoisted into registers) and
+// stores X as the row's panel-p factor; then the warp updates panel p+1's
+// columns, A(rows, panel p+1) -= X Lnx^T, on the FP64 tensor cores.
+__device__ __forceinline__ void panel_rows_pass(double *A, int Mp, int k0, int kb, int n0, int kb1,
+                                                int rb, const BlockShared &sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int r8 = lane >> 2, c4 = lane & 3;
+    int cof[kNB];
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) cof[c] = poff(k0 + (c < kb ? c : 0), Mp);
+    for (int base = rb + 32 * warp; base < Mp; base += 32 * kWarps) {
+        const int r = base + lane;
+        if (r < Mp) {
+            double w[kNB];
+#pragma unroll
+            for (int c = 0; c < kNB; ++c) w[c] = (c < kb) ? A[cof[c] + r] : 0.0;
+#pragma unroll
+            for (int q = 0; q < kNB; ++q) {
+                if (q < kb) {
+                    asm volatile("" ::: "memory");
+                    double2 col[kNB / 2];
+                    const double2 *src = reinterpret_cast<const double2 *>(sh.Lt[q]);
+#pragma unroll
+                    for (int h = 0; h < kNB / 2; ++h) col[h] = src[h];
+                    w[q] *= sh.inv[q];
+#pragma unroll
+                    for (int c = q + 1; c < kNB; ++c) {
+                        const double l = (c & 1) ? col[c >> 1].y : col[c >> 1].x;
+                        w[c] = fma(-w[q], l, w[c]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < kNB; ++c)
+                if (c < kb) A[cof[c] + r] = w[c];
+        }
+        if (kb1 <= 0) continue;
+        __syncwarp();
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int i0 = base + 16 * half;
+            if (i0 >= Mp) break;
+            double tacc[2][2][2];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int nj = 0; nj < 2; ++nj) tacc[mi][nj][0] = tacc[mi][nj][1] = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < kNB; kk += 4) {
+                const int k = kk + c4;
+                const bool kval = k < kb;
+                const int o = poff(k0 + (kval ? k : 0), Mp);
+                double a[2], b[2];
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi) {
+                    const int i = i0 + 8 * mi + r8;
+                    a[mi] = (kval && i < Mp) ? A[o + i] : 0.0;
+                }
+#pragma unroll
+                for (int nj = 0; nj < 2; ++nj) b[nj] = sh.Lnx[8 * nj + r8][k];  // B[k][n] = Lnx[n][k]
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int nj = 0; nj < 2; ++nj)
+                        dmma_8x8x4(tacc[mi][nj][0], tacc[mi][nj][1], a[mi], b[nj]);
+            }
+#pragma unroll
+            for (int nj = 0; nj < 2; ++nj)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int c = 8 * nj + 2 * c4 + e;
+                    if (c < kb1) {
+                        const int o = poff(n0 + c, Mp);
+#pragma unroll
+                        for (int mi = 0; mi < 2; ++mi) {
+                            const int i = i0 + 8 * mi + r8;
+                            if (i < Mp) A[o + i] -= tacc[mi][nj][e];
+                        }
+                    }
+                }
         }
     }
 }
 
 // Blocked right-looking Cholesky of the first M columns of the packed
-// (M+1)-row system with one panel of look-ahead.
-__device__ __forceinline__ void cholesky_lookahead(double *A, int M, int mc, BlockShared &sh)
+// (M+1)-row system.  Per 16-wide panel p: warp 0 applies panels p-2, p-1 to
+// the diagonal block and factors it together with the rows of panel p+1;
+// meanwhile the warps outside sub-partition 0 apply panel p-1 to the
+// columns beyond panel p+1's diagonal block.  Then all warps solve the rows
+// below panel p+1 and update panel p+1's columns.  Two barriers per panel.
+__device__ __forceinline__ void cholesky_pipelined(double *A, int M, int mc, BlockShared &sh)
 {
     const int Mp = M + 1;
     const int P = (M + kNB - 1) / kNB;
-    const int tid = threadIdx.x;
+    const int warp = threadIdx.x >> 5;
     for (int p = 0; p < P; ++p) {
         const int k0 = p * kNB, kb = min(kNB, M - k0);
-        const int n0 = k0 + kb;           // first column after panel p
-        const int n1 = min(M, n0 + kNB);  // end of panel p+1
-        if (tid < 32) {
-            const unsigned st = factor_diag(A, Mp, k0, kb, mc, sh);
-            if (tid == 0 && st) sh.status |= st;
-        } else if (p > 0) {
-            // Deferred update with panel p-1 of the columns beyond panel p
-            // (warps outside sub-partition 0).
-            update_cols<2>(A, Mp, k0 - kNB, kNB, n0, M, true);
+        const int n0 = k0 + kb;             // first column of panel p+1
+        const int kb1 = max(0, min(kNB, M - n0));
+        const int n1 = n0 + kb1;            // end of panel p+1
+        if (warp == 0) {
+            if (p > 0) update_diag_block(A, Mp, k0, kb, p);
+            __syncwarp();
+            const unsigned st = factor_diag(A, Mp, k0, kb, n0, kb1, mc, sh);
+            if (threadIdx.x == 0 && st) sh.status |= st;
+        } else if (p > 0 && (warp & 3) != 0) {
+            update_cols<2>(A, Mp, k0 - kNB, kNB, n0, M, true, n1);
         }
         __syncthreads();
-        panel_trsm(A, Mp, k0, kb, sh);
+        panel_rows_pass(A, Mp, k0, kb, n0, kb1, n1, sh);
         __syncthreads();
-        if (n0 < M) {
-            // Look-ahead: panel p+1's columns with panel p.
-            update_cols<2>(A, Mp, k0, kb, n0, n1, false);
-            __syncthreads();
-        }
     }
 }
 
@@ -371,7 +470,7 @@ __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternPara
 
     // Cholesky of the first M columns; row M rides along as the
     // forward-substitution right-hand side.
-    cholesky_lookahead(A, M, mc, sh);
+    cholesky_pipelined(A, M, mc, sh);
 
     // log det of the conditional factor (positive pivots only, as
     // core_Xlogdet) and |u|^2 from row M.

@@ -28,6 +28,8 @@ struct MaternParams {
     double nu;          // theta[2]
     double con;         // sigma2 / (2^(nu-1) Gamma(nu)), as the reference computes it
     double dist_scale;  // --dist_scale
+    double inv_range;   // RN(1 / range), host-computed
+    double inv_ds;      // RN(1 / dist_scale), host-computed
     int nu_kind;        // NuKind
     int scale_is_one;   // dist_scale == 1.0: the second division is exact and skipped
 };
@@ -147,15 +149,27 @@ static __device__ __noinline__ double matern_general(double r, double con, doubl
     return con * pow(r, nu) * besselk(nu, r);
 }
 
-// Scaled distance r of core_dcmg for two points.
+// a / b from the correctly rounded reciprocal y = RN(1/b) with one
+// correction step (P. Markstein, IBM J. Res. Dev. 34 (1990) 111-119): the
+// remainder a - b*q is exact in one FMA and q + rem*y is the correctly
+// rounded quotient except in rare tie cases, where it is within 1 ulp.
+__device__ __forceinline__ double div_by_recip(double a, double b, double y)
+{
+    const double q = a * y;
+    const double rem = fma(-q, b, a);
+    return fma(rem, y, q);
+}
+
+// Scaled distance r of core_dcmg for two points: dist / range / dist_scale,
+// the two divisions done by div_by_recip.
 __device__ __forceinline__ double matern_r(double x1, double y1, double x2, double y2,
                                            const MaternParams &p)
 {
     const double dx = x2 - x1;
     const double dy = y2 - y1;
     const double dist = __dsqrt_rn(__fma_rn(dx, dx, __dmul_rn(dy, dy)));
-    double r = __ddiv_rn(dist, p.range);
-    if (!p.scale_is_one) r = __ddiv_rn(r, p.dist_scale);
+    double r = div_by_recip(dist, p.range, p.inv_range);
+    if (!p.scale_is_one) r = div_by_recip(r, p.dist_scale, p.inv_ds);
     return r;
 }
 
