@@ -456,6 +456,109 @@ def run_reference(args):
     }
     print(json.dumps(out))
 
+# ------------------------------------------------------------------ serving
+
+def run_serve(args):
+    """Serving workload: independent fitting jobs with Poisson arrivals.  Per
+    job: n log-uniform in 5,000-500,000 locations uniform on [0,1]^2, nu from
+    {0.5, 1.5, 2.5}, sigma2 uniform in 0.5-2, range uniform in 0.02-0.2, cs
+    from {60, 120, 300}, bc = n/10; observations one random-Fourier-feature
+    draw of the job's process.  Each job is a client that opens the job,
+    issues `--serve-evals` sequential evaluations (the first at the true
+    parameters, then optimizer-like probes around them, nu included, so the
+    general-nu Bessel path runs too) and closes the job.  Reports throughput
+    and request latency (submit to result) percentiles."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    import blockvecchia_b200 as bv
+
+    torch.cuda.set_device(0)
+    J, E = args.serve_jobs, args.serve_evals
+    g = np.random.default_rng(20241)
+    ns = np.exp(g.uniform(np.log(5_000), np.log(500_000), J)).astype(np.int64)
+    nus = g.choice([0.5, 1.5, 2.5], J)
+    s2 = g.uniform(0.5, 2.0, J)
+    rg = g.uniform(0.02, 0.2, J)
+    css = g.choice([60, 120, 300], J)
+    arrivals = np.cumsum(g.exponential(1.0 / args.serve_rate, J))
+
+    t_prep = time.perf_counter()
+    draws = []
+    for i in range(J):
+        x, y = make_locations(int(ns[i]), 1000 + i)
+        obs = rff_draw(x, y, s2[i], rg[i], nus[i], 256, 1000 + i, device="cuda")
+        draws.append((x, y, obs))
+
+    def prep(i):
+        x, y, obs = draws[i]
+        return bv.build_layout(x, y, obs, int(ns[i]) // 10, int(css[i]), seed=i, epochs=10, threads=1)
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 8) as ex:
+        layouts = list(ex.map(prep, range(J)))
+    del draws
+    for L in layouts:
+        L.knn_idx = bv.knn(L)
+    prep_s = time.perf_counter() - t_prep
+
+    srv = bv.Server(device=0, max_inflight=args.serve_inflight)
+    # Warm-up: every kernel variant once (closed-form and general nu, a
+    # shared-memory job and a global-slab job), then clear the record.
+    for i in range(min(J, 6)):
+        j = srv.open_job(layouts[i])
+        srv.evaluate(j, (s2[i], rg[i], nus[i]))
+        srv.evaluate(j, (s2[i], rg[i], nus[i] * 1.03))
+        srv.close_job(j)
+    srv.reset_stats()
+
+    results = [None] * J
+    t0 = time.perf_counter()
+
+    def client(i):
+        time.sleep(max(0.0, t0 + arrivals[i] - time.perf_counter()))
+        r = np.random.default_rng(5000 + i)
+        j = srv.open_job(layouts[i])
+        th0 = np.array([s2[i], rg[i], nus[i]])
+        out = []
+        for e in range(E):
+            th = th0 if e == 0 else th0 * np.exp(0.1 * r.standard_normal(3))
+            out.append(srv.wait(srv.submit(j, th)))
+        srv.close_job(j)
+        results[i] = (out, time.perf_counter())
+
+    clocks = ClockSampler(0)
+    clocks.start()
+    threads = [threading.Thread(target=client, args=(i,)) for i in range(J)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    wall = max(r[1] for r in results) - t0
+    clk = clocks.stop()
+    st = srv.stats()
+    srv.close()
+    lat = np.array([lt for r in results for (_, lt) in r[0]])
+    evals = len(lat)
+    bad = int(sum(1 for r in results for (v, _) in r[0] if not math.isfinite(v)))
+    out = {
+        "metric": "serve p50/p99 ms and evals/s, mixed-size concurrent fitting jobs",
+        "value": round(evals / wall, 3), "unit": "evals/s", "n_gpus": 1,
+        "higher_is_better": True, "impl": "ours", "mode": "serve",
+        "p50_ms": round(float(np.percentile(lat, 50)), 2),
+        "p99_ms": round(float(np.percentile(lat, 99)), 2),
+        "max_ms": round(float(lat.max()), 2),
+        "mean_batch": round(st["mean_batch"], 2), "batches": st["batches"],
+        "evals": evals, "nonfinite_llk": bad, "wall_s": round(wall, 2), "prep_s": round(prep_s, 1),
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{J} jobs, Poisson arrivals at {args.serve_rate}/s, n log-uniform "
+                               f"5k-500k, cs in {{60,120,300}}, bc=n/10, nu in {{0.5,1.5,2.5}}, "
+                               f"{E} sequential evaluations per job",
+                   "total_points": int(ns.sum()), "max_inflight": args.serve_inflight},
+        "clocks": clk,
+    }
+    print(json.dumps(out))
+
 
 def main():
     ap = argparse.ArgumentParser()
@@ -465,6 +568,12 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving workload: concurrent fitting jobs through the request loop")
+    ap.add_argument("--serve-jobs", type=int, default=512)
+    ap.add_argument("--serve-evals", type=int, default=6)
+    ap.add_argument("--serve-rate", type=float, default=8.0, help="job arrivals per second")
+    ap.add_argument("--serve-inflight", type=int, default=2)
     ap.add_argument("--case", choices=sorted(WORKLOADS), default="c3",
                     help="c3: the headline workload (default); c3-small: profiling case")
     args = ap.parse_args()
@@ -472,7 +581,9 @@ def main():
     WORKLOAD = WORKLOADS[args.case]
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.serve:
+        run_serve(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -55,6 +55,16 @@ EXPORTS = {
     "bv_llh_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_int, C.c_int, C.c_int, _D, C.c_double, C.c_void_p,
                                  C.POINTER(C.c_uint), C.c_void_p]),
+    "bv_server_default_opts": (None, [C.c_void_p]),
+    "bv_server_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "bv_server_destroy": (None, [C.c_void_p]),
+    "bv_server_open_job": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, _I]),
+    "bv_server_job_admitted": (C.c_int, [C.c_void_p, C.c_int, _I]),
+    "bv_server_close_job": (C.c_int, [C.c_void_p, C.c_int]),
+    "bv_server_submit": (C.c_int, [C.c_void_p, C.c_int, _D, C.POINTER(C.c_longlong)]),
+    "bv_server_wait": (C.c_int, [C.c_void_p, C.c_longlong, _D, _D, C.c_int]),
+    "bv_server_get_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "bv_server_reset_stats": (C.c_int, [C.c_void_p]),
 }
 
 
@@ -76,6 +86,18 @@ class BvStatus(C.Structure):
     _fields_ = [("blocks", C.c_int), ("cond_fail", C.c_int), ("schur_fail", C.c_int),
                 ("fp32_fallback", C.c_int), ("nonfinite", C.c_int), ("flags_or", C.c_uint),
                 ("llk", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double)]
+
+
+class BvServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget", C.c_size_t), ("max_batch", C.c_int),
+                ("on_failure", C.c_int), ("max_inflight", C.c_int)]
+
+
+class BvServerStats(C.Structure):
+    _fields_ = [("evals", C.c_longlong), ("batches", C.c_longlong), ("mean_batch", C.c_double),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
+                ("bytes_in_use", C.c_size_t), ("hbm_budget", C.c_size_t),
+                ("jobs_admitted", C.c_int), ("jobs_waiting", C.c_int)]
 
 
 class BvError(RuntimeError):

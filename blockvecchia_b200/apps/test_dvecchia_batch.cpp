@@ -1,0 +1,413 @@
+// test_dvecchia_batch -- command-line driver with the reference's flags
+// (src/test_Xvecchia_batch.cpp, include/vecchia_helper_data.h:256-739) over
+// libbv_b200.so.
+//
+// Flags kept: --kernel --ikernel --kernel_init --vecchia_cs --vecchia_bc
+// --num_loc --knn --perf --seed --xy_path --obs_path --tol --maxiter
+// --omp_threads --permutation --dist_scale --lower_bound --upper_bound.
+// --perf evaluates once at --ikernel with zero observations on GenerateXYLoc
+// locations; otherwise the locations/observations CSVs are fitted from
+// --kernel_init.  The objective is bv_llh (the NLopt signature of
+// llh_Xvecchia_batch); NLopt BOBYQA is used when <nlopt.h> exists at build
+// time, else a bounded Nelder-Mead (Nelder & Mead, Comput. J. 7 (1965)
+// 308-313) with the same stopping rule (relative change of the parameters
+// below --tol, at most --maxiter evaluations).  Additional flags:
+// --precision fp64|mixed, --device N, --print-opts (print the parsed options
+// as JSON and exit; needs no GPU).
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <limits>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "bv.h"
+
+#if defined(__has_include)
+#if __has_include(<nlopt.h>)
+#include <nlopt.h>
+#define BV_HAVE_NLOPT 1
+#endif
+#endif
+
+namespace {
+
+struct Opts {
+    int kernel = 1, num_params = 3, num_loc = 2000;
+    double sigma = 1.0, beta = 0.1, nu = 0.5, nugget = 0.0, dist_scale = 1.0;
+    double sigma_init = 0.01, beta_init = 0.01, nu_init = 0.01, nugget_init = 0.01;
+    int knn = 1, seed = 0, perf = 0, vecchia_cs = 100, vecchia_bc = 200, maxiter = 1000;
+    double tol = 1e-5, lower_bound = 0.01, upper_bound = 3.0;
+    int omp_threads = 40, device = 0, precision = BV_PREC_FP64, print_opts = 0;
+    std::string xy_path, obs_path, permutation = "random";
+};
+
+[[noreturn]] void die(const char *msg, const char *arg = "")
+{
+    fprintf(stderr, "error: %s%s\n", msg, arg);
+    exit(1);
+}
+
+// "a:b:c[:d]" with "?" keeping the current value.
+void parse_theta(const char *s, double *a, double *b, double *c, double *d)
+{
+    std::vector<std::string> parts;
+    std::stringstream ss(s);
+    std::string tok;
+    while (std::getline(ss, tok, ':')) parts.push_back(tok);
+    double *dst[4] = {a, b, c, d};
+    for (size_t i = 0; i < parts.size() && i < 4; ++i)
+        if (parts[i] != "?") *dst[i] = atof(parts[i].c_str());
+}
+
+Opts parse(int argc, char **argv)
+{
+    Opts o;
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        const bool has = i + 1 < argc;
+        auto next = [&]() -> const char * { return argv[++i]; };
+        if (a == "--help" || a == "-h") {
+            printf("Usage: test_dvecchia_batch [--kernel K] [--ikernel s2:range:nu] [--kernel_init s2:range:nu]\n"
+                   "  [--vecchia_cs N] [--vecchia_bc N] [--num_loc N] [--knn x] [--perf x] [--seed N]\n"
+                   "  [--xy_path F] [--obs_path F] [--tol k (1e-k)] [--maxiter N] [--omp_threads N]\n"
+                   "  [--permutation random] [--dist_scale d] [--lower_bound b] [--upper_bound b]\n"
+                   "  [--precision fp64|mixed] [--device N] [--print-opts]\n");
+            exit(0);
+        } else if (a == "--xy_path" && has) {
+            o.xy_path = next();
+        } else if (a == "--obs_path" && has) {
+            o.obs_path = next();
+        } else if (a == "--num_loc" && has) {
+            o.num_loc = atoi(next());
+            if (o.num_loc <= 0) die("--num_loc must be positive");
+        } else if (a == "--dist_scale" && has) {
+            o.dist_scale = atof(next());
+            if (!(o.dist_scale > 0)) die("--dist_scale must be > 0");
+        } else if (a == "--vecchia_cs" && has) {
+            o.vecchia_cs = atoi(next());
+            if (o.vecchia_cs < 0) die("--vecchia_cs must be >= 0");
+        } else if (a == "--vecchia_bc" && has) {
+            o.vecchia_bc = atoi(next());
+            if (o.vecchia_bc <= 0) die("--vecchia_bc must be > 0");
+        } else if (a == "--perf" && has) {
+            ++i;  // the reference requires (and ignores) an argument
+            o.perf = 1;
+            o.maxiter = 1;
+        } else if (a == "--knn" && has) {
+            ++i;
+            o.knn = 1;
+        } else if (a == "--kernel" && has) {
+            const std::string k = next();
+            if (k == "univariate_matern_stationary_no_nugget") {
+                o.kernel = 1;
+                o.num_params = 3;
+            } else if (k == "univariate_powexp_stationary_no_nugget") {
+                o.kernel = 2;  // evaluated as Matern by the likelihood, as in the reference
+                o.num_params = 3;
+            } else if (k == "univariate_powexp_nugget_stationary") {
+                o.kernel = 3;
+                o.num_params = 4;
+            } else {
+                die("unsupported kernel: ", k.c_str());
+            }
+        } else if (a == "--ikernel" && has) {
+            parse_theta(next(), &o.sigma, &o.beta, &o.nu, &o.nugget);
+        } else if (a == "--kernel_init" && has) {
+            parse_theta(next(), &o.sigma_init, &o.beta_init, &o.nu_init, &o.nugget_init);
+        } else if (a == "--seed" && has) {
+            o.seed = atoi(next());
+        } else if (a == "--omp_threads" && has) {
+            o.omp_threads = atoi(next());
+        } else if (a == "--maxiter" && has) {
+            o.maxiter = atoi(next());
+            if (o.maxiter <= 0) die("--maxiter must be > 0");
+        } else if (a == "--tol" && has) {
+            const int t = atoi(next());
+            if (t <= 0) die("--tol must be > 0 (k for 1e-k)");
+            o.tol = std::pow(10.0, -t);
+        } else if (a == "--lower_bound" && has) {
+            o.lower_bound = atof(next());
+            if (!(o.lower_bound > 0)) die("--lower_bound must be > 0");
+        } else if (a == "--upper_bound" && has) {
+            o.upper_bound = atof(next());
+            if (!(o.upper_bound < 100)) die("--upper_bound must be < 100");
+        } else if (a == "--permutation" && has) {
+            o.permutation = next();
+            if (o.permutation != "random") die("only --permutation random is supported: ", o.permutation.c_str());
+        } else if (a == "--precision" && has) {
+            const std::string p = next();
+            o.precision = (p == "mixed") ? BV_PREC_MIXED : BV_PREC_FP64;
+        } else if (a == "--device" && has) {
+            o.device = atoi(next());
+        } else if (a == "--print-opts") {
+            o.print_opts = 1;
+        } else if (a == "--3D" || a == "--earth" || a == "--t_slots") {
+            die("not supported by this build (2-D Euclidean only): ", a.c_str());
+        } else {
+            die("unknown or incomplete option: ", a.c_str());
+        }
+    }
+    return o;
+}
+
+void print_opts(const Opts &o)
+{
+    printf("{\"kernel\": %d, \"num_params\": %d, \"num_loc\": %d, \"sigma\": %.17g, \"beta\": %.17g, "
+           "\"nu\": %.17g, \"sigma_init\": %.17g, \"beta_init\": %.17g, \"nu_init\": %.17g, "
+           "\"vecchia_cs\": %d, \"vecchia_bc\": %d, \"knn\": %d, \"perf\": %d, \"seed\": %d, "
+           "\"tol\": %.17g, \"maxiter\": %d, \"lower_bound\": %.17g, \"upper_bound\": %.17g, "
+           "\"dist_scale\": %.17g, \"omp_threads\": %d, \"precision\": %d, \"xy_path\": \"%s\", "
+           "\"obs_path\": \"%s\"}\n",
+           o.kernel, o.num_params, o.num_loc, o.sigma, o.beta, o.nu, o.sigma_init, o.beta_init,
+           o.nu_init, o.vecchia_cs, o.vecchia_bc, o.knn, o.perf, o.seed, o.tol, o.maxiter,
+           o.lower_bound, o.upper_bound, o.dist_scale, o.omp_threads, o.precision,
+           o.xy_path.c_str(), o.obs_path.c_str());
+}
+
+// include/utils.h:27-87: "x,y" per line; one observation per line.
+void load_xy(const std::string &path, int n, std::vector<double> &x, std::vector<double> &y)
+{
+    std::ifstream f(path);
+    if (!f) die("cannot open ", path.c_str());
+    x.assign(n, 0.0);
+    y.assign(n, 0.0);
+    std::string line;
+    int i = 0;
+    while (i < n && std::getline(f, line)) {
+        std::stringstream ss(line);
+        std::string t;
+        if (!std::getline(ss, t, ',')) continue;
+        x[i] = std::stod(t);
+        if (!std::getline(ss, t, ',')) die("malformed line in ", path.c_str());
+        y[i] = std::stod(t);
+        ++i;
+    }
+    if (i < n) die("too few locations in ", path.c_str());
+}
+
+void load_obs(const std::string &path, int n, std::vector<double> &z)
+{
+    std::ifstream f(path);
+    if (!f) die("cannot open ", path.c_str());
+    z.assign(n, 0.0);
+    std::string line;
+    int i = 0;
+    while (i < n && std::getline(f, line)) {
+        std::istringstream ss(line);
+        double v;
+        if (ss >> v) z[i++] = v;
+    }
+    if (i < n) die("too few observations in ", path.c_str());
+}
+
+// Bounded Nelder-Mead maximisation of f on [lb, ub]^d; points are clipped to
+// the box.  Stops when every simplex vertex is within tol (relative) of the
+// best one in every coordinate, or after maxeval evaluations.
+double nelder_mead_max(double (*f)(unsigned, const double *, double *, void *), void *data, int d,
+                       std::vector<double> &x, double lb, double ub, double tol, int maxeval,
+                       int *evals)
+{
+    auto clip = [&](std::vector<double> &v) {
+        for (double &t : v) t = std::min(ub, std::max(lb, t));
+    };
+    int ne = 0;
+    auto F = [&](std::vector<double> &v) {
+        clip(v);
+        ++ne;
+        const double r = f((unsigned)d, v.data(), nullptr, data);
+        return std::isfinite(r) ? r : -std::numeric_limits<double>::infinity();
+    };
+    std::vector<std::vector<double>> s(d + 1, x);
+    std::vector<double> fv(d + 1, -std::numeric_limits<double>::infinity());  // unevaluated vertices never win
+    clip(s[0]);
+    fv[0] = F(s[0]);
+    for (int i = 0; i < d && ne < maxeval; ++i) {
+        s[i + 1] = s[0];
+        double step = 0.1 * (ub - lb);
+        if (s[0][i] + step > ub) step = -step;
+        s[i + 1][i] += step;
+        fv[i + 1] = F(s[i + 1]);
+    }
+    while (ne < maxeval) {
+        std::vector<int> idx(d + 1);
+        for (int i = 0; i <= d; ++i) idx[i] = i;
+        std::sort(idx.begin(), idx.end(), [&](int a, int b) { return fv[a] > fv[b]; });
+        std::vector<std::vector<double>> s2(d + 1);
+        std::vector<double> f2(d + 1);
+        for (int i = 0; i <= d; ++i) {
+            s2[i] = s[idx[i]];
+            f2[i] = fv[idx[i]];
+        }
+        s.swap(s2);
+        fv.swap(f2);
+        double spread = 0.0;
+        for (int i = 1; i <= d; ++i)
+            for (int j = 0; j < d; ++j)
+                spread = std::max(spread, std::fabs(s[i][j] - s[0][j]) / std::max(std::fabs(s[0][j]), 1e-12));
+        if (spread <= tol) break;
+        std::vector<double> c(d, 0.0);
+        for (int i = 0; i < d; ++i)
+            for (int j = 0; j < d; ++j) c[j] += s[i][j] / d;
+        auto along = [&](double t) {
+            std::vector<double> v(d);
+            for (int j = 0; j < d; ++j) v[j] = c[j] + t * (s[d][j] - c[j]);
+            return v;
+        };
+        std::vector<double> xr = along(-1.0);
+        const double fr = F(xr);
+        if (fr > fv[0]) {
+            std::vector<double> xe = along(-2.0);
+            const double fe = ne < maxeval ? F(xe) : -INFINITY;
+            if (fe > fr) {
+                s[d] = xe;
+                fv[d] = fe;
+            } else {
+                s[d] = xr;
+                fv[d] = fr;
+            }
+        } else if (fr > fv[d - 1]) {
+            s[d] = xr;
+            fv[d] = fr;
+        } else {
+            const bool outside = fr > fv[d];
+            std::vector<double> xc = along(outside ? -0.5 : 0.5);
+            const double fc = ne < maxeval ? F(xc) : -INFINITY;
+            if (fc > (outside ? fr : fv[d])) {
+                s[d] = xc;
+                fv[d] = fc;
+            } else {
+                for (int i = 1; i <= d && ne < maxeval; ++i) {
+                    for (int j = 0; j < d; ++j) s[i][j] = s[0][j] + 0.5 * (s[i][j] - s[0][j]);
+                    fv[i] = F(s[i]);
+                }
+            }
+        }
+    }
+    int best = 0;
+    for (int i = 1; i <= d; ++i)
+        if (fv[i] > fv[best]) best = i;
+    x = s[best];
+    *evals = ne;
+    return fv[best];
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    Opts o = parse(argc, argv);
+    if (o.print_opts) {
+        print_opts(o);
+        return 0;
+    }
+    const int n = o.num_loc;
+    std::vector<double> x, y, z;
+    std::vector<double> theta(3);
+    if (o.perf) {
+        x.resize(n);
+        y.resize(n);
+        if (bv_generate_xy(n, o.seed, x.data(), y.data())) die(bv_last_error());
+        z.assign(n, 0.0);  // src/test_Xvecchia_batch.cpp:151-152
+        theta = {o.sigma, o.beta, o.nu};
+    } else {
+        if (o.xy_path.empty() || o.obs_path.empty())
+            die("--xy_path and --obs_path are required unless --perf is given");
+        load_xy(o.xy_path, n, x, y);
+        load_obs(o.obs_path, n, z);
+        theta = {o.sigma_init, o.beta_init, o.nu_init};
+    }
+    fprintf(stderr, n < 2 * o.vecchia_bc ? "You are using the classic Vecchia!\n"
+                                         : "You are using the cluster Vecchia!\n");
+    const int k = (n < 2 * o.vecchia_bc) ? n : o.vecchia_bc;
+    std::vector<int> bn(k), acc(k + 1);
+    std::vector<double> xn(n), yn(n), zn(n), cx(k), cy(k);
+    int bc = 0, fcc = 0;
+    if (bv_layout_build(x.data(), y.data(), z.data(), n, o.vecchia_bc, o.vecchia_cs, o.seed, 50,
+                        o.omp_threads, bn.data(), acc.data(), xn.data(), yn.data(), zn.data(),
+                        cx.data(), cy.data(), &bc, &fcc))
+        die(bv_last_error());
+    fprintf(stderr, "--------------Clustering Done-----------------\n");
+    const int cs = o.vecchia_cs;
+    std::vector<int> knn((size_t)bc * cs);
+    if (cs > 0) {
+        if (o.knn) {
+            if (bv_knn(xn.data(), yn.data(), n, bc, cs, acc.data(), cx.data(), cy.data(), knn.data(),
+                       o.device))
+                die(bv_last_error());
+        } else {
+            // src/test_Xvecchia_batch.cpp:391-404: the cs points before each block.
+            for (int t = 0; t < cs; ++t) knn[t] = t;
+            for (int i = 1; i < bc; ++i)
+                for (int t = 0; t < cs; ++t) knn[(size_t)i * cs + t] = acc[i] - cs + t;
+        }
+    }
+    fprintf(stderr, "--------------Nearest Neighbor Done-----------------\n");
+    bv_layout L = {n, bc, cs, bn.data(), acc.data(), xn.data(), yn.data(), zn.data(), knn.data(),
+                   cx.data(), cy.data()};
+    bv_opts bo;
+    bv_default_opts(&bo);
+    bo.kernel = o.kernel;
+    bo.dist_scale = o.dist_scale;
+    bo.device = o.device;
+    bo.precision = o.precision;
+    bo.print_iter = o.perf ? 0 : 1;
+    bv_handle *h = nullptr;
+    if (bv_create(&L, &bo, &h)) die(bv_last_error());
+
+    const auto t0 = std::chrono::steady_clock::now();
+    double maxf = -HUGE_VAL;
+    int evals = 0;
+    bool ok = true;
+#ifdef BV_HAVE_NLOPT
+    nlopt_opt opt = nlopt_create(NLOPT_LN_BOBYQA, 3);
+    nlopt_set_max_objective(opt, bv_llh, h);
+    std::vector<double> lb(3, o.lower_bound), ub(3, o.upper_bound);
+    nlopt_set_lower_bounds(opt, lb.data());
+    nlopt_set_upper_bounds(opt, ub.data());
+    nlopt_set_xtol_rel(opt, o.tol);
+    nlopt_set_maxeval(opt, o.maxiter);
+    ok = nlopt_optimize(opt, theta.data(), &maxf) >= 0;
+    nlopt_destroy(opt);
+    evals = bv_iterations(h);
+#else
+    maxf = nelder_mead_max(bv_llh, h, 3, theta, o.lower_bound, o.upper_bound, o.tol, o.maxiter,
+                           &evals);
+#endif
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (!ok)
+        printf("nlopt failed!\n");
+    else
+        printf("Found maximum at f(%g, %g, %g) = %0.10g\n", theta[0], theta[1], theta[2], maxf);
+    // include/utils.h:155-171 summary lines and ./log CSV.
+    printf("Total Number of Iterations = %d \n", bv_iterations(h));
+    printf("Total Optimization Time = %lf secs \n", secs);
+    printf("Model Parameters (Variance, range, smoothness): (%.8f, %.8f, %.8f) -> Loglik: %.18f \n",
+           theta[0], theta[1], theta[2], maxf);
+    mkdir("./log", 0755);
+    char path[512];
+    snprintf(path, sizeof(path), "./log/locs_%d_cs_%d_bc_%d_seed_%d_kernel_%f:%f:%f_random", n, cs,
+             o.vecchia_bc, o.seed, o.sigma, o.beta, o.nu);
+    std::ofstream out(path);
+    out << "Iterations, variance, range, smoothness, log-likelihood, time " << std::endl;
+    out << bv_iterations(h) << ", " << theta[0] << ", " << theta[1] << ", " << theta[2] << ", "
+        << std::setprecision(std::numeric_limits<double>::max_digits10) << maxf << ", " << secs
+        << std::endl;
+    bv_status st;
+    bv_get_status(h, &st);
+    if (st.cond_fail + st.schur_fail)
+        fprintf(stderr, "note: %d blocks met a non-positive pivot in the last evaluation\n",
+                st.cond_fail + st.schur_fail);
+    bv_destroy(h);
+    fprintf(stderr, "Done! \n");
+    (void)evals;
+    return 0;
+}

@@ -25,7 +25,9 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
                   "--expt-relaxed-constexpr", "-I", INCLUDE]
 CXXFLAGS = ["-O3", "-fPIC", "-fopenmp", "-std=c++17", "-I", INCLUDE]
 
-CU_SOURCES = ["bv_llh.cu", "bv_knn.cu", "bv_llh_mixed.cu"]
+CU_SOURCES = ["bv_llh.cu", "bv_knn.cu", "bv_llh_mixed.cu", "bv_server.cu"]
+APPS = {"test_dvecchia_batch": os.path.join(HERE, "apps", "test_dvecchia_batch.cpp")}
+BIN = os.path.join(HERE, "bin")
 CPP_SOURCES = ["bv_layout.cpp"]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] if os.path.isdir(CSRC) else []
 
@@ -71,6 +73,14 @@ def build(clean: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
         objs.append(obj)
     if changed or not os.path.exists(LIB):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"])
+        changed = True
+    # Command-line driver with the reference's flags, linked against the library.
+    os.makedirs(BIN, exist_ok=True)
+    for name, src in APPS.items():
+        exe = os.path.join(BIN, name)
+        if changed or not os.path.exists(exe) or os.path.getmtime(src) > os.path.getmtime(exe):
+            _run([CXX, "-O2", "-std=c++17", "-I", INCLUDE, src, "-o", exe, "-L", HERE, "-lbv_b200",
+                  "-Wl,-rpath,$ORIGIN/.."])
     return LIB
 
 

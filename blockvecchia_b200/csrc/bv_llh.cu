@@ -23,8 +23,10 @@
 #include "../../include/bv.h"
 #include "bv_common.cuh"
 #include "bv_knn.cuh"
+#define BV_DEFINE_FP64_KERNEL 1
 #include "bv_llh_fp64.cuh"
 #include "bv_llh_mixed.cuh"
+#include "bv_reduce.cuh"
 
 namespace bv {
 
@@ -39,101 +41,12 @@ void set_error(const char *fmt, ...)
 }
 const char *get_error() { return g_err; }
 
-// Result record of one evaluation (device, then pinned host).
-struct EvalResult {
-    double llk;
-    int blocks, cond_fail, schur_fail, fallback, nonfinite;
-    unsigned flags_or;
-    int pad;
-};
-
-constexpr int kReduceThreads = 1024;
-
-// Deterministic reduction of the per-block contributions: every thread sums
-// a contiguous chunk in block order with Neumaier compensation, then the
-// partial (sum, compensation) pairs are combined in a fixed tree order.
 __global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const double *v,
                                                                 const unsigned *st, int n,
                                                                 EvalResult *out)
 {
-    __shared__ double s_s[kReduceThreads], s_c[kReduceThreads];
-    __shared__ int s_cnt[5][kReduceThreads / 32];
-    __shared__ unsigned s_or[kReduceThreads / 32];
-    const int t = threadIdx.x;
-    const int chunk = (n + kReduceThreads - 1) / kReduceThreads;
-    const int b0 = t * chunk, b1 = min(n, b0 + chunk);
-    double s = 0.0, c = 0.0;
-    int cf = 0, sf = 0, fb = 0, nf = 0, nb = 0;
-    unsigned fo = 0;
-    for (int i = b0; i < b1; ++i) {
-        const double x = v[i];
-        const double tt = s + x;
-        if (fabs(s) >= fabs(x))
-            c += (s - tt) + x;
-        else
-            c += (x - tt) + s;
-        s = tt;
-        const unsigned f = st[i];
-        fo |= f;
-        cf += (f & BV_ST_COND_FAIL) ? 1 : 0;
-        sf += (f & BV_ST_SCHUR_FAIL) ? 1 : 0;
-        fb += (f & BV_ST_FP32_FALLBACK) ? 1 : 0;
-        nf += (f & BV_ST_NONFINITE) ? 1 : 0;
-        ++nb;
-    }
-    s_s[t] = s;
-    s_c[t] = c;
-    // counts: warp reduce
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        cf += __shfl_xor_sync(0xffffffffu, cf, o);
-        sf += __shfl_xor_sync(0xffffffffu, sf, o);
-        fb += __shfl_xor_sync(0xffffffffu, fb, o);
-        nf += __shfl_xor_sync(0xffffffffu, nf, o);
-        nb += __shfl_xor_sync(0xffffffffu, nb, o);
-        fo |= __shfl_xor_sync(0xffffffffu, fo, o);
-    }
-    if ((t & 31) == 0) {
-        s_cnt[0][t >> 5] = cf;
-        s_cnt[1][t >> 5] = sf;
-        s_cnt[2][t >> 5] = fb;
-        s_cnt[3][t >> 5] = nf;
-        s_cnt[4][t >> 5] = nb;
-        s_or[t >> 5] = fo;
-    }
-    __syncthreads();
-    for (int w = kReduceThreads / 2; w > 0; w >>= 1) {
-        if (t < w) {
-            const double a = s_s[t], b = s_s[t + w];
-            const double tt = a + b;
-            double cc = s_c[t] + s_c[t + w];
-            if (fabs(a) >= fabs(b))
-                cc += (a - tt) + b;
-            else
-                cc += (b - tt) + a;
-            s_s[t] = tt;
-            s_c[t] = cc;
-        }
-        __syncthreads();
-    }
-    if (t == 0) {
-        EvalResult r;
-        r.llk = s_s[0] + s_c[0];
-        int c5[5] = {0, 0, 0, 0, 0};
-        unsigned o = 0;
-        for (int w = 0; w < kReduceThreads / 32; ++w) {
-            for (int q = 0; q < 5; ++q) c5[q] += s_cnt[q][w];
-            o |= s_or[w];
-        }
-        r.cond_fail = c5[0];
-        r.schur_fail = c5[1];
-        r.fallback = c5[2];
-        r.nonfinite = c5[3];
-        r.blocks = c5[4];
-        r.flags_or = o;
-        r.pad = 0;
-        *out = r;
-    }
+    __shared__ __align__(16) unsigned char scratch[kReduceScratchBytes];
+    reduce_blocks(v, st, n, out, scratch);
 }
 
 }  // namespace bv
@@ -258,26 +171,26 @@ extern "C" int bv_shard_blocks(const int *batchNum, int bc, int cs, int shard_co
 
 extern "C" const char *bv_last_error(void) { return get_error(); }
 
-static int validate_layout(const bv_layout *L)
+int bv::validate_layout(const bv_layout *L)
 {
     if (!L || L->n <= 0 || L->bc <= 0 || L->cs < 0 || !L->batchNum || !L->batchNumAccum ||
         !L->x || !L->y || !L->obs) {
-        set_error("bv_create: null or non-positive layout field");
+        set_error("layout: null or non-positive field");
         return BV_E_INVALID;
     }
     if (L->batchNumAccum[0] != 0 || L->batchNumAccum[L->bc] != L->n) {
-        set_error("bv_create: batchNumAccum must start at 0 and end at n (got %d, %d, n=%d)",
+        set_error("layout: batchNumAccum must start at 0 and end at n (got %d, %d, n=%d)",
                   L->batchNumAccum[0], L->batchNumAccum[L->bc], L->n);
         return BV_E_INVALID;
     }
     for (int i = 0; i < L->bc; ++i) {
         if (L->batchNum[i] < 0 || L->batchNumAccum[i + 1] - L->batchNumAccum[i] != L->batchNum[i]) {
-            set_error("bv_create: batchNum[%d] inconsistent with batchNumAccum", i);
+            set_error("layout: batchNum[%d] inconsistent with batchNumAccum", i);
             return BV_E_INVALID;
         }
     }
     if (L->cs > 0 && L->bc > 1 && L->batchNum[0] < L->cs) {
-        set_error("bv_create: block 0 has %d points < cs=%d (firstbatch merges clusters until "
+        set_error("layout: block 0 has %d points < cs=%d (firstbatch merges clusters until "
                   ">= cs)", L->batchNum[0], L->cs);
         return BV_E_INVALID;
     }
@@ -287,19 +200,19 @@ static int validate_layout(const bv_layout *L)
             const int *k = L->knn_idx + (size_t)i * L->cs;
             for (int t = 0; t < L->cs; ++t)
                 if (k[t] < 0 || k[t] >= lim) {
-                    set_error("bv_create: knn_idx[%d*cs+%d]=%d outside the earlier blocks [0,%d)",
+                    set_error("layout: knn_idx[%d*cs+%d]=%d outside the earlier blocks [0,%d)",
                               i, t, k[t], lim);
                     return BV_E_INVALID;
                 }
         }
         for (int t = 0; t < L->cs; ++t)
             if (L->knn_idx[t] < 0 || L->knn_idx[t] >= L->n) {
-                set_error("bv_create: knn_idx[%d]=%d outside [0,n)", t, L->knn_idx[t]);
+                set_error("layout: knn_idx[%d]=%d outside [0,n)", t, L->knn_idx[t]);
                 return BV_E_INVALID;
             }
     }
     if (L->cs > 0 && !L->knn_idx && (!L->cx || !L->cy)) {
-        set_error("bv_create: knn_idx is NULL and no block centroids were given");
+        set_error("layout: knn_idx is NULL and no block centroids were given");
         return BV_E_INVALID;
     }
     return BV_OK;

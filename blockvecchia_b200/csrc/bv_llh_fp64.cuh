@@ -506,9 +506,11 @@ __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternPara
 }
 
 // ---------------------------------------------------------------------------
-// The kernel.
+// The kernel (defined in the translation unit that sets BV_DEFINE_FP64_KERNEL;
+// other units use process_block in kernels of their own).
 // ---------------------------------------------------------------------------
 
+#ifdef BV_DEFINE_FP64_KERNEL
 __global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel(LlhArgs a)
 {
     extern __shared__ __align__(16) double smem[];
@@ -541,5 +543,6 @@ __global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel(LlhArgs a)
         __syncthreads();
     }
 }
+#endif  // BV_DEFINE_FP64_KERNEL
 
 }  // namespace bv

@@ -168,6 +168,51 @@ int bv_llh_noalloc(const double *x, const double *y, const double *obs,
                    int cs, const double *theta, double dist_scale,
                    double *llk_out, unsigned *status_flags, void *stream);
 
+/* ---------------------------------------------------------------- serving */
+/* Continuous-batching evaluation server for many concurrent fitting jobs
+ * on one device (no counterpart in the reference, whose driver fits one
+ * dataset per process).  Jobs are copied to HBM while their footprint
+ * (locations, observations, offsets, conditioning indices) fits the budget;
+ * the others wait in FIFO order and are admitted as jobs close.  A scheduler
+ * thread batches every pending request of the admitted jobs into one
+ * persistent launch over all their blocks; requests arriving meanwhile join
+ * the next batch, which starts on the SMs the running batch releases.  Each
+ * result is bit-identical to bv_llh_eval on the same layout, alone or in a
+ * mix. */
+typedef struct bv_server bv_server;
+typedef struct {
+    int device;
+    size_t hbm_budget;  /* bytes for job data; 0 = 90% of free memory      */
+    int max_batch;      /* requests per batch (default 256)                */
+    int on_failure;     /* BV_FAIL_NEGINF | BV_FAIL_CONTINUE               */
+    int max_inflight;   /* batches on the device at once, 1..8 (default 2) */
+} bv_server_opts;
+typedef struct {
+    long long evals, batches;
+    double mean_batch;   /* requests per batch                              */
+    double p50_ms, p99_ms, max_ms;  /* request latency, submit to result    */
+    size_t bytes_in_use, hbm_budget;
+    int jobs_admitted, jobs_waiting;
+} bv_server_stats;
+void bv_server_default_opts(bv_server_opts *o);
+int bv_server_create(const bv_server_opts *opts, bv_server **out);
+void bv_server_destroy(bv_server *s);
+/* Copies the layout (conditioning indices required); *job_id identifies it. */
+int bv_server_open_job(bv_server *s, const bv_layout *layout, double dist_scale,
+                       int *job_id);
+int bv_server_job_admitted(bv_server *s, int job_id, int *admitted);
+/* The job's memory is released once its in-flight requests complete. */
+int bv_server_close_job(bv_server *s, int job_id);
+/* Queue one evaluation at theta = {sigma2, range, nu}; returns at once. */
+int bv_server_submit(bv_server *s, int job_id, const double *theta,
+                     long long *req_id);
+/* Wait for a request (timeout_ms < 0: no limit; BV_E_TIMEOUT otherwise). */
+int bv_server_wait(bv_server *s, long long req_id, double *llk,
+                   double *latency_ms, int timeout_ms);
+int bv_server_get_stats(bv_server *s, bv_server_stats *st);
+/* Clears the evaluation count and latency record (e.g. after a warm-up). */
+int bv_server_reset_stats(bv_server *s);
+
 /* Block sharding for multi-GPU evaluation (blocks are independent given
  * theta; the reference runs them all on one GPU).  Blocks are ranked by cost
  * (M^3 with M = cs + bs, block 0 unconditioned), largest first, ties by

@@ -46,3 +46,14 @@ def test_errors_without_device(bvlib):
                                      mask.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)))
     assert rc == -1
     assert b"invalid" in bvlib.lib().bv_last_error()
+
+
+def test_server_without_device(bvlib):
+    """bv_server_create reports a CUDA error (it does not crash) where no
+    device is usable."""
+    import pytest
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(bvlib.BvError):
+        bvlib.Server()

@@ -1,0 +1,57 @@
+"""test_dvecchia_batch option parsing (no GPU needed): the reference's flags
+and defaults (include/vecchia_helper_data.h:256-739)."""
+import json
+import os
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+EXE = os.path.join(ROOT, "blockvecchia_b200", "bin", "test_dvecchia_batch")
+
+
+@pytest.fixture(scope="module")
+def exe(bvlib):
+    from blockvecchia_b200 import build
+    build.build()
+    assert os.path.exists(EXE)
+    return EXE
+
+
+def _opts(exe, *args):
+    r = subprocess.run([exe, *args, "--print-opts"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    return json.loads(r.stdout)
+
+
+def test_defaults(exe):
+    o = _opts(exe)
+    assert (o["kernel"], o["num_loc"], o["vecchia_cs"], o["vecchia_bc"]) == (1, 2000, 100, 200)
+    assert (o["sigma"], o["beta"], o["nu"]) == (1.0, 0.1, 0.5)
+    assert (o["sigma_init"], o["beta_init"], o["nu_init"]) == (0.01, 0.01, 0.01)
+    assert o["tol"] == 1e-5 and o["maxiter"] == 1000 and o["perf"] == 0 and o["knn"] == 1
+    assert (o["lower_bound"], o["upper_bound"]) == (0.01, 3.0)
+
+
+def test_reference_readme_flags(exe):
+    o = _opts(exe, "--vecchia_cs", "300", "--vecchia_bc", "1500", "--kernel",
+              "univariate_matern_stationary_no_nugget", "--num_loc", "20000", "--ikernel",
+              "1.5:0.1:0.5", "--kernel_init", "0.1:0.1:0.1", "--tol", "4", "--perf", "1",
+              "--knn", "1", "--seed", "0")
+    assert (o["vecchia_cs"], o["vecchia_bc"], o["num_loc"]) == (300, 1500, 20000)
+    assert (o["sigma"], o["beta"], o["nu"]) == (1.5, 0.1, 0.5)
+    assert (o["sigma_init"], o["beta_init"], o["nu_init"]) == (0.1, 0.1, 0.1)
+    assert o["tol"] == pytest.approx(1e-4) and o["perf"] == 1 and o["maxiter"] == 1
+
+
+def test_question_mark_keeps_value(exe):
+    o = _opts(exe, "--ikernel", "?:0.2:?")
+    assert (o["sigma"], o["beta"], o["nu"]) == (1.0, 0.2, 0.5)
+
+
+@pytest.mark.parametrize("bad", [["--tol", "0"], ["--maxiter", "-3"], ["--upper_bound", "200"],
+                                 ["--permutation", "kdtree"], ["--3D", "1"], ["--kernel", "foo"]])
+def test_rejected(exe, bad):
+    r = subprocess.run([exe, *bad, "--print-opts"], capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0 and "error" in r.stderr

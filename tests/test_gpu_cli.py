@@ -1,0 +1,72 @@
+"""test_dvecchia_batch on the device: one --perf evaluation against the
+oracle, and a fit whose optimum matches a fit of the oracle's likelihood."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+EXE = os.path.join(ROOT, "blockvecchia_b200", "bin", "test_dvecchia_batch")
+
+
+@pytest.fixture(scope="module")
+def exe(bvlib):
+    from blockvecchia_b200 import build
+    build.build()
+    return EXE
+
+
+def _run(exe, args, cwd):
+    r = subprocess.run([exe, *args], capture_output=True, text=True, timeout=600, cwd=cwd)
+    assert r.returncode == 0, r.stdout + r.stderr
+    # Per-evaluation lines ("<k>th Model Parameters ...") come first; the
+    # summary line of the optimum is the last match.
+    m = re.findall(r"Model Parameters \(Variance, range, smoothness\): \(([-\d.e]+), ([-\d.e]+), "
+                   r"([-\d.e]+)\) -> Loglik: ([-\d.eE+]+)", r.stdout)
+    assert m, r.stdout
+    last = m[-1]
+    return np.array([float(last[i]) for i in (0, 1, 2)]), float(last[3]), r.stdout
+
+
+def test_perf_mode_matches_oracle(exe, bvlib, oracle, tmp_path):
+    """--perf: GenerateXYLoc locations, zero observations, one evaluation."""
+    n, bc, cs = 3000, 200, 60
+    _, llk, _ = _run(exe, ["--num_loc", str(n), "--vecchia_bc", str(bc), "--vecchia_cs", str(cs),
+                           "--ikernel", "1.5:0.1:0.5", "--perf", "1", "--seed", "0"], tmp_path)
+    x, y = bvlib.generate_xy(n, 0)
+    L = bvlib.build_layout(x, y, np.zeros(n), bc, cs, seed=0, epochs=50)
+    knn = oracle.knn_all(L.x, L.y, cs, L.batchNumAccum, L.cx, L.cy)
+    P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, knn, cs)
+    ref = oracle.llh(P, (1.5, 0.1, 0.5))
+    assert abs(llk - ref) <= 1e-10 * abs(ref)
+
+
+def test_fit_matches_oracle_fit(exe, bvlib, oracle, tmp_path):
+    """A fit from 0.1:0.1:0.1 on an exact GP draw; the optimum agrees with a
+    Nelder-Mead maximisation of the oracle's likelihood to the optimizer
+    tolerance, and the device optimum's likelihood is at least as high."""
+    scipy_opt = pytest.importorskip("scipy.optimize")
+    n, bc, cs = 1500, 150, 40
+    theta_true = (1.5, 0.1, 0.5)
+    x, y = bvlib.generate_xy(n, 1)
+    Sigma = oracle.matern(x, y, x, y, theta_true)
+    z = np.linalg.cholesky(Sigma + 1e-12 * np.eye(n)) @ np.random.default_rng(1).standard_normal(n)
+    np.savetxt(tmp_path / "xy.csv", np.stack([x, y], 1), delimiter=",", fmt="%.17g")
+    np.savetxt(tmp_path / "z.csv", z, fmt="%.17g")
+    th, llk, out = _run(exe, ["--num_loc", str(n), "--vecchia_bc", str(bc), "--vecchia_cs", str(cs),
+                              "--xy_path", "xy.csv", "--obs_path", "z.csv", "--kernel_init",
+                              "0.1:0.1:0.1", "--tol", "7", "--maxiter", "2000", "--seed", "0"],
+                        tmp_path)
+    assert "Loglik" in out and "Found maximum" in out
+    L = bvlib.build_layout(x, y, z, bc, cs, seed=0, epochs=50)
+    knn = oracle.knn_all(L.x, L.y, cs, L.batchNumAccum, L.cx, L.cy)
+    P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, knn, cs)
+    res = scipy_opt.minimize(lambda t: -oracle.llh(P, np.clip(t, 0.01, 3.0)), th, method="Nelder-Mead",
+                             options=dict(xatol=1e-8, fatol=1e-10, maxiter=4000))
+    ref_th = np.clip(res.x, 0.01, 3.0)
+    assert np.all(np.abs(th - ref_th) <= 1e-3 * np.abs(ref_th)), (th, ref_th)
+    assert llk >= -res.fun - 1e-6 * abs(res.fun)
