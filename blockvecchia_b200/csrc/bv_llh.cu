@@ -137,7 +137,7 @@ extern "C" void bv_default_opts(bv_opts *o)
     o->print_iter = 0;
     o->use_graph = 1;
     o->schedule = 0;
-    o->mixed_tol = 1e-11;
+    o->mixed_tol = 1e-8;
     o->shard_count = 1;
     o->shard_index = 0;
 }
@@ -314,31 +314,59 @@ static int enqueue_eval(bv_handle *h, cudaStream_t s)
     BV_CUDA_TRY(cudaMemcpyAsync(h->d_mp, h->h_mp, sizeof(MaternParams), cudaMemcpyHostToDevice, s));
     BV_CUDA_TRY(cudaMemsetAsync(h->d_counters, 0, sizeof(unsigned) * std::max<size_t>(1, h->launches.size()), s));
     BV_CUDA_TRY(record_timing(h->evk0, s));
+    auto fp64_args = [&](unsigned *counter, const int *order, int begin, int end) {
+        LlhArgs a{};
+        a.x = h->d_x;
+        a.y = h->d_y;
+        a.obs = h->d_obs;
+        a.acc = h->d_acc;
+        a.knn = h->d_knn;
+        a.order = order;
+        a.bc = h->bc;
+        a.cs = h->cs;
+        a.smem_max_m = h->smem_max_m;
+        a.slab_max_m = h->max_m;
+        a.block_llk = h->d_block_llk;
+        a.block_status = h->d_block_status;
+        a.work_counter = counter;
+        a.gslab = h->d_slab;
+        a.gslab_stride = h->slab_stride;
+        a.log2pi = std::log(2 * 3.141592653589793);
+        a.mp = h->d_mp;
+        a.task_begin = begin;
+        a.task_end = end;
+        return a;
+    };
     if (h->opts.precision == BV_PREC_MIXED) {
-        int rc = mixed_enqueue(h->mixed, s);
+        // Mixed pass over the handle's blocks, then the FP64 kernel over the
+        // blocks it handed back (the count is read on the device).
+        MixedArgs ma{};
+        ma.x = h->d_x;
+        ma.y = h->d_y;
+        ma.obs = h->d_obs;
+        ma.acc = h->d_acc;
+        ma.knn = h->d_knn;
+        ma.order = h->d_order;
+        ma.bc = h->bc;
+        ma.cs = h->cs;
+        ma.task_end = h->owned;
+        ma.block_llk = h->d_block_llk;
+        ma.block_status = h->d_block_status;
+        ma.mp = h->d_mp;
+        ma.tol = h->opts.mixed_tol;
+        ma.log2pi = std::log(2 * 3.141592653589793);
+        int rc = mixed_enqueue(h->mixed, ma, s);
         if (rc) return rc;
+        if (h->owned > 0) {
+            LlhArgs a = fp64_args(h->d_counters, h->mixed.fallback_list, 0, h->owned);
+            a.task_count = h->mixed.fallback_count;
+            a.status_or = BV_ST_FP32_FALLBACK;
+            llh_fp64_kernel<<<h->grid, kThreads, h->smem_bytes, s>>>(a);
+            BV_CUDA_TRY(cudaGetLastError());
+        }
     } else {
         for (size_t l = 0; l < h->launches.size(); ++l) {
-            LlhArgs a;
-            a.x = h->d_x;
-            a.y = h->d_y;
-            a.obs = h->d_obs;
-            a.acc = h->d_acc;
-            a.knn = h->d_knn;
-            a.order = h->d_order;
-            a.bc = h->bc;
-            a.cs = h->cs;
-            a.smem_max_m = h->smem_max_m;
-            a.slab_max_m = h->max_m;
-            a.block_llk = h->d_block_llk;
-            a.block_status = h->d_block_status;
-            a.work_counter = h->d_counters + l;
-            a.gslab = h->d_slab;
-            a.gslab_stride = h->slab_stride;
-            a.log2pi = std::log(2 * 3.141592653589793);
-            a.mp = h->d_mp;
-            a.task_begin = h->launches[l].begin;
-            a.task_end = h->launches[l].end;
+            LlhArgs a = fp64_args(h->d_counters + l, h->d_order, h->launches[l].begin, h->launches[l].end);
             llh_fp64_kernel<<<h->launches[l].grid, kThreads, h->smem_bytes, s>>>(a);
             BV_CUDA_TRY(cudaGetLastError());
         }
@@ -465,26 +493,9 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
     }
     BV_TRY_H(plan_launches(h));
     if (h->opts.precision == BV_PREC_MIXED) {
-        MixedSetup ms;
-        ms.x = h->d_x;
-        ms.y = h->d_y;
-        ms.obs = h->d_obs;
-        ms.acc = h->d_acc;
-        ms.knn = h->d_knn;
-        ms.order = h->d_order;
-        ms.bc = h->bc;
-        ms.cs = h->cs;
-        ms.max_m = h->max_m;
-        ms.block_llk = h->d_block_llk;
-        ms.block_status = h->d_block_status;
-        ms.mp = h->d_mp;
-        ms.tol = h->opts.mixed_tol;
-        ms.fp64_smem_max_m = h->smem_max_m;
-        ms.fp64_smem_bytes = h->smem_bytes;
-        ms.fp64_grid = h->grid;
-        ms.fp64_slab = h->d_slab;
-        ms.fp64_slab_stride = h->slab_stride;
-        BV_TRY_H(mixed_create(h->mixed, ms));
+        int max_bs = 0;
+        for (int t = 0; t < h->owned; ++t) max_bs = std::max(max_bs, h->batchNum[h->order[t]]);
+        BV_TRY_H(mixed_create(h->mixed, h->device, h->bc, h->cs, max_bs, h->order.data(), h->owned));
     }
     if (h->opts.use_graph) {
         BV_CUDA_H(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -823,7 +834,7 @@ extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *ob
     const size_t smem = block_doubles(smem_max_m) * sizeof(double);
     BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
-    LlhArgs a;
+    LlhArgs a{};
     a.x = x;
     a.y = y;
     a.obs = obs;

@@ -55,6 +55,8 @@ struct LlhArgs {
     double log2pi;              // log(2 * 3.141592653589793)
     const MaternParams *mp;     // device copy of this evaluation's parameters
     int task_begin, task_end;   // slice of `order` this launch serves
+    const int *task_count;      // if set, the slice also ends at *task_count (device)
+    unsigned status_or;         // flags OR-ed into every block status written
 };
 
 __host__ __device__ inline size_t packed_elems(int Mp) { return (size_t)Mp * (Mp + 1) / 2; }
@@ -501,7 +503,7 @@ __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternPara
         unsigned st = sh.status;
         if (!isfinite(v)) st |= 8u;
         a.block_llk[b] = v;
-        a.block_status[b] = st;
+        a.block_status[b] = st | a.status_or;
     }
 }
 
@@ -518,12 +520,13 @@ __global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel(LlhArgs a)
 
     const MaternParams mp = *a.mp;
     const int tid = threadIdx.x;
+    const int task_end = a.task_count ? min(a.task_end, *a.task_count) : a.task_end;
 
     for (;;) {
         if (tid == 0) sh.task = (int)atomicAdd(a.work_counter, 1u) + a.task_begin;
         __syncthreads();
         const int task = sh.task;
-        if (task >= a.task_end) break;
+        if (task >= task_end) break;
         const int b = a.order[task];
         const int bs = a.acc[b + 1] - a.acc[b];
         const int M = ((b == 0) ? 0 : a.cs) + bs;
@@ -532,7 +535,7 @@ __global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel(LlhArgs a)
         if (bs == 0) {  // empty block: contributes -(0 + 0 + 0) / 2
             if (tid == 0) {
                 a.block_llk[b] = -0.0;
-                a.block_status[b] = 0u;
+                a.block_status[b] = a.status_or;
             }
         } else if (M <= a.smem_max_m) {
             process_block(a, mp, b, smem, smem + M, smem + 2 * M, sh);

@@ -140,7 +140,7 @@ class LlhData:
     def __init__(self, layout: Layout, precision: str = "fp64", kernel: int = 1,
                  dist_scale: float = 1.0, device: int = 0, on_failure: str = "neginf",
                  print_iter: bool = False, use_graph: bool = True, schedule: str = "persistent",
-                 mixed_tol: float = 1e-11, shard_count: int = 1, shard_index: int = 0):
+                 mixed_tol: float = 1e-8, shard_count: int = 1, shard_index: int = 0):
         L = layout.normalized()
         self.layout = L
         o = _lib.BvOpts()

@@ -75,7 +75,10 @@ typedef struct {
     int use_graph;     /* capture one evaluation in a CUDA graph (default 1)  */
     int schedule;      /* 0 persistent work queue (default), 1 one launch per
                           size bucket (the comparison baseline)               */
-    double mixed_tol;  /* mixed path: refinement residual tolerance           */
+    double mixed_tol;  /* mixed path: a block is accepted when the estimated
+                          relative error of its refined Sigma22^-1 Sigma21
+                          (|dX_last| / |X| times the first step's
+                          contraction) is at most this; default 1e-8       */
     int shard_count;   /* > 1: this handle evaluates only its shard of the
                           blocks (bv_shard_blocks); partial log-likelihoods of
                           all shards sum to the full one                      */
