@@ -354,7 +354,53 @@ def run_ours(args):
         cpu = {"value": rate, "unit": "evals/s", "cores": cs_.threads, "kind": "port",
                "sample": cs_.describe()}
 
-    launches_per_eval = 2 if args.precision == "fp64" else 4
+    # Mixed precision on the same workload (the FP64 path is the reference):
+    # timed like the FP64 loop, plus the range sweep's relative error and
+    # fallback counts.
+    mixed = None
+    if world == 1 and not args.no_mixed and args.precision == "fp64":
+        with bv.LlhData(L, precision="mixed", device=local, on_failure="continue") as Mx:
+            Mx.set_stream(stream.cuda_stream)
+            for _ in range(args.warmup):
+                step_mx = Mx(theta)
+            torch.cuda.synchronize()
+            m0 = torch.cuda.Event(enable_timing=True)
+            m1 = torch.cuda.Event(enable_timing=True)
+            m0.record(stream)
+            for _ in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
+                vm = Mx(theta)
+            m1.record(stream)
+            torch.cuda.synchronize()
+            ms_mx = m0.elapsed_time(m1)
+            stm = Mx.status()
+            sweep = []
+            for rg_ in (0.02, 0.05, 0.1, 0.2, 0.3):
+                th_ = (w["sigma2"], rg_, w["nu"])
+                v64_ = D(th_)
+                s64_ = D.status()
+                vm_ = Mx(th_)
+                sm_ = Mx.status()
+                sweep.append({"range": rg_, "rel_err": abs(vm_ - v64_) / abs(v64_) if v64_ else None,
+                              "fp32_fallback_blocks": sm_["fp32_fallback"],
+                              "fp64_failed_blocks": s64_["cond_fail"] + s64_["schur_fail"]})
+            D(theta)
+        mixed = {"value": args.steps / (ms_mx / 1e3), "unit": "evals/s",
+                 "vs_fp64": (args.steps / (ms_mx / 1e3)) / (args.steps / (ms / 1e3)),
+                 "rel_err_vs_fp64": abs(vm - v) / abs(v), "fp32_fallback_blocks": stm["fp32_fallback"],
+                 "blocks": int(L.bc), "tol": 1e-8, "range_sweep": sweep,
+                 "note": "FP32 factor of Sigma22 + FP64 refinement; blocks whose FP32 factor or "
+                         "refinement fails are recomputed in FP64 (a probe of every 64th block "
+                         "skips the FP32 pass when most would fail)"}
+    serve = None
+    if world == 1 and args.serve_sample > 0:
+        serve = serve_workload(args.serve_sample, 4, 6.0, 2)
+        serve.pop("clocks", None)
+
+    # FP64: fused kernel + reduction; mixed: probe, decision, mixed pass,
+    # FP64 fallback pass, reduction.
+    launches_per_eval = 2 if args.precision == "fp64" else 5
     value = args.steps / (ms / 1e3)
     out = {
         "metric": METRIC,
@@ -387,6 +433,8 @@ def run_ours(args):
         "clocks": clk,
         "gpu_launches": launches_per_eval * args.steps,
         "llk": v,
+        "mixed": mixed,
+        "serve": serve,
     }
     print(json.dumps(out))
     D.close()
@@ -458,16 +506,16 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ serving
 
-def run_serve(args):
+def serve_workload(jobs, evals, rate, inflight, seed=20241):
     """Serving workload: independent fitting jobs with Poisson arrivals.  Per
     job: n log-uniform in 5,000-500,000 locations uniform on [0,1]^2, nu from
     {0.5, 1.5, 2.5}, sigma2 uniform in 0.5-2, range uniform in 0.02-0.2, cs
     from {60, 120, 300}, bc = n/10; observations one random-Fourier-feature
     draw of the job's process.  Each job is a client that opens the job,
-    issues `--serve-evals` sequential evaluations (the first at the true
-    parameters, then optimizer-like probes around them, nu included, so the
-    general-nu Bessel path runs too) and closes the job.  Reports throughput
-    and request latency (submit to result) percentiles."""
+    issues `evals` sequential evaluations (the first at the true parameters,
+    then optimizer-like probes around them, nu included, so the general-nu
+    Bessel path runs too) and closes the job.  Returns throughput and request
+    latency (submit to result) percentiles."""
     from concurrent.futures import ThreadPoolExecutor
 
     import torch
@@ -475,14 +523,14 @@ def run_serve(args):
     import blockvecchia_b200 as bv
 
     torch.cuda.set_device(0)
-    J, E = args.serve_jobs, args.serve_evals
-    g = np.random.default_rng(20241)
+    J, E = jobs, evals
+    g = np.random.default_rng(seed)
     ns = np.exp(g.uniform(np.log(5_000), np.log(500_000), J)).astype(np.int64)
     nus = g.choice([0.5, 1.5, 2.5], J)
     s2 = g.uniform(0.5, 2.0, J)
     rg = g.uniform(0.02, 0.2, J)
     css = g.choice([60, 120, 300], J)
-    arrivals = np.cumsum(g.exponential(1.0 / args.serve_rate, J))
+    arrivals = np.cumsum(g.exponential(1.0 / rate, J))
 
     t_prep = time.perf_counter()
     draws = []
@@ -502,9 +550,9 @@ def run_serve(args):
         L.knn_idx = bv.knn(L)
     prep_s = time.perf_counter() - t_prep
 
-    srv = bv.Server(device=0, max_inflight=args.serve_inflight)
-    # Warm-up: every kernel variant once (closed-form and general nu, a
-    # shared-memory job and a global-slab job), then clear the record.
+    srv = bv.Server(device=0, max_inflight=inflight)
+    # Warm-up: closed-form and general nu, shared-memory and global-slab
+    # jobs, then clear the record.
     for i in range(min(J, 6)):
         j = srv.open_job(layouts[i])
         srv.evaluate(j, (s2[i], rg[i], nus[i]))
@@ -539,24 +587,33 @@ def run_serve(args):
     st = srv.stats()
     srv.close()
     lat = np.array([lt for r in results for (_, lt) in r[0]])
-    evals = len(lat)
     bad = int(sum(1 for r in results for (v, _) in r[0] if not math.isfinite(v)))
-    out = {
-        "metric": "serve p50/p99 ms and evals/s, mixed-size concurrent fitting jobs",
-        "value": round(evals / wall, 3), "unit": "evals/s", "n_gpus": 1,
-        "higher_is_better": True, "impl": "ours", "mode": "serve",
+    return {
+        "evals_per_s": round(len(lat) / wall, 3),
         "p50_ms": round(float(np.percentile(lat, 50)), 2),
         "p99_ms": round(float(np.percentile(lat, 99)), 2),
         "max_ms": round(float(lat.max()), 2),
         "mean_batch": round(st["mean_batch"], 2), "batches": st["batches"],
-        "evals": evals, "nonfinite_llk": bad, "wall_s": round(wall, 2), "prep_s": round(prep_s, 1),
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{J} jobs, Poisson arrivals at {args.serve_rate}/s, n log-uniform "
-                               f"5k-500k, cs in {{60,120,300}}, bc=n/10, nu in {{0.5,1.5,2.5}}, "
-                               f"{E} sequential evaluations per job",
-                   "total_points": int(ns.sum()), "max_inflight": args.serve_inflight},
+        "evals": int(len(lat)), "nonfinite_llk": bad, "wall_s": round(wall, 2),
+        "prep_s": round(prep_s, 1),
+        "workload": f"{J} jobs, Poisson arrivals at {rate}/s, n log-uniform 5k-500k, "
+                    f"cs in {{60,120,300}}, bc=n/10, nu in {{0.5,1.5,2.5}}, {E} sequential "
+                    f"evaluations per job, {inflight} batches in flight",
+        "total_points": int(ns.sum()),
         "clocks": clk,
     }
+
+
+def run_serve(args):
+    r = serve_workload(args.serve_jobs, args.serve_evals, args.serve_rate, args.serve_inflight)
+    out = {
+        "metric": "serve p50/p99 ms and evals/s, mixed-size concurrent fitting jobs",
+        "value": r["evals_per_s"], "unit": "evals/s", "n_gpus": 1, "higher_is_better": True,
+        "impl": "ours", "mode": "serve", "dtype": "f64", "data": "synthetic",
+        "config": {"workload": r["workload"], "total_points": r["total_points"]},
+        "clocks": r.pop("clocks"),
+    }
+    out.update({k: v for k, v in r.items() if k not in ("workload", "total_points")})
     print(json.dumps(out))
 
 
@@ -568,6 +625,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    ap.add_argument("--serve-sample", type=int, default=64,
+                    help="jobs in the short serving sample of the default run (0: none)")
     ap.add_argument("--serve", action="store_true",
                     help="serving workload: concurrent fitting jobs through the request loop")
     ap.add_argument("--serve-jobs", type=int, default=512)
