@@ -20,6 +20,9 @@ BV_E_TOOLARGE = -5
 BV_E_TIMEOUT = -6
 BV_PREC_FP64 = 0
 BV_PREC_MIXED = 1
+BV_LARGE_AUTO = 0
+BV_LARGE_STREAMED = 1
+BV_LARGE_SLAB = 2
 BV_FAIL_NEGINF = 0
 BV_FAIL_CONTINUE = 1
 BV_ST_COND_FAIL = 1
@@ -79,7 +82,7 @@ class BvOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("kernel", C.c_int), ("dist_scale", C.c_double),
                 ("device", C.c_int), ("on_failure", C.c_int), ("print_iter", C.c_int),
                 ("use_graph", C.c_int), ("schedule", C.c_int), ("mixed_tol", C.c_double),
-                ("shard_count", C.c_int), ("shard_index", C.c_int)]
+                ("shard_count", C.c_int), ("shard_index", C.c_int), ("large_blocks", C.c_int)]
 
 
 class BvStatus(C.Structure):

@@ -19,6 +19,20 @@ const char *get_error();
 // sets the error message and returns BV_E_INVALID on the first violation.
 int validate_layout(const bv_layout *L);
 
+// Shared-memory limits of the fused FP64 kernel on `device` (bv_llh.cu):
+// the dynamic bytes available next to its static shared memory, the largest
+// block M the shared-memory path holds, and the largest M the streamed
+// large-block path holds.  Every caller (handles, the server, the
+// allocation-free entry point) uses the same limits, so a block always takes
+// the same path.
+int fp64_limits(int device, size_t *avail, int *small_m, int *big_m);
+
+// Whether a layout's evaluation compiles the streamed large-block path in:
+// only when more than one wave (sm_count) of blocks has small_m < M <= big_m;
+// otherwise those few blocks take the slab path of the shared-memory
+// algorithm.  Block 0 is unconditioned (M = bs).
+bool use_big_path(const int *batchNum, int bc, int cs, int small_m, int big_m, int sm_count);
+
 #define BV_CUDA_TRY(expr)                                                          \
     do {                                                                           \
         cudaError_t _e = (expr);                                                   \

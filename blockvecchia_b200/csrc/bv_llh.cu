@@ -23,12 +23,37 @@
 #include "../../include/bv.h"
 #include "bv_common.cuh"
 #include "bv_knn.cuh"
-#define BV_DEFINE_FP64_KERNEL 1
+#include "bv_llh_big.cuh"
 #include "bv_llh_fp64.cuh"
 #include "bv_llh_mixed.cuh"
 #include "bv_reduce.cuh"
 
 namespace bv {
+
+// The fused FP64 kernel: persistent CTAs pull blocks from a work counter
+// (largest first) and evaluate each by the path its size calls for.
+template <bool kBig>
+__global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel_t(LlhArgs a)
+{
+    extern __shared__ __align__(128) double smem[];
+    __shared__ BlockShared sh;
+    const MaternParams mp = *a.mp;
+    const int tid = threadIdx.x;
+    const int task_end = a.task_count ? min(a.task_end, *a.task_count) : a.task_end;
+    for (;;) {
+        if (tid == 0) sh.task = (int)atomicAdd(a.work_counter, 1u) + a.task_begin;
+        __syncthreads();
+        const int task = sh.task;
+        if (task >= task_end) break;
+        run_block<kBig>(a, mp, a.order[task], smem, sh);
+        __syncthreads();
+    }
+}
+
+// Without the streamed large-block path compiled in (every layout whose
+// blocks fit shared memory, and the allocation-free entry point), and with it.
+static void (*const llh_fp64_kernel)(LlhArgs) = llh_fp64_kernel_t<false>;
+static void (*const llh_fp64_big_kernel)(LlhArgs) = llh_fp64_kernel_t<true>;
 
 static thread_local char g_err[1024] = "";
 
@@ -77,6 +102,9 @@ struct bv_handle {
     EvalResult *h_res = nullptr;
     // launch plan
     int smem_max_m = 0;
+    int big_max_m = 0;  // largest M of the streamed large-block path
+    bool use_big = false;
+    void (*kernel)(LlhArgs) = nullptr;
     size_t smem_bytes = 0;
     int grid = 0;
     struct Launch {
@@ -140,6 +168,7 @@ extern "C" void bv_default_opts(bv_opts *o)
     o->mixed_tol = 1e-8;
     o->shard_count = 1;
     o->shard_index = 0;
+    o->large_blocks = BV_LARGE_AUTO;
 }
 
 // Cost rank (largest first, ties by index) shared by the schedule and the
@@ -222,12 +251,14 @@ int bv::validate_layout(const bv_layout *L)
 // gets the rest of the per-block opt-in limit.
 static size_t fused_static_smem()
 {
-    cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, llh_fp64_kernel) != cudaSuccess) {
+    cudaFuncAttributes fa, fb;
+    if (cudaFuncGetAttributes(&fa, llh_fp64_kernel) != cudaSuccess ||
+        cudaFuncGetAttributes(&fb, llh_fp64_big_kernel) != cudaSuccess) {
         cudaGetLastError();
         return 16384;
     }
-    return fa.sharedSizeBytes + 1024;
+    // Static plus dynamic shared memory may use the whole opt-in maximum.
+    return std::max(fa.sharedSizeBytes, fb.sharedSizeBytes);
 }
 
 // Largest M whose block fits in `bytes` of dynamic shared memory.
@@ -244,30 +275,66 @@ static int max_m_for_bytes(size_t bytes, size_t per_double)
     return lo;
 }
 
+int bv::fp64_limits(int device, size_t *avail, int *small_m, int *big_m)
+{
+    int optin = 0;
+    BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    const size_t av = (size_t)optin - fused_static_smem();
+    if (avail) *avail = av;
+    if (small_m) *small_m = max_m_for_bytes(av, sizeof(double));
+    if (big_m) *big_m = big_max_m_for_bytes(av);
+    return BV_OK;
+}
+
+bool bv::use_big_path(const int *batchNum, int bc, int cs, int small_m, int big_m, int sm_count)
+{
+    int n_big = 0;
+    for (int b = 0; b < bc; ++b) {
+        const int m = batchNum[b] + (b == 0 ? 0 : cs);
+        if (m > small_m && m <= big_m) ++n_big;
+    }
+    return n_big > sm_count;
+}
+
 static int plan_launches(bv_handle *h)
 {
     cudaDeviceProp prop;
     BV_CUDA_TRY(cudaGetDeviceProperties(&prop, h->device));
-    int optin = 0;
-    BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-    const size_t avail = (size_t)optin - fused_static_smem();
-    const int cap_m = max_m_for_bytes(avail, sizeof(double));
+    size_t avail = 0;
+    int cap_m = 0;
+    {
+        const int rc = fp64_limits(h->device, &avail, &cap_m, &h->big_max_m);
+        if (rc) return rc;
+    }
     h->smem_max_m = std::min(cap_m, h->max_m);
-    h->smem_bytes = block_doubles(h->smem_max_m) * sizeof(double);
     // The cap is per kernel, not per handle: set it to what the device allows
     // so that handles with different block sizes can coexist.
     BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(block_doubles(cap_m) * sizeof(double))));
+                                     (int)avail));
+    BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)avail));
+    // Decided on the whole layout (not the shard), so every shard and the
+    // server take the same path for a given block.
+    h->use_big = (h->opts.large_blocks == BV_LARGE_STREAMED) ||
+                 (h->opts.large_blocks == BV_LARGE_AUTO &&
+                  use_big_path(h->batchNum.data(), h->bc, h->cs, cap_m, h->big_max_m,
+                               prop.multiProcessorCount));
+    h->kernel = h->use_big ? llh_fp64_big_kernel : llh_fp64_kernel;
+    if (h->use_big) {
+        h->smem_bytes = big_launch_smem(h->max_m, cap_m, h->big_max_m);
+        h->slab_stride = big_slab_stride(h->max_m, cap_m, h->big_max_m);
+    } else {
+        h->smem_bytes = block_doubles(h->smem_max_m) * sizeof(double);
+        h->slab_stride = (h->max_m > cap_m) ? (block_doubles(h->max_m) + 31) & ~(size_t)31 : 0;
+    }
     int occ = 0;
-    BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, llh_fp64_kernel, kThreads,
-                                                              h->smem_bytes));
+    BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, h->kernel, kThreads, h->smem_bytes));
     if (occ < 1) {
         set_error("plan: fused kernel cannot be resident (smem %zu B)", h->smem_bytes);
         return BV_E_TOOLARGE;
     }
     h->grid = prop.multiProcessorCount * occ;
-    if (h->max_m > h->smem_max_m) {
-        h->slab_stride = (block_doubles(h->max_m) + 31) & ~(size_t)31;
+    if (h->slab_stride > 0) {
         const size_t bytes = h->slab_stride * sizeof(double) * (size_t)h->grid;
         if (cudaMalloc(&h->d_slab, bytes) != cudaSuccess) {
             cudaGetLastError();
@@ -331,6 +398,7 @@ static int enqueue_eval(bv_handle *h, cudaStream_t s)
         a.work_counter = counter;
         a.gslab = h->d_slab;
         a.gslab_stride = h->slab_stride;
+        a.big_max_m = h->use_big ? h->big_max_m : 0;
         a.log2pi = std::log(2 * 3.141592653589793);
         a.mp = h->d_mp;
         a.task_begin = begin;
@@ -361,13 +429,13 @@ static int enqueue_eval(bv_handle *h, cudaStream_t s)
             LlhArgs a = fp64_args(h->d_counters, h->mixed.fallback_list, 0, h->owned);
             a.task_count = h->mixed.fallback_count;
             a.status_or = BV_ST_FP32_FALLBACK;
-            llh_fp64_kernel<<<h->grid, kThreads, h->smem_bytes, s>>>(a);
+            h->kernel<<<h->grid, kThreads, h->smem_bytes, s>>>(a);
             BV_CUDA_TRY(cudaGetLastError());
         }
     } else {
         for (size_t l = 0; l < h->launches.size(); ++l) {
             LlhArgs a = fp64_args(h->d_counters + l, h->d_order, h->launches[l].begin, h->launches[l].end);
-            llh_fp64_kernel<<<h->launches[l].grid, kThreads, h->smem_bytes, s>>>(a);
+            h->kernel<<<h->launches[l].grid, kThreads, h->smem_bytes, s>>>(a);
             BV_CUDA_TRY(cudaGetLastError());
         }
     }
@@ -830,10 +898,13 @@ extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *ob
     int sms = 0;
     BV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // The kernel's dynamic shared-memory limit is a per-function setting that
-    // other callers also set, so it is set for every call.
+    // other callers also set; every caller sets the same device maximum, and
+    // it is set for every call.
     const size_t smem = block_doubles(smem_max_m) * sizeof(double);
+    int optin_na = 0;
+    BV_CUDA_TRY(cudaDeviceGetAttribute(&optin_na, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+                                     (int)((size_t)optin_na - fused_static_smem())));
     LlhArgs a{};
     a.x = x;
     a.y = y;

@@ -1,0 +1,510 @@
+// bv_llh_big.cuh -- FP64 block evaluation for blocks too large for one SM's
+// shared memory (M = cs + bs above ~235: cs = 300, skewed blocks, a large
+// block 0).
+//
+// Left-looking blocked Cholesky of the same augmented (M+1) x M system as the
+// shared-memory path (rows 0..M-1 covariance, row M the observations), in
+// 16-wide panels, with only two panels resident in shared memory:
+//
+//   * Pcur: panel p (rows k0..M, 16 columns), fully updated; warp 0 factors
+//     its diagonal block (Crout) while
+//   * Pnext: panel p+1 is generated (Matern) and brought up to date with
+//     panels 0..p-1 by warps 1..15: the finished panels live in a per-CTA
+//     global slab (L2-resident), and each one's rows n0..M are streamed into
+//     shared memory by cp.async.bulk copies on an mbarrier, two stages deep,
+//     and applied as rank-16 updates on the FP64 tensor cores (m8n8k4).
+//   * then all warps solve panel p's rows against its diagonal block, panel
+//     p is written to the slab, and panel p+1 takes panel p's update from
+//     shared memory.
+//
+// Panel q is stored in the slab as rows k0_q..M of 16 doubles (row-major),
+// with column c of row r at position c ^ ((r & 3) << 2) (a swizzle that makes
+// the tensor-core fragment loads conflict-free); shared-memory panels and
+// stages use the same layout, so the bulk copies move rows unchanged.
+//
+// The block's contribution is read off the finished panels exactly as in the
+// shared-memory path: positive-pivot log-determinant of the last bs columns
+// and |u|^2 from row M.  Failure semantics are the same (a non-positive pivot
+// stays on the diagonal, its column is zeroed below, the block is flagged).
+// Every wait on an mbarrier is bounded; a wait that gives up flags the block
+// BV_ST_DEVICE_TIMEOUT and the remaining waits are skipped.
+#pragma once
+
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "bv_llh_fp64.cuh"
+
+namespace bv {
+
+constexpr int kBigRC = 256;              // rows per streamed chunk
+constexpr unsigned kBigWaitIters = 1u << 20;
+constexpr unsigned kStDeviceTimeout = 16u;
+
+__host__ __device__ inline int big_panels(int M) { return (M + kNB - 1) / kNB; }
+
+// Doubles of the per-CTA slab: panel q holds rows 16q..M (M+1-16q rows) x 16.
+__host__ __device__ inline size_t big_slab_doubles(int M)
+{
+    const size_t Mp = (size_t)M + 1, P = (size_t)big_panels(M);
+    return 16 * (P * Mp - 8 * P * (P - 1));
+}
+
+__host__ __device__ inline size_t big_panel_base(int q, int Mp)
+{
+    return 16 * ((size_t)q * Mp - 8 * (size_t)q * (q - 1));
+}
+
+// Shared-memory layout (bytes): X, Y, Z (M doubles each), Pcur, Pnext (Mp x
+// 16 doubles), two stages of (kBigRC + 16) x 16 doubles, two mbarriers.
+struct BigLayout {
+    unsigned o_X, o_Y, o_Z, o_cur, o_next, o_stage0, o_stage1, o_bar, total;
+};
+
+__host__ __device__ inline unsigned big_align(unsigned v) { return (v + 127u) & ~127u; }
+
+__host__ __device__ inline BigLayout big_layout(int M)
+{
+    BigLayout l;
+    const unsigned Mp = (unsigned)M + 1;
+    unsigned o = 0;
+    l.o_X = o;      o = big_align(o + 8u * M);
+    l.o_Y = o;      o = big_align(o + 8u * M);
+    l.o_Z = o;      o = big_align(o + 8u * M);
+    l.o_cur = o;    o = big_align(o + 128u * Mp);
+    l.o_next = o;   o = big_align(o + 128u * Mp);
+    l.o_stage0 = o; o = big_align(o + 128u * (kBigRC + 16));
+    l.o_stage1 = o; o = big_align(o + 128u * (kBigRC + 16));
+    l.o_bar = o;    o = o + 16;
+    l.total = o;
+    return l;
+}
+
+// Largest M whose streamed-path layout fits in `bytes` of dynamic shared memory.
+inline int big_max_m_for_bytes(size_t bytes)
+{
+    int lo = 1, hi = 8192;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (big_layout(mid).total <= bytes)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Dynamic shared memory and per-CTA slab (doubles) for blocks up to M = max_m,
+// given the shared-memory path's limit small_m and the streamed path's big_m.
+inline size_t big_launch_smem(int max_m, int small_m, int big_m)
+{
+    size_t b = block_doubles(std::min(max_m, small_m)) * sizeof(double);
+    if (max_m > small_m) {
+        const size_t t = big_layout(std::min(max_m, big_m)).total;
+        if (t > b) b = t;
+    }
+    return b;
+}
+
+inline size_t big_slab_stride(int max_m, int small_m, int big_m)
+{
+    if (max_m <= small_m) return 0;
+    size_t d = big_slab_doubles(std::min(max_m, big_m));
+    if (max_m > big_m) d = std::max(d, block_doubles(max_m));
+    return (d + 31) & ~(size_t)31;
+}
+
+__device__ __forceinline__ int swz(int r, int c) { return c ^ ((r & 3) << 2); }
+
+__device__ __forceinline__ unsigned smem_addr(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase; false when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
+{
+    for (unsigned it = 0; it < kBigWaitIters; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_shared()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_global()
+{
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Named barrier over warps 1..15 (the update warps).
+__device__ __forceinline__ void update_warps_sync()
+{
+    asm volatile("bar.sync 1, %0;" ::"n"(kThreads - 32) : "memory");
+}
+
+// Entry (i, j) of the augmented system: covariance for i < M, the
+// observation of point j on row M.  Same argument order as the
+// shared-memory path's generation, so the entries are identical.
+__device__ __forceinline__ double big_entry(const double *X, const double *Y, const double *Z, int M,
+                                            int i, int j, const MaternParams &mp)
+{
+    return (i < M) ? matern(X[i], Y[i], X[j], Y[j], mp) : Z[j];
+}
+
+// Rank-16 update of a panel held in shared memory, dst rows [d0, d1) (panel
+// local rows relative to dst_r0) and 16 columns:
+//     dst(i, n) -= sum_k A(i, k) * B(n, k)
+// A rows come from `asrc` (local row = i - a_r0), B rows n = 0..15 from
+// `bsrc` (row-major 16 doubles, swizzled by absolute row b_r0 + n).  Tiles of
+// 8 rows x 16 columns are dealt to warps [w0, w0 + nw).
+__device__ __forceinline__ void panel_update_tiles(double *dst, int dst_r0, const double *asrc, int a_r0,
+                                                   const double *bsrc, int b_r0, int r_begin, int r_end,
+                                                   int w0, int nw)
+{
+    const int warp = (threadIdx.x >> 5) - w0, lane = threadIdx.x & 31;
+    if (warp < 0 || warp >= nw) return;
+    const int r8 = lane >> 2, c4 = lane & 3;
+    // B fragments are shared by every tile: B[k][n] = bsrc(n, k).
+    double bf[4][2];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+        for (int nj = 0; nj < 2; ++nj) {
+            const int n = 8 * nj + r8, k = 4 * kk + c4;
+            bf[kk][nj] = bsrc[n * 16 + swz(b_r0 + n, k)];
+        }
+    for (int i0 = r_begin + 8 * warp; i0 < r_end; i0 += 8 * nw) {
+        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+        const int ia = i0 + r8;
+        const bool in = ia < r_end;
+        const double *arow = asrc + (in ? ia - a_r0 : 0) * 16;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const int k = 4 * kk + c4;
+            const double a = in ? arow[swz(ia, k)] : 0.0;
+#pragma unroll
+            for (int nj = 0; nj < 2; ++nj) dmma_8x8x4(acc[nj][0], acc[nj][1], a, bf[kk][nj]);
+        }
+        if (ia < r_end) {
+            double *drow = dst + (ia - dst_r0) * 16;
+#pragma unroll
+            for (int nj = 0; nj < 2; ++nj)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int n = 8 * nj + 2 * c4 + e;
+                    drow[swz(ia, n)] -= acc[nj][e];
+                }
+        }
+    }
+}
+
+// One block with M > the shared-memory capacity.  smem: the dynamic area;
+// slab: this CTA's global slab (big_slab_doubles(M) doubles).
+static __device__ __noinline__ void process_block_big(const LlhArgs &a, const MaternParams &mp, int b,
+                                               unsigned char *smem, double *slab, BlockShared &sh)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int off = a.acc[b];
+    const int bs = a.acc[b + 1] - off;
+    const int mc = (b == 0) ? 0 : a.cs;
+    const int M = mc + bs, Mp = M + 1;
+    const int P = big_panels(M);
+    const BigLayout l = big_layout(M);
+    double *X = reinterpret_cast<double *>(smem + l.o_X);
+    double *Y = reinterpret_cast<double *>(smem + l.o_Y);
+    double *Z = reinterpret_cast<double *>(smem + l.o_Z);
+    double *cur = reinterpret_cast<double *>(smem + l.o_cur);
+    double *nxt = reinterpret_cast<double *>(smem + l.o_next);
+    double *stage[2] = {reinterpret_cast<double *>(smem + l.o_stage0),
+                        reinterpret_cast<double *>(smem + l.o_stage1)};
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + l.o_bar);
+
+    const int *kidx = a.knn + (size_t)b * a.cs;
+    for (int t = tid; t < M; t += kThreads) {
+        const int src = (t < mc) ? __ldg(kidx + t) : off + (t - mc);
+        X[t] = __ldg(a.x + src);
+        Y[t] = __ldg(a.y + src);
+        Z[t] = __ldg(a.obs + src);
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    // Panel 0 into Pcur.
+    for (int e = tid; e < Mp * 16; e += kThreads) {
+        const int r = e >> 4, c = e & 15;
+        const double v = (c < M && r >= c) ? big_entry(X, Y, Z, M, r, c, mp) : 0.0;
+        cur[r * 16 + swz(r, c)] = v;
+    }
+    __syncthreads();
+
+    unsigned st = 0;          // thread 0: pivot flags
+    unsigned phase_bits = 0;  // parity of the next wait per stage (update warps)
+    bool timed_out = false;
+
+    for (int p = 0; p < P; ++p) {
+        const int k0 = p * kNB, kb = min(kNB, M - k0);
+        const int n0 = k0 + kb;                       // first row / column of panel p+1
+        const int kb1 = max(0, min(kNB, M - n0));     // its width
+        if (warp == 0) {
+            // Crout factorization of the diagonal block (lane r < kb owns row k0+r).
+            const bool valid = lane < kb;
+            const int row = k0 + lane;
+            double v[kNB];
+#pragma unroll
+            for (int c = 0; c < kNB; ++c)
+                v[c] = (valid && c < kb && c <= lane) ? cur[lane * 16 + swz(row, c)] : 0.0;
+            unsigned fst = 0;
+#pragma unroll
+            for (int q = 0; q < kNB; ++q) {
+                if (q < kb) {
+                    double s4[4] = {v[q], 0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int k = 0; k < q; ++k) {
+                        const double lqk = __shfl_sync(0xffffffffu, v[k], q);
+                        s4[k & 3] = fma(-v[k], lqk, s4[k & 3]);
+                    }
+                    const double s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+                    const double piv = __shfl_sync(0xffffffffu, s, q);
+                    const bool ok = piv > 0.0;
+                    const double inv = ok ? rsqrt(piv) : 0.0;
+                    if (!ok) fst |= (k0 + q < mc) ? BV_ST_COND_FAIL : BV_ST_SCHUR_FAIL;
+                    if (lane == q) {
+                        v[q] = ok ? piv * inv : piv;
+                        sh.inv[q] = inv;
+                    } else if (lane > q) {
+                        v[q] = s * inv;
+                    }
+                }
+            }
+            if (valid) {
+#pragma unroll
+                for (int c = 0; c < kNB; ++c)
+                    if (c < kb && c <= lane) cur[lane * 16 + swz(row, c)] = v[c];
+            }
+            if (lane < kNB) {
+#pragma unroll
+                for (int c = 0; c < kNB; ++c) {
+                    const double lv = (c <= lane && lane < kb) ? v[c] : 0.0;
+                    sh.Lt[c][lane] = lv;
+                }
+                if (lane >= kb) sh.inv[lane] = 0.0;
+            }
+            if (lane == 0) st |= fst;
+        } else if (kb1 > 0) {
+            // Panel p+1: generate, then apply panels 0..p-1 from the slab.
+            const int nrows = Mp - n0;
+            for (int e = tid - 32; e < nrows * 16; e += kThreads - 32) {
+                const int r = n0 + (e >> 4), c = e & 15;
+                const int j = n0 + c;
+                const double v = (c < kb1 && r >= j) ? big_entry(X, Y, Z, M, r, j, mp) : 0.0;
+                nxt[(r - n0) * 16 + swz(r, c)] = v;
+            }
+            update_warps_sync();
+            const int nchunk = (nrows + kBigRC - 1) / kBigRC;
+            const int items = nchunk * p;       // (chunk, q), q fastest
+            const bool producer = (tid == 32);
+            auto issue = [&](int it) {
+                const int ch = it / p, q = it - ch * p;
+                const int s = it & 1;
+                const int r0 = n0 + ch * kBigRC, r1 = min(Mp, r0 + kBigRC);
+                const int nb = min(kNB, Mp - n0);
+                const double *pq = slab + big_panel_base(q, Mp);
+                const int q0 = q * kNB;
+                const unsigned abytes = 128u * (unsigned)(r1 - r0), bbytes = 128u * (unsigned)nb;
+                mbar_arrive_expect_tx(&bar[s], abytes + bbytes);
+                bulk_g2s(stage[s], pq + (size_t)(r0 - q0) * 16, abytes, &bar[s]);
+                bulk_g2s(stage[s] + kBigRC * 16, pq + (size_t)(n0 - q0) * 16, bbytes, &bar[s]);
+            };
+            // The producer (thread 32) counts the copies it issued per stage
+            // and the phases it saw complete, to drain after a timeout.
+            int issued[2] = {0, 0}, landed[2] = {0, 0};
+            if (producer) {
+                for (int it = 0; it < min(2, items); ++it) {
+                    issue(it);
+                    issued[it & 1]++;
+                }
+            }
+            for (int it = 0; it < items; ++it) {
+                const int ch = it / p;
+                const int s = it & 1;
+                const int r0 = n0 + ch * kBigRC, r1 = min(Mp, r0 + kBigRC);
+                const unsigned par = (phase_bits >> s) & 1u;
+                if (!timed_out) {
+                    if (mbar_wait_bounded(&bar[s], par))
+                        landed[s]++;
+                    else
+                        timed_out = true;
+                }
+                phase_bits ^= 1u << s;
+                panel_update_tiles(nxt, n0, stage[s], r0, stage[s] + kBigRC * 16, n0, r0, r1, 1,
+                                   kWarps - 1);
+                update_warps_sync();
+                if (producer && !timed_out && it + 2 < items) {
+                    fence_proxy_async_shared();
+                    issue(it + 2);
+                    issued[s]++;
+                }
+            }
+            if (producer && timed_out) {
+                // Copies still in flight must land before this shared memory
+                // is used again: wait (bounded) for each stage's last phase.
+                for (int s = 0; s < 2; ++s)
+                    if (issued[s] > landed[s]) mbar_wait_bounded(&bar[s], (unsigned)(issued[s] - 1) & 1u);
+            }
+        }
+        __syncthreads();
+        // Rows below the diagonal block: forward substitution against L_kk.
+        for (int r = k0 + kb + tid; r < Mp; r += kThreads) {
+            double *row = cur + (r - k0) * 16;
+            double w[kNB];
+#pragma unroll
+            for (int c = 0; c < kNB; ++c) w[c] = (c < kb) ? row[swz(r, c)] : 0.0;
+#pragma unroll
+            for (int q = 0; q < kNB; ++q) {
+                if (q < kb) {
+                    asm volatile("" ::: "memory");
+                    double2 col[kNB / 2];
+                    const double2 *srcp = reinterpret_cast<const double2 *>(sh.Lt[q]);
+#pragma unroll
+                    for (int h = 0; h < kNB / 2; ++h) col[h] = srcp[h];
+                    w[q] *= sh.inv[q];
+#pragma unroll
+                    for (int c = q + 1; c < kNB; ++c) {
+                        const double lc = (c & 1) ? col[c >> 1].y : col[c >> 1].x;
+                        w[c] = fma(-w[q], lc, w[c]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < kNB; ++c)
+                if (c < kb) row[swz(r, c)] = w[c];
+        }
+        __syncthreads();
+        // Panel p to the slab; panel p+1 takes panel p's update.
+        {
+            double *pg = slab + big_panel_base(p, Mp);
+            const double2 *s2 = reinterpret_cast<const double2 *>(cur);
+            double2 *g2 = reinterpret_cast<double2 *>(pg);
+            for (int e = tid; e < (Mp - k0) * 8; e += kThreads) g2[e] = s2[e];
+        }
+        if (kb1 > 0)
+            panel_update_tiles(nxt, n0, cur, k0, cur + (n0 - k0) * 16, n0, n0, Mp, 0, kWarps);
+        fence_proxy_async_global();
+        __syncthreads();
+        double *t = cur;
+        cur = nxt;
+        nxt = t;
+    }
+
+    // log det of the conditional factor (positive pivots) and |u|^2 (row M).
+    double ld = 0.0, qf = 0.0;
+    for (int j = mc + tid; j < M; j += kThreads) {
+        const int q = j / kNB, c = j - q * kNB;
+        const double *pq = slab + big_panel_base(q, Mp);
+        const double d = pq[(j - q * kNB) * 16 + swz(j, c)];
+        if (d > 0) ld += log(d * d);
+        const double u = pq[(M - q * kNB) * 16 + swz(M, c)];
+        qf = fma(u, u, qf);
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        ld += __shfl_xor_sync(0xffffffffu, ld, s);
+        qf += __shfl_xor_sync(0xffffffffu, qf, s);
+    }
+    if (lane == 0) {
+        sh.red[0][warp] = ld;
+        sh.red[1][warp] = qf;
+    }
+    if (timed_out) atomicOr(&sh.status, kStDeviceTimeout);
+    if (tid == 0 && st) atomicOr(&sh.status, st);
+    __syncthreads();
+    if (tid == 0) {
+        double Ls = 0.0, Qs = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            Ls += sh.red[0][w];
+            Qs += sh.red[1][w];
+        }
+        const double v = -(Qs + Ls + (double)bs * a.log2pi) * 0.5;
+        unsigned s2 = sh.status;
+        if (!isfinite(v)) s2 |= BV_ST_NONFINITE;
+        a.block_llk[b] = v;
+        a.block_status[b] = s2 | a.status_or;
+        // The barriers are re-initialised for the next block.
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar[0])) : "memory");
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar[1])) : "memory");
+    }
+}
+
+// One block by the path its size calls for: shared memory, the streamed
+// large-block path, or (beyond the streamed path's shared-memory limit) the
+// shared-memory algorithm on this CTA's global slab.
+// kBig = false compiles the shared-memory and slab paths only, so layouts
+// without large blocks run the same code as before the streamed path existed.
+template <bool kBig>
+__device__ __forceinline__ void run_block(const LlhArgs &a, const MaternParams &mp, int b, double *smem,
+                                          BlockShared &sh)
+{
+    const int tid = threadIdx.x;
+    const int bs = a.acc[b + 1] - a.acc[b];
+    const int M = ((b == 0) ? 0 : a.cs) + bs;
+    if (tid == 0) sh.status = 0u;
+    if (bs == 0) {  // empty block: contributes -(0 + 0 + 0) / 2
+        if (tid == 0) {
+            a.block_llk[b] = -0.0;
+            a.block_status[b] = a.status_or;
+        }
+    } else if (M <= a.smem_max_m) {
+        process_block(a, mp, b, smem, smem + M, smem + 2 * M, sh);
+    } else {
+        double *slab = a.gslab + (size_t)blockIdx.x * a.gslab_stride;
+        if (kBig && M <= a.big_max_m)
+            process_block_big(a, mp, b, reinterpret_cast<unsigned char *>(smem), slab, sh);
+        else
+            process_block(a, mp, b, slab, slab + M, slab + 2 * M, sh);
+    }
+}
+
+}  // namespace bv

@@ -57,6 +57,7 @@ struct LlhArgs {
     int task_begin, task_end;   // slice of `order` this launch serves
     const int *task_count;      // if set, the slice also ends at *task_count (device)
     unsigned status_or;         // flags OR-ed into every block status written
+    int big_max_m;              // blocks with smem_max_m < M <= big_max_m: streamed path
 };
 
 __host__ __device__ inline size_t packed_elems(int Mp) { return (size_t)Mp * (Mp + 1) / 2; }
@@ -68,8 +69,8 @@ __device__ __forceinline__ int poff(int j, int Mp) { return j * Mp - ((j * (j + 
 
 // Shared scratch of the kernel besides the block itself.
 struct alignas(16) BlockShared {
-    double L[kNB][kNB];         // factored diagonal block of panel p, L[r][c], 0 above
-    double Lt[kNB][kNB];        // its transpose, Lt[c][r] = L[r][c]: column c contiguous
+    double Lt[kNB][kNB];        // factored diagonal block of panel p, transposed:
+                                // Lt[c][r] = L_rc (0 above the diagonal), column c contiguous
     double Lnx[kNB][kNB + 2];   // L(rows of panel p+1, columns of panel p)
     double inv[kNB];            // 1 / L_jj of panel p (0: failed pivot)
     double red[2][kWarps];
@@ -139,7 +140,7 @@ __device__ __forceinline__ void generate(double *A, const double *X, const doubl
 // by shuffles from lane q), lane q's value is the pivot, and one rsqrt scales
 // the column.  A non-positive or NaN pivot is kept on the diagonal and its
 // column is zeroed below (the block is reported; its log-determinant skips
-// the pivot, as core_Xlogdet does).  Results: L to A, sh.L (diagonal block)
+// the pivot, as core_Xlogdet does).  Results: L to A, sh.Lt (diagonal block)
 // and sh.Lnx (panel p+1 rows), 1/L_jj to sh.inv (0 for a failed pivot).
 __device__ __forceinline__ unsigned factor_diag(double *A, int Mp, int k0, int kb, int n0, int kb1,
                                                 int mc, BlockShared &sh)
@@ -186,7 +187,6 @@ __device__ __forceinline__ unsigned factor_diag(double *A, int Mp, int k0, int k
 #pragma unroll
         for (int c = 0; c < kNB; ++c) {
             const double l = (c <= r && r < kb) ? v[c] : 0.0;
-            sh.L[r][c] = l;
             sh.Lt[c][r] = l;
         }
         if (r >= kb) sh.inv[r] = 0.0;
@@ -506,46 +506,5 @@ __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternPara
         a.block_status[b] = st | a.status_or;
     }
 }
-
-// ---------------------------------------------------------------------------
-// The kernel (defined in the translation unit that sets BV_DEFINE_FP64_KERNEL;
-// other units use process_block in kernels of their own).
-// ---------------------------------------------------------------------------
-
-#ifdef BV_DEFINE_FP64_KERNEL
-__global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel(LlhArgs a)
-{
-    extern __shared__ __align__(16) double smem[];
-    __shared__ BlockShared sh;
-
-    const MaternParams mp = *a.mp;
-    const int tid = threadIdx.x;
-    const int task_end = a.task_count ? min(a.task_end, *a.task_count) : a.task_end;
-
-    for (;;) {
-        if (tid == 0) sh.task = (int)atomicAdd(a.work_counter, 1u) + a.task_begin;
-        __syncthreads();
-        const int task = sh.task;
-        if (task >= task_end) break;
-        const int b = a.order[task];
-        const int bs = a.acc[b + 1] - a.acc[b];
-        const int M = ((b == 0) ? 0 : a.cs) + bs;
-        if (tid == 0) sh.status = 0u;
-
-        if (bs == 0) {  // empty block: contributes -(0 + 0 + 0) / 2
-            if (tid == 0) {
-                a.block_llk[b] = -0.0;
-                a.block_status[b] = a.status_or;
-            }
-        } else if (M <= a.smem_max_m) {
-            process_block(a, mp, b, smem, smem + M, smem + 2 * M, sh);
-        } else {
-            double *slab = a.gslab + (size_t)blockIdx.x * a.gslab_stride;
-            process_block(a, mp, b, slab, slab + M, slab + 2 * M, sh);
-        }
-        __syncthreads();
-    }
-}
-#endif  // BV_DEFINE_FP64_KERNEL
 
 }  // namespace bv

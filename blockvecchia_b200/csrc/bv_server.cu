@@ -36,7 +36,7 @@
 
 #include "../../include/bv.h"
 #include "bv_common.cuh"
-#include "bv_llh_fp64.cuh"
+#include "bv_llh_big.cuh"
 #include "bv_reduce.cuh"
 
 namespace bv {
@@ -53,11 +53,12 @@ struct JobDesc {
 // all requests first.  After a block, thread 0 publishes its contribution
 // (fence, then the request's completion counter); the CTA that completes a
 // request's last block reduces all of the request's blocks.
+template <bool kBig>
 __global__ void __launch_bounds__(kThreads, 1) llh_fp64_server_kernel(const JobDesc *descs,
                                                                      const int2 *tasks, int ntasks,
                                                                      unsigned *counter)
 {
-    extern __shared__ __align__(16) double smem[];
+    extern __shared__ __align__(128) double smem[];
     __shared__ BlockShared sh;
     __shared__ int s_last;
     const int tid = threadIdx.x;
@@ -70,21 +71,7 @@ __global__ void __launch_bounds__(kThreads, 1) llh_fp64_server_kernel(const JobD
         const JobDesc &d = descs[tk.x];
         const LlhArgs a = d.a;
         const MaternParams mp = d.mp;
-        const int b = tk.y;
-        const int bs = a.acc[b + 1] - a.acc[b];
-        const int M = ((b == 0) ? 0 : a.cs) + bs;
-        if (tid == 0) sh.status = 0u;
-        if (bs == 0) {
-            if (tid == 0) {
-                a.block_llk[b] = -0.0;
-                a.block_status[b] = 0u;
-            }
-        } else if (M <= a.smem_max_m) {
-            process_block(a, mp, b, smem, smem + M, smem + 2 * M, sh);
-        } else {
-            double *slab = a.gslab + (size_t)blockIdx.x * a.gslab_stride;
-            process_block(a, mp, b, slab, slab + M, slab + 2 * M, sh);
-        }
+        run_block<kBig>(a, mp, tk.y, smem, sh);
         __syncthreads();
         if (tid == 0) {
             __threadfence();
@@ -97,20 +84,6 @@ __global__ void __launch_bounds__(kThreads, 1) llh_fp64_server_kernel(const JobD
             reduce_blocks(a.block_llk, a.block_status, a.bc, d.out, smem);
         }
     }
-}
-
-// Largest M whose block fits in `bytes` of dynamic shared memory.
-static int server_max_m(size_t bytes)
-{
-    int lo = 1, hi = 4096;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) / 2;
-        if (block_doubles(mid) * sizeof(double) <= bytes)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
 }
 
 }  // namespace bv
@@ -129,6 +102,7 @@ struct Job {
     std::vector<int> sorted;   // blocks by M descending (ties by index)
     std::vector<int> m_start;  // runs of equal M in `sorted`: start offsets
     std::vector<int> m_value;  // ... and their M
+    bool big = false;  // blocks above the shared-memory limit use the streamed path
     size_t footprint = 0;
     bool admitted = false, uploading = false, closing = false;
     int inflight = 0;
@@ -228,6 +202,7 @@ struct bv_server {
     std::vector<std::unique_ptr<Slot>> slots;
     // device constants
     int smem_cap_m = 0;
+    int big_max_m = 0;
     size_t smem_bytes = 0;
     int grid = 0;
     cudaStream_t upload = nullptr;
@@ -338,16 +313,21 @@ bool launch_batch(bv_server *S, bv_server::Slot &sl, const std::vector<Job *> &j
     const int R = (int)jobs.size();
     size_t total = 0;
     int max_m = 1;
+    bool any_big = false;
     for (const Job *j : jobs) {
         total += j->bc;
         max_m = std::max(max_m, j->max_m);
+        any_big = any_big || j->big;
     }
     cudaStream_t s = sl.s;
     bool ok = grow_async(sl.bllk, sl.cap_bllk, total, s) && grow_async(sl.bst, sl.cap_bst, total, s) &&
               grow_async(sl.tasks, sl.cap_tasks, total, s) && grow_pinned(sl.h_tasks, sl.cap_h_tasks, total);
     if (ok && max_m > S->smem_cap_m && max_m > sl.slab_max_m) {
         if (sl.slab) cudaFreeAsync(sl.slab, s);
-        sl.slab_stride = (block_doubles(max_m) + 31) & ~(size_t)31;
+        // Covers both a streamed-path job and any job whose large blocks take
+        // the slab path.
+        sl.slab_stride = std::max(big_slab_stride(max_m, S->smem_cap_m, S->big_max_m),
+                                  (block_doubles(max_m) + 31) & ~(size_t)31);
         ok = cudaMallocAsync(reinterpret_cast<void **>(&sl.slab), sl.slab_stride * 8 * S->grid, s) ==
              cudaSuccess;
         sl.slab_max_m = ok ? max_m : 0;
@@ -382,6 +362,7 @@ bool launch_batch(bv_server *S, bv_server::Slot &sl, const std::vector<Job *> &j
         a.work_counter = nullptr;
         a.gslab = sl.slab;
         a.gslab_stride = sl.slab_stride;
+        a.big_max_m = j.big ? S->big_max_m : 0;
         a.log2pi = std::log(2 * 3.141592653589793);
         a.mp = nullptr;
         a.task_begin = a.task_end = 0;
@@ -419,7 +400,9 @@ bool launch_batch(bv_server *S, bv_server::Slot &sl, const std::vector<Job *> &j
          cudaMemcpyAsync(sl.tasks, sl.h_tasks, total * sizeof(int2), cudaMemcpyHostToDevice, s) == cudaSuccess;
     if (ok) {
         const int grid = std::max(1, std::min<int>(S->grid, (int)total));
-        llh_fp64_server_kernel<<<grid, kThreads, S->smem_bytes, s>>>(sl.desc, sl.tasks, (int)total,
+        // The streamed large-block path is compiled in only when a block needs it.
+        auto kern = any_big ? llh_fp64_server_kernel<true> : llh_fp64_server_kernel<false>;
+        kern<<<grid, kThreads, S->smem_bytes, s>>>(sl.desc, sl.tasks, (int)total,
                                                                      sl.counters);
         ok = cudaGetLastError() == cudaSuccess;
     }
@@ -617,17 +600,33 @@ extern "C" int bv_server_create(const bv_server_opts *opts, bv_server **out)
         BV_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
         S->opts.hbm_budget = fr / 10 * 9;
     }
+    // The same shared-memory limits as the handles, so a block takes the same
+    // path (and gives the same bits) here and under bv_llh_eval.
+    {
+        const int rc = fp64_limits(S->opts.device, nullptr, &S->smem_cap_m, &S->big_max_m);
+        if (rc) return rc;
+    }
     int optin = 0;
     BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, S->opts.device));
-    cudaFuncAttributes fa;
-    BV_CUDA_TRY(cudaFuncGetAttributes(&fa, llh_fp64_server_kernel));
-    S->smem_cap_m = server_max_m((size_t)optin - fa.sharedSizeBytes - 1024);
-    // The dynamic area also holds the reduction scratch of a finishing request.
-    S->smem_bytes = std::max<size_t>(block_doubles(S->smem_cap_m) * sizeof(double), kReduceScratchBytes);
-    BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_server_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)S->smem_bytes));
+    cudaFuncAttributes fa, fb;
+    BV_CUDA_TRY(cudaFuncGetAttributes(&fa, llh_fp64_server_kernel<false>));
+    BV_CUDA_TRY(cudaFuncGetAttributes(&fb, llh_fp64_server_kernel<true>));
+    const size_t stat = std::max(fa.sharedSizeBytes, fb.sharedSizeBytes);
+    const size_t need = std::max<size_t>(std::max(block_doubles(S->smem_cap_m) * sizeof(double),
+                                                  (size_t)big_layout(S->big_max_m).total),
+                                         kReduceScratchBytes);
+    if (need + stat > (size_t)optin) {
+        set_error("bv_server_create: %zu B of dynamic shared memory does not fit next to %zu B static",
+                  need, stat);
+        return BV_E_TOOLARGE;
+    }
+    S->smem_bytes = need;
+    BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_server_kernel<false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_bytes));
+    BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_server_kernel<true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_bytes));
     int occ = 0;
-    BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, llh_fp64_server_kernel, kThreads,
+    BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, llh_fp64_server_kernel<true>, kThreads,
                                                               S->smem_bytes));
     S->grid = prop.multiProcessorCount * std::max(1, occ);
     BV_CUDA_TRY(cudaStreamCreateWithFlags(&S->upload, cudaStreamNonBlocking));
@@ -713,6 +712,11 @@ extern "C" int bv_server_open_job(bv_server *S, const bv_layout *L, double dist_
     j->x.assign(L->x, L->x + L->n);
     j->y.assign(L->y, L->y + L->n);
     j->obs.assign(L->obs, L->obs + L->n);
+    {
+        int sms = 0;
+        BV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->opts.device));
+        j->big = use_big_path(L->batchNum, L->bc, L->cs, S->smem_cap_m, S->big_max_m, sms);
+    }
     j->footprint = job_footprint(*j);
     if (j->footprint > S->opts.hbm_budget) {
         set_error("bv_server_open_job: job needs %zu bytes, more than the budget %zu", j->footprint,

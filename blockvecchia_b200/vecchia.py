@@ -131,6 +131,7 @@ def knn(layout: Layout, device: int = 0) -> np.ndarray:
 _PREC = {"fp64": _lib.BV_PREC_FP64, "mixed": _lib.BV_PREC_MIXED}
 _FAIL = {"neginf": _lib.BV_FAIL_NEGINF, "continue": _lib.BV_FAIL_CONTINUE}
 _SCHED = {"persistent": 0, "bucketed": 1}
+_LARGE = {"auto": _lib.BV_LARGE_AUTO, "streamed": _lib.BV_LARGE_STREAMED, "slab": _lib.BV_LARGE_SLAB}
 
 
 class LlhData:
@@ -140,7 +141,8 @@ class LlhData:
     def __init__(self, layout: Layout, precision: str = "fp64", kernel: int = 1,
                  dist_scale: float = 1.0, device: int = 0, on_failure: str = "neginf",
                  print_iter: bool = False, use_graph: bool = True, schedule: str = "persistent",
-                 mixed_tol: float = 1e-8, shard_count: int = 1, shard_index: int = 0):
+                 mixed_tol: float = 1e-8, shard_count: int = 1, shard_index: int = 0,
+                 large_blocks: str = "auto"):
         L = layout.normalized()
         self.layout = L
         o = _lib.BvOpts()
@@ -156,6 +158,7 @@ class LlhData:
         o.mixed_tol = float(mixed_tol)
         o.shard_count = int(shard_count)
         o.shard_index = int(shard_index)
+        o.large_blocks = _LARGE[large_blocks]
         null_i = C.POINTER(C.c_int)()
         null_d = C.POINTER(C.c_double)()
         self._l = _lib.BvLayout(L.n, L.bc, L.cs, ip(L.batchNum), ip(L.batchNumAccum), dp(L.x),

@@ -29,6 +29,9 @@ extern "C" {
 #define BV_PREC_FP64 0  /* plain FP64 method (reference semantics)           */
 #define BV_PREC_MIXED 1 /* FP32 factor + FP64 refinement, FP64 fallback      */
 
+#define BV_LARGE_AUTO 0     /* large-block path choice (bv_opts.large_blocks) */
+#define BV_LARGE_STREAMED 1 /* left-looking, panels streamed through L2      */
+#define BV_LARGE_SLAB 2     /* shared-memory algorithm on a global slab      */
 #define BV_FAIL_NEGINF 0   /* a failed block makes bv_llh return -HUGE_VAL  */
 #define BV_FAIL_CONTINUE 1 /* keep going like the reference: a non-positive
                               pivot is skipped in the log-determinant        */
@@ -83,6 +86,10 @@ typedef struct {
                           blocks (bv_shard_blocks); partial log-likelihoods of
                           all shards sum to the full one                      */
     int shard_index;   /* 0 .. shard_count-1                                  */
+    int large_blocks;  /* blocks too large for one SM's shared memory:
+                          BV_LARGE_AUTO (default: the streamed path when more
+                          than one wave of blocks needs it, else the slab),
+                          BV_LARGE_STREAMED, BV_LARGE_SLAB                   */
 } bv_opts;
 
 typedef struct {

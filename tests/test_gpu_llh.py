@@ -191,3 +191,41 @@ def test_handles_with_different_block_sizes_coexist(bvlib, oracle, golden_layout
             Ds(th)
             vb1 = Db(th)
     assert vb0 == vb1
+
+
+@pytest.mark.parametrize("n,bc,cs,theta", [
+    (3000, 150, 300, (1.5, 0.1, 0.5)),     # M ~ 320
+    (4000, 20, 300, (1.0, 0.05, 0.5)),     # bs ~ 200, M ~ 500
+    (3000, 100, 240, (1.0, 0.1, 0.8)),     # general nu; block 0 alone exceeds shared memory
+    (6000, 15, 200, (1.0, 0.1, 0.5)),      # M ~ 600: beyond the streamed path, global slab
+])
+@pytest.mark.parametrize("path", ["streamed", "slab", "auto"])
+def test_large_blocks(bvlib, oracle, n, bc, cs, theta, path):
+    """Blocks larger than one SM's shared memory, by both large-block paths,
+    against the oracle at the FP64 parity bound."""
+    L = _gen(bvlib, n, bc, cs)
+    assert int(L.batchNum.max()) + cs > 236
+    P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, L.knn_idx, L.cs)
+    ref, pb = oracle.llh(P, theta, per_block=True)
+    with bvlib.LlhData(L, large_blocks=path) as D:
+        v = D(theta)
+        st = D.status()
+        bl = D.block_llk()
+    per = -(pb[:, 1] ** 2 + pb[:, 0] + L.batchNum * np.log(2 * 3.141592653589793)) * 0.5
+    assert st["cond_fail"] == 0 and st["schur_fail"] == 0 and st["flags_or"] == 0
+    assert abs(v - ref) <= REL * abs(ref), (v, ref)
+    assert np.all(np.abs(bl - per) <= 1e-7 * np.maximum(1.0, np.abs(per)))
+
+
+def test_large_blocks_deterministic_and_served(bvlib):
+    """The streamed path (chosen automatically: more than one wave of large
+    blocks) is deterministic and the server gives the same bits."""
+    L = _gen(bvlib, 8000, 400, 300, seed=2)
+    th = (1.0, 0.08, 1.5)
+    with bvlib.LlhData(L, on_failure="continue") as D, \
+            bvlib.LlhData(L, on_failure="continue", use_graph=False) as E:
+        v = [D(th) for _ in range(2)] + [E(th)]
+    assert v[0] == v[1] == v[2]
+    with bvlib.Server(on_failure="continue") as srv:
+        j = srv.open_job(L)
+        assert srv.evaluate(j, th) == v[0]
