@@ -142,7 +142,7 @@ __device__ __forceinline__ void generate(double *A, const double *X, const doubl
 // column is zeroed below (the block is reported; its log-determinant skips
 // the pivot, as core_Xlogdet does).  Results: L to A, sh.Lt (diagonal block)
 // and sh.Lnx (panel p+1 rows), 1/L_jj to sh.inv (0 for a failed pivot).
-__device__ __forceinline__ unsigned factor_diag(double *A, int Mp, int k0, int kb, int n0, int kb1,
+__device__ __forceinline__ unsigned factor_diag(const double *A, int Mp, int k0, int kb, int n0, int kb1,
                                                 int mc, BlockShared &sh)
 {
     const int lane = threadIdx.x & 31;
@@ -155,20 +155,31 @@ __device__ __forceinline__ unsigned factor_diag(double *A, int Mp, int k0, int k
     for (int c = 0; c < kNB; ++c)
         v[c] = (valid && c < kb && (!low || c <= r)) ? A[poff(k0 + c, Mp) + row] : 0.0;
     unsigned st = 0;
+    // Lagged Crout: the sum for pivot q over k < q-1 was formed while pivot
+    // q-1's reciprocal square root was in flight; only the k = q-1 term (row q
+    // of L by one shuffle) stays on the dependent chain.
+    double pre = v[0];
 #pragma unroll
     for (int q = 0; q < kNB; ++q) {
         if (q < kb) {
-            // Four independent partial sums keep the dependent chain short.
-            double s4[4] = {v[q], 0.0, 0.0, 0.0};
-#pragma unroll
-            for (int k = 0; k < q; ++k) {
-                const double lqk = __shfl_sync(0xffffffffu, v[k], q);
-                s4[k & 3] = fma(-v[k], lqk, s4[k & 3]);
+            double s = pre;
+            if (q > 0) {
+                const double l = __shfl_sync(0xffffffffu, v[q - 1], q);
+                s = fma(-v[q - 1], l, s);
             }
-            const double s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
             const double piv = __shfl_sync(0xffffffffu, s, q);
             const bool ok = piv > 0.0;
             const double inv = ok ? rsqrt(piv) : 0.0;
+            if (q + 1 < kNB) {
+                // Four independent partial sums keep this chain short too.
+                double s4[4] = {v[q + 1], 0.0, 0.0, 0.0};
+#pragma unroll
+                for (int k = 0; k < q; ++k) {
+                    const double lk = __shfl_sync(0xffffffffu, v[k], q + 1);
+                    s4[k & 3] = fma(-v[k], lk, s4[k & 3]);
+                }
+                pre = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+            }
             if (!ok) st |= (k0 + q < mc) ? 1u : 2u;
             if (low && r == q) {
                 v[q] = ok ? piv * inv : piv;
@@ -178,11 +189,9 @@ __device__ __forceinline__ unsigned factor_diag(double *A, int Mp, int k0, int k
             }
         }
     }
-    if (valid) {
-#pragma unroll
-        for (int c = 0; c < kNB; ++c)
-            if (c < kb && (!low || c <= r)) A[poff(k0 + c, Mp) + row] = v[c];
-    }
+    // The factor goes to shared scratch only; store_diag() copies it into A
+    // while the other warps solve the panel rows (nothing reads those entries
+    // of A before then).
     if (low) {
 #pragma unroll
         for (int c = 0; c < kNB; ++c) {
@@ -195,6 +204,22 @@ __device__ __forceinline__ unsigned factor_diag(double *A, int Mp, int k0, int k
         for (int c = 0; c < kNB; ++c) sh.Lnx[r][c] = (valid && c < kb) ? v[c] : 0.0;
     }
     return st;
+}
+
+// Copy the factored diagonal block of panel p (sh.Lt) and the rows of panel
+// p+1 in panel p's columns (sh.Lnx) into A; one element per thread.
+__device__ __forceinline__ void store_diag(double *A, int Mp, int k0, int kb, int n0, int kb1,
+                                           const BlockShared &sh)
+{
+    const int t = threadIdx.x;
+    if (t < kNB * kNB) {
+        const int c = t >> 4, r = t & 15;
+        if (c < kb && r < kb && r >= c) A[poff(k0 + c, Mp) + k0 + r] = sh.Lt[c][r];
+    } else if (t < 2 * kNB * kNB) {
+        const int e = t - kNB * kNB;
+        const int c = e >> 4, r = e & 15;
+        if (c < kb && r < kb1) A[poff(k0 + c, Mp) + n0 + r] = sh.Lnx[r][c];
+    }
 }
 
 __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b)
@@ -442,6 +467,7 @@ __device__ __forceinline__ void cholesky_pipelined(double *A, int M, int mc, Blo
             update_cols<2>(A, Mp, k0 - kNB, kNB, n0, M, true, n1);
         }
         __syncthreads();
+        store_diag(A, Mp, k0, kb, n0, kb1, sh);
         panel_rows_pass(A, Mp, k0, kb, n0, kb1, n1, sh);
         __syncthreads();
     }
