@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel_t(LlhArgs a)
     const MaternParams mp = *a.mp;
     const int tid = threadIdx.x;
     const int task_end = a.task_count ? min(a.task_end, *a.task_count) : a.task_end;
+    init_block_sync(sh);
     for (;;) {
         if (tid == 0) sh.task = (int)atomicAdd(a.work_counter, 1u) + a.task_begin;
         __syncthreads();

@@ -39,8 +39,6 @@
 namespace bv {
 
 constexpr int kBigRC = 256;              // rows per streamed chunk
-constexpr unsigned kBigWaitIters = 1u << 20;
-constexpr unsigned kStDeviceTimeout = 16u;
 
 __host__ __device__ inline int big_panels(int M) { return (M + kNB - 1) / kNB; }
 
@@ -116,65 +114,6 @@ inline size_t big_slab_stride(int max_m, int small_m, int big_m)
 }
 
 __device__ __forceinline__ int swz(int r, int c) { return c ^ ((r & 3) << 2); }
-
-__device__ __forceinline__ unsigned smem_addr(const void *p)
-{
-    return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
-{
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait on an mbarrier phase; false when it gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
-{
-    for (unsigned it = 0; it < kBigWaitIters; ++it)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
-{
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async_shared()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async_global()
-{
-    asm volatile("fence.proxy.async.global;" ::: "memory");
-}
-
-__device__ __forceinline__ void fence_mbar_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
 
 // Named barrier over warps 1..15 (the update warps).
 __device__ __forceinline__ void update_warps_sync()

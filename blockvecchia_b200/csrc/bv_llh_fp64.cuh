@@ -31,6 +31,8 @@
 // tensor cores (mma.sync m8n8k4 f64).
 #pragma once
 
+#include <stdint.h>
+
 #include "bv_matern.cuh"
 
 namespace bv {
@@ -38,6 +40,8 @@ namespace bv {
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kNB = 16;  // panel width of the blocked Cholesky
+constexpr unsigned kWaitIters = 1u << 20;      // bound on every mbarrier wait
+constexpr unsigned kStDeviceTimeout = 16u;     // block status: a bounded wait gave up
 
 struct LlhArgs {
     const double *x, *y, *obs;  // [n] block-ordered
@@ -60,6 +64,74 @@ struct LlhArgs {
     int big_max_m;              // blocks with smem_max_m < M <= big_max_m: streamed path
 };
 
+// ---------------------------------------------------------------------------
+// mbarrier, bulk-copy and proxy-fence helpers (inline PTX).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned smem_addr(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Bounded wait on an mbarrier phase; false when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
+{
+    for (unsigned it = 0; it < kWaitIters; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_shared()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_global()
+{
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
 __host__ __device__ inline size_t packed_elems(int Mp) { return (size_t)Mp * (Mp + 1) / 2; }
 
 // Doubles a block of size M needs: x[M], y[M], packed (M+1)-row triangle.
@@ -74,9 +146,26 @@ struct alignas(16) BlockShared {
     double Lnx[kNB][kNB + 2];   // L(rows of panel p+1, columns of panel p)
     double inv[kNB];            // 1 / L_jj of panel p (0: failed pivot)
     double red[2][kWarps];
+    uint64_t bar_lready;        // warp 0 -> warps 1..15: panel p's factor is in Lt/Lnx/inv
+    uint64_t bar_crit;          // warp 1 -> warp 0: the rows warp 0 needs next are done
+    uint64_t bar_free;          // warps 1..15 -> warp 0: Lt/Lnx/inv may be overwritten
+    unsigned phase_base;        // panels completed by this CTA (parity of the barriers)
     unsigned status;
     int task;
 };
+
+// Once per CTA, before the first block.
+__device__ __forceinline__ void init_block_sync(BlockShared &sh)
+{
+    if (threadIdx.x == 0) {
+        mbar_init(&sh.bar_lready, 1);
+        mbar_init(&sh.bar_crit, 1);
+        mbar_init(&sh.bar_free, 1);
+        sh.phase_base = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+}
 
 // ---------------------------------------------------------------------------
 // Matern generation.
@@ -142,19 +231,19 @@ __device__ __forceinline__ void generate(double *A, const double *X, const doubl
 // column is zeroed below (the block is reported; its log-determinant skips
 // the pivot, as core_Xlogdet does).  Results: L to A, sh.Lt (diagonal block)
 // and sh.Lnx (panel p+1 rows), 1/L_jj to sh.inv (0 for a failed pivot).
-__device__ __forceinline__ unsigned factor_diag(const double *A, int Mp, int k0, int kb, int n0, int kb1,
-                                                int mc, BlockShared &sh)
+__device__ __forceinline__ unsigned factor_diag_regs(const double *A, int Mp, int k0, int kb, int n0,
+                                                     int kb1, int mc, double (&v)[kNB], double &myinv)
 {
     const int lane = threadIdx.x & 31;
     const bool low = lane < kNB;
     const int r = low ? lane : lane - kNB;  // row within its 16-row group
     const bool valid = low ? (r < kb) : (r < kb1);
     const int row = low ? k0 + r : n0 + r;
-    double v[kNB];
 #pragma unroll
     for (int c = 0; c < kNB; ++c)
         v[c] = (valid && c < kb && (!low || c <= r)) ? A[poff(k0 + c, Mp) + row] : 0.0;
     unsigned st = 0;
+    myinv = 0.0;
     // Lagged Crout: the sum for pivot q over k < q-1 was formed while pivot
     // q-1's reciprocal square root was in flight; only the k = q-1 term (row q
     // of L by one shuffle) stays on the dependent chain.
@@ -183,42 +272,34 @@ __device__ __forceinline__ unsigned factor_diag(const double *A, int Mp, int k0,
             if (!ok) st |= (k0 + q < mc) ? 1u : 2u;
             if (low && r == q) {
                 v[q] = ok ? piv * inv : piv;
-                sh.inv[q] = inv;
+                myinv = inv;
             } else if (!low || r > q) {
                 v[q] = s * inv;
             }
         }
     }
-    // The factor goes to shared scratch only; store_diag() copies it into A
-    // while the other warps solve the panel rows (nothing reads those entries
-    // of A before then).
+    return st;
+}
+
+// The factored diagonal block to sh.Lt (transposed), its reciprocal pivots
+// to sh.inv, and the rows of panel p+1 to sh.Lnx.
+__device__ __forceinline__ void publish_diag(BlockShared &sh, const double (&v)[kNB], double myinv, int kb,
+                                             int kb1)
+{
+    const int lane = threadIdx.x & 31;
+    const bool low = lane < kNB;
+    const int r = low ? lane : lane - kNB;
     if (low) {
 #pragma unroll
         for (int c = 0; c < kNB; ++c) {
             const double l = (c <= r && r < kb) ? v[c] : 0.0;
             sh.Lt[c][r] = l;
         }
-        if (r >= kb) sh.inv[r] = 0.0;
+        sh.inv[r] = (r < kb) ? myinv : 0.0;
     } else {
+        const bool valid = r < kb1;
 #pragma unroll
         for (int c = 0; c < kNB; ++c) sh.Lnx[r][c] = (valid && c < kb) ? v[c] : 0.0;
-    }
-    return st;
-}
-
-// Copy the factored diagonal block of panel p (sh.Lt) and the rows of panel
-// p+1 in panel p's columns (sh.Lnx) into A; one element per thread.
-__device__ __forceinline__ void store_diag(double *A, int Mp, int k0, int kb, int n0, int kb1,
-                                           const BlockShared &sh)
-{
-    const int t = threadIdx.x;
-    if (t < kNB * kNB) {
-        const int c = t >> 4, r = t & 15;
-        if (c < kb && r < kb && r >= c) A[poff(k0 + c, Mp) + k0 + r] = sh.Lt[c][r];
-    } else if (t < 2 * kNB * kNB) {
-        const int e = t - kNB * kNB;
-        const int c = e >> 4, r = e & 15;
-        if (c < kb && r < kb1) A[poff(k0 + c, Mp) + n0 + r] = sh.Lnx[r][c];
     }
 }
 
@@ -283,45 +364,6 @@ __device__ __forceinline__ void mma_tile(double *A, int Mp, int k0, int kb_rt, i
     }
 }
 
-// Rows [cb, Mp) x cols [cb, ce) (lower part) with panel k0..k0+kb-1, by warps
-// [w0, w0+nw), in tiles of 32 rows x (8*NJ) columns.
-// skip_sp0: leave the warps of sub-partition 0 (ids = 0 mod 4) out, so warp
-// 0's diagonal factorization does not queue behind their tensor-core work.
-// Elements with both indices below `excl` are left alone (a diagonal block
-// another warp updates).
-template <int NJ>
-__device__ __forceinline__ void update_cols(double *A, int Mp, int k0, int kb, int cb, int ce,
-                                            bool skip_sp0, int excl)
-{
-    constexpr int TW = 8 * NJ;
-    const int nrow = Mp - cb, ncol = ce - cb;
-    if (nrow <= 0 || ncol <= 0) return;
-    const int wid = threadIdx.x >> 5;
-    int warp, nw;
-    if (skip_sp0) {
-        if ((wid & 3) == 0) return;
-        warp = wid - (wid >> 2) - 1;
-        nw = kWarps - kWarps / 4;
-    } else {
-        warp = wid;
-        nw = kWarps;
-    }
-    const int TR = (nrow + 31) >> 5, TC = (ncol + TW - 1) / TW;
-    // Enumerate lower tiles (tc, tr >= first row tile reaching column tile tc).
-    int t = 0;
-    for (int tc = 0; tc < TC; ++tc) {
-        const int j0 = cb + tc * TW;
-        const int tr0 = (j0 - cb) >> 5;
-        for (int tr = tr0; tr < TR; ++tr, ++t) {
-            if (t % nw != warp) continue;
-            if (kb == kNB)
-                mma_tile<4, NJ, kNB>(A, Mp, k0, kb, cb + (tr << 5), j0, ce, excl);
-            else
-                mma_tile<4, NJ, 0>(A, Mp, k0, kb, cb + (tr << 5), j0, ce, excl);
-        }
-    }
-}
-
 // Warp 0: the diagonal block of panel p (rows/cols k0..k0+kb-1, lower part)
 // takes the updates of panels p-2 and p-1, which the bulk updates leave to
 // it (FP64 tensor cores, three 8x8 sub-tiles).
@@ -354,123 +396,245 @@ __device__ __forceinline__ void update_diag_block(double *A, int Mp, int k0, int
     }
 }
 
-// All warps, 32-row groups of rows [rb, Mp): each lane solves its row of
-// X L_kk^T = A(row, panel p) by forward substitution (backward stable; column
-// q of L_kk read per stage as eight 16-byte broadcasts behind a compiler
-// fence so the 120 factor values are not all hoisted into registers) and
-// stores X as the row's panel-p factor; then the warp updates panel p+1's
-// columns, A(rows, panel p+1) -= X Lnx^T, on the FP64 tensor cores.
-__device__ __forceinline__ void panel_rows_pass(double *A, int Mp, int k0, int kb, int n0, int kb1,
-                                                int rb, const BlockShared &sh)
+// ---------------------------------------------------------------------------
+// Warp-specialised Cholesky of the first M columns of the packed (M+1)-row
+// system.
+//
+// Warp 0 walks the diagonal: for panel p it applies panels p-2 and p-1 to
+// the diagonal block, waits until the critical rows below it are done,
+// factors the block together with the rows of panel p+1 (registers), waits
+// until the bulk warps are done with the previous factor, publishes the new
+// one (Lt, Lnx, inv), signals, and stores panel p+1's rows for its next
+// diagonal update.  The critical-rows warp then brings the 16 rows below
+// panel p+1 up to date in panel p+1's columns (panel p-1's and panel p's
+// contributions) and signals warp 0, while the bulk warps solve the
+// remaining rows of panel p and apply panel p-1 to the columns beyond panel
+// p+1.  Every element of panel c's columns receives panel q's
+// contribution exactly once: q = c-1 and c-2 from warp 0 on the diagonal
+// block and from the row work of panel c-1 below it, q <= c-3 from the
+// column work of iteration q+1.  Hand-offs are mbarriers with bounded waits;
+// while one side runs, the data the other side touches is disjoint (the
+// diagonal block and next-panel rows for warp 0; everything below or to the
+// right of them for the others).
+// ---------------------------------------------------------------------------
+
+// Lanes < nl solve rows base+lane of panel p against L_pp (sh.Lt, sh.inv):
+// forward substitution, column q of L_pp read per stage as eight 16-byte
+// broadcasts behind a compiler fence so the factor values are not all
+// hoisted into registers.
+__device__ __forceinline__ void solve_rows(double *A, int Mp, int k0, int kb, int base, int nl,
+                                           const BlockShared &sh)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int r8 = lane >> 2, c4 = lane & 3;
+    const int lane = threadIdx.x & 31;
+    const int r = base + lane;
+    if (lane >= nl || r >= Mp) return;
     int cof[kNB];
 #pragma unroll
     for (int c = 0; c < kNB; ++c) cof[c] = poff(k0 + (c < kb ? c : 0), Mp);
-    for (int base = rb + 32 * warp; base < Mp; base += 32 * kWarps) {
-        const int r = base + lane;
-        if (r < Mp) {
-            double w[kNB];
+    double w[kNB];
 #pragma unroll
-            for (int c = 0; c < kNB; ++c) w[c] = (c < kb) ? A[cof[c] + r] : 0.0;
+    for (int c = 0; c < kNB; ++c) w[c] = (c < kb) ? A[cof[c] + r] : 0.0;
 #pragma unroll
-            for (int q = 0; q < kNB; ++q) {
-                if (q < kb) {
-                    asm volatile("" ::: "memory");
-                    double2 col[kNB / 2];
-                    const double2 *src = reinterpret_cast<const double2 *>(sh.Lt[q]);
+    for (int q = 0; q < kNB; ++q) {
+        if (q < kb) {
+            asm volatile("" ::: "memory");
+            double2 col[kNB / 2];
+            const double2 *src = reinterpret_cast<const double2 *>(sh.Lt[q]);
 #pragma unroll
-                    for (int h = 0; h < kNB / 2; ++h) col[h] = src[h];
-                    w[q] *= sh.inv[q];
+            for (int h = 0; h < kNB / 2; ++h) col[h] = src[h];
+            w[q] *= sh.inv[q];
 #pragma unroll
-                    for (int c = q + 1; c < kNB; ++c) {
-                        const double l = (c & 1) ? col[c >> 1].y : col[c >> 1].x;
-                        w[c] = fma(-w[q], l, w[c]);
-                    }
-                }
+            for (int c = q + 1; c < kNB; ++c) {
+                const double l = (c & 1) ? col[c >> 1].y : col[c >> 1].x;
+                w[c] = fma(-w[q], l, w[c]);
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kNB; ++c)
+        if (c < kb) A[cof[c] + r] = w[c];
+}
+
+// One warp: rows i0..i0+15 (below panel p+1) of panel p+1's columns take
+// panel p's contribution (solved rows in A, panel p+1's rows from sh.Lnx) and,
+// when prev, panel p-1's (both operands in A), on the FP64 tensor cores.
+// Fragments (m8n8k4, .row.col): lane l holds A[l>>2][l&3], B[l&3][l>>2] and
+// C[l>>2][2(l&3)+{0,1}].
+__device__ __forceinline__ void update_next_rows16(double *A, int Mp, int k0, int kb, int n0, int kb1,
+                                                   int i0, bool prev, const BlockShared &sh)
+{
+    const int lane = threadIdx.x & 31;
+    const int r8 = lane >> 2, c4 = lane & 3;
+    double acc[2][2][2];
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int nj = 0; nj < 2; ++nj) acc[mi][nj][0] = acc[mi][nj][1] = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < kNB; kk += 4) {
+        const int k = kk + c4;
+        const bool kval = k < kb;
+        const int o = poff(k0 + (kval ? k : 0), Mp);
+        double a[2], b[2];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+            const int i = i0 + 8 * mi + r8;
+            a[mi] = (kval && i < Mp) ? A[o + i] : 0.0;
+        }
+#pragma unroll
+        for (int nj = 0; nj < 2; ++nj) b[nj] = sh.Lnx[8 * nj + r8][k];  // B[k][n] = Lnx[n][k]
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int nj = 0; nj < 2; ++nj) dmma_8x8x4(acc[mi][nj][0], acc[mi][nj][1], a[mi], b[nj]);
+    }
+    if (prev) {
+#pragma unroll
+        for (int kk = 0; kk < kNB; kk += 4) {
+            const int o = poff(k0 - kNB + kk + c4, Mp);
+            double a[2], b[2];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi) {
+                const int i = i0 + 8 * mi + r8;
+                a[mi] = (i < Mp) ? A[o + i] : 0.0;
             }
 #pragma unroll
-            for (int c = 0; c < kNB; ++c)
-                if (c < kb) A[cof[c] + r] = w[c];
-        }
-        if (kb1 <= 0) continue;
-        __syncwarp();
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            const int i0 = base + 16 * half;
-            if (i0 >= Mp) break;
-            double tacc[2][2][2];
+            for (int nj = 0; nj < 2; ++nj) {
+                const int j = 8 * nj + r8;
+                b[nj] = (j < kb1) ? A[o + n0 + j] : 0.0;
+            }
 #pragma unroll
             for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-                for (int nj = 0; nj < 2; ++nj) tacc[mi][nj][0] = tacc[mi][nj][1] = 0.0;
+                for (int nj = 0; nj < 2; ++nj) dmma_8x8x4(acc[mi][nj][0], acc[mi][nj][1], a[mi], b[nj]);
+        }
+    }
 #pragma unroll
-            for (int kk = 0; kk < kNB; kk += 4) {
-                const int k = kk + c4;
-                const bool kval = k < kb;
-                const int o = poff(k0 + (kval ? k : 0), Mp);
-                double a[2], b[2];
+    for (int nj = 0; nj < 2; ++nj)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int c = 8 * nj + 2 * c4 + e;
+            if (c < kb1) {
+                const int o = poff(n0 + c, Mp);
 #pragma unroll
                 for (int mi = 0; mi < 2; ++mi) {
                     const int i = i0 + 8 * mi + r8;
-                    a[mi] = (kval && i < Mp) ? A[o + i] : 0.0;
+                    if (i < Mp) A[o + i] -= acc[mi][nj][e];
                 }
-#pragma unroll
-                for (int nj = 0; nj < 2; ++nj) b[nj] = sh.Lnx[8 * nj + r8][k];  // B[k][n] = Lnx[n][k]
-#pragma unroll
-                for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                    for (int nj = 0; nj < 2; ++nj)
-                        dmma_8x8x4(tacc[mi][nj][0], tacc[mi][nj][1], a[mi], b[nj]);
             }
-#pragma unroll
-            for (int nj = 0; nj < 2; ++nj)
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int c = 8 * nj + 2 * c4 + e;
-                    if (c < kb1) {
-                        const int o = poff(n0 + c, Mp);
-#pragma unroll
-                        for (int mi = 0; mi < 2; ++mi) {
-                            const int i = i0 + 8 * mi + r8;
-                            if (i < Mp) A[o + i] -= tacc[mi][nj][e];
-                        }
-                    }
-                }
         }
-    }
 }
 
-// Blocked right-looking Cholesky of the first M columns of the packed
-// (M+1)-row system.  Per 16-wide panel p: warp 0 applies panels p-2, p-1 to
-// the diagonal block and factors it together with the rows of panel p+1;
-// meanwhile the warps outside sub-partition 0 apply panel p-1 to the
-// columns beyond panel p+1's diagonal block.  Then all warps solve the rows
-// below panel p+1 and update panel p+1's columns.  Two barriers per panel.
-__device__ __forceinline__ void cholesky_pipelined(double *A, int M, int mc, BlockShared &sh)
+// Roles (512 threads): warp 0 walks the diagonal; warp 4 (the same SM
+// sub-partition, idle while warp 0 computes and vice versa) handles the
+// critical rows; the 12 warps of sub-partitions 1-3 do the bulk work;
+// warps 8 and 12 stay out of the way of warps 0 and 4.
+constexpr int kCritWarp = 4;
+constexpr int kBulkWarps = kWarps - kWarps / 4;  // warps with (warp & 3) != 0
+
+__device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShared &sh)
 {
     const int Mp = M + 1;
     const int P = (M + kNB - 1) / kNB;
-    const int warp = threadIdx.x >> 5;
-    for (int p = 0; p < P; ++p) {
-        const int k0 = p * kNB, kb = min(kNB, M - k0);
-        const int n0 = k0 + kb;             // first column of panel p+1
-        const int kb1 = max(0, min(kNB, M - n0));
-        const int n1 = n0 + kb1;            // end of panel p+1
-        if (warp == 0) {
-            if (p > 0) update_diag_block(A, Mp, k0, kb, p);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const unsigned base = sh.phase_base;
+    bool timed_out = false;
+    if (warp == 0) {
+        for (int p = 0; p < P; ++p) {
+            const int k0 = p * kNB, kb = min(kNB, M - k0);
+            const int n0 = k0 + kb;
+            const int kb1 = max(0, min(kNB, M - n0));
+            if (p > 0) {
+                // Panels p-2 and p-1 on the diagonal block (their rows here are
+                // final: panel p-1's were stored below, panel p-2's by the
+                // critical rows of two panels ago), then the rows below.
+                update_diag_block(A, Mp, k0, kb, p);
+                __syncwarp();
+                if (!mbar_wait_bounded(&sh.bar_crit, (base + p - 1) & 1u)) timed_out = true;
+            }
+            double v[kNB];
+            double myinv;
+            const unsigned st = factor_diag_regs(A, Mp, k0, kb, n0, kb1, mc, v, myinv);
+            if (p > 0 && !mbar_wait_bounded(&sh.bar_free, (base + p - 1) & 1u)) timed_out = true;
+            publish_diag(sh, v, myinv, kb, kb1);
+            if (lane == 0 && st) atomicOr(&sh.status, st);
+            __threadfence_block();
             __syncwarp();
-            const unsigned st = factor_diag(A, Mp, k0, kb, n0, kb1, mc, sh);
-            if (threadIdx.x == 0 && st) sh.status |= st;
-        } else if (p > 0 && (warp & 3) != 0) {
-            update_cols<2>(A, Mp, k0 - kNB, kNB, n0, M, true, n1);
+            if (lane == 0) mbar_arrive(&sh.bar_lready);
+            // Panel p+1's rows in panel p's columns, for the next diagonal update.
+            if (lane >= kNB && lane - kNB < kb1) {
+#pragma unroll
+                for (int c = 0; c < kNB; ++c)
+                    if (c < kb) A[poff(k0 + c, Mp) + n0 + (lane - kNB)] = v[c];
+            }
+            __syncwarp();
         }
-        __syncthreads();
-        store_diag(A, Mp, k0, kb, n0, kb1, sh);
-        panel_rows_pass(A, Mp, k0, kb, n0, kb1, n1, sh);
-        __syncthreads();
+    } else if (warp == kCritWarp) {
+        for (int p = 0; p < P; ++p) {
+            const int k0 = p * kNB, kb = min(kNB, M - k0);
+            const int n0 = k0 + kb;
+            const int kb1 = max(0, min(kNB, M - n0));
+            const int n1 = n0 + kb1;
+            const int n2 = min(Mp, n1 + kNB);
+            if (!mbar_wait_bounded(&sh.bar_lready, (base + p) & 1u)) timed_out = true;
+            // The 16 rows below panel p+1: solved in panel p, then brought up
+            // to date in panel p+1's columns (panels p and p-1).
+            solve_rows(A, Mp, k0, kb, n1, n2 - n1, sh);
+            __syncwarp();
+            if (kb1 > 0 && n2 > n1) update_next_rows16(A, Mp, k0, kb, n0, kb1, n1, p > 0, sh);
+            __threadfence_block();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sh.bar_crit);
+        }
+    } else if ((warp & 3) != 0) {
+        const int wb = warp - (warp >> 2) - 1, nwb = kBulkWarps;
+        for (int p = 0; p < P; ++p) {
+            const int k0 = p * kNB, kb = min(kNB, M - k0);
+            const int n0 = k0 + kb;
+            const int kb1 = max(0, min(kNB, M - n0));
+            const int n1 = n0 + kb1;
+            const int n2 = min(Mp, n1 + kNB);
+            if (!mbar_wait_bounded(&sh.bar_lready, (base + p) & 1u)) timed_out = true;
+            // The factored diagonal block into A.
+            {
+                const int t = wb * 32 + lane;
+                if (t < kNB * kNB) {
+                    const int c = t >> 4, r = t & 15;
+                    if (c < kb && r < kb && r >= c) A[poff(k0 + c, Mp) + k0 + r] = sh.Lt[c][r];
+                }
+            }
+            // Rows >= n2 in 32-row groups (solve, then panel p+1's columns take
+            // panels p and p-1), then panel p-1 on the columns beyond panel p+1.
+            const int G = (Mp > n2) ? (Mp - n2 + 31) >> 5 : 0;
+            int item = 0;
+            for (int g = 0; g < G; ++g, ++item) {
+                if (item % nwb != wb) continue;
+                const int rb = n2 + 32 * g;
+                solve_rows(A, Mp, k0, kb, rb, 32, sh);
+                __syncwarp();
+                if (kb1 > 0) {
+                    update_next_rows16(A, Mp, k0, kb, n0, kb1, rb, p > 0, sh);
+                    if (rb + 16 < Mp) update_next_rows16(A, Mp, k0, kb, n0, kb1, rb + 16, p > 0, sh);
+                }
+            }
+            if (p > 0 && M > n1) {
+                const int TR = (Mp - n1 + 31) >> 5, TC = (M - n1 + 15) >> 4;
+                for (int tc = 0; tc < TC; ++tc) {
+                    const int j0 = n1 + tc * 16;
+                    for (int tr = (j0 - n1) >> 5; tr < TR; ++tr, ++item) {
+                        if (item % nwb != wb) continue;
+                        mma_tile<4, 2, kNB>(A, Mp, k0 - kNB, kNB, n1 + (tr << 5), j0, M, 0);
+                    }
+                }
+            }
+            __threadfence_block();
+            asm volatile("bar.sync 1, %0;" ::"n"(kBulkWarps * 32) : "memory");
+            if (tid == 32) mbar_arrive(&sh.bar_free);
+        }
     }
+    if (timed_out) atomicOr(&sh.status, kStDeviceTimeout);
+    __syncthreads();
+    if (tid == 0) sh.phase_base = base + (unsigned)P;
 }
 
 // One block, with its matrix at A (shared memory or the global slab).
@@ -498,7 +662,7 @@ __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternPara
 
     // Cholesky of the first M columns; row M rides along as the
     // forward-substitution right-hand side.
-    cholesky_pipelined(A, M, mc, sh);
+    cholesky_ws(A, M, mc, sh);
 
     // log det of the conditional factor (positive pivots only, as
     // core_Xlogdet) and |u|^2 from row M.

@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(kThreads, 1) llh_fp64_server_kernel(const JobD
     __shared__ BlockShared sh;
     __shared__ int s_last;
     const int tid = threadIdx.x;
+    init_block_sync(sh);
     for (;;) {
         if (tid == 0) sh.task = (int)atomicAdd(counter, 1u);
         __syncthreads();
