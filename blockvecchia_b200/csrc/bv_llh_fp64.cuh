@@ -247,16 +247,20 @@ __device__ __forceinline__ unsigned factor_diag_regs(const double *A, int Mp, in
     // Lagged Crout: the sum for pivot q over k < q-1 was formed while pivot
     // q-1's reciprocal square root was in flight; only the k = q-1 term (row q
     // of L by one shuffle) stays on the dependent chain.
+    // Every lane also forms the pivot itself from lane q's partial sum
+    // (broadcast early) and L_{q,q-1}, with the operands lane q uses, so the
+    // pivot needs no second shuffle on the chain.
     double pre = v[0];
 #pragma unroll
     for (int q = 0; q < kNB; ++q) {
         if (q < kb) {
-            double s = pre;
+            const double preq = __shfl_sync(0xffffffffu, pre, q);
+            double s = pre, piv = preq;
             if (q > 0) {
                 const double l = __shfl_sync(0xffffffffu, v[q - 1], q);
                 s = fma(-v[q - 1], l, s);
+                piv = fma(-l, l, preq);
             }
-            const double piv = __shfl_sync(0xffffffffu, s, q);
             const bool ok = piv > 0.0;
             const double inv = ok ? rsqrt(piv) : 0.0;
             if (q + 1 < kNB) {
@@ -558,7 +562,8 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
             if (p > 0 && !mbar_wait_bounded(&sh.bar_free, (base + p - 1) & 1u)) timed_out = true;
             publish_diag(sh, v, myinv, kb, kb1);
             if (lane == 0 && st) atomicOr(&sh.status, st);
-            __threadfence_block();
+            // __syncwarp orders the lanes' writes before lane 0's arrive, whose
+            // release semantics (CTA scope) publish them to the waiters.
             __syncwarp();
             if (lane == 0) mbar_arrive(&sh.bar_lready);
             // Panel p+1's rows in panel p's columns, for the next diagonal update.
@@ -582,7 +587,6 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
             solve_rows(A, Mp, k0, kb, n1, n2 - n1, sh);
             __syncwarp();
             if (kb1 > 0 && n2 > n1) update_next_rows16(A, Mp, k0, kb, n0, kb1, n1, p > 0, sh);
-            __threadfence_block();
             __syncwarp();
             if (lane == 0) mbar_arrive(&sh.bar_crit);
         }
@@ -627,7 +631,6 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
                     }
                 }
             }
-            __threadfence_block();
             asm volatile("bar.sync 1, %0;" ::"n"(kBulkWarps * 32) : "memory");
             if (tid == 32) mbar_arrive(&sh.bar_free);
         }
