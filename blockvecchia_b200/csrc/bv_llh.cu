@@ -611,6 +611,7 @@ static int fill_params(bv_handle *h, const double *theta)
     p.inv_ds = 1.0 / h->opts.dist_scale;
     p.nu_kind = (nu == 0.5) ? kNuHalf : (nu == 1.5) ? kNuThreeHalves : (nu == 2.5) ? kNuFiveHalves
                                                                                   : kNuGeneral;
+    matern_prepare(p);
     return BV_OK;
 }
 
@@ -891,6 +892,7 @@ extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *ob
     mp.inv_ds = 1.0 / dist_scale;
     mp.nu_kind = (nu == 0.5) ? kNuHalf : (nu == 1.5) ? kNuThreeHalves : (nu == 2.5) ? kNuFiveHalves
                                                                                   : kNuGeneral;
+    matern_prepare(mp);
     MaternParams *d_mp = reinterpret_cast<MaternParams *>(base + kNaParams);
     BV_CUDA_TRY(cudaMemcpyAsync(d_mp, &mp, sizeof(mp), cudaMemcpyHostToDevice, s));
     // The work counter must start at zero; per-block results are fully

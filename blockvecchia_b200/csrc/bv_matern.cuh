@@ -7,15 +7,18 @@
 //   C = (r == 0) ? sigma2 : con * r^nu * K_nu(r),  con = sigma2/(2^(nu-1) Gamma(nu))
 // with closed forms for nu = 1/2, 3/2, 5/2:
 //   sigma2 e^-r,  sigma2 (1+r) e^-r,  sigma2 (1 + r + r^2/3) e^-r.
-// General nu uses the FP64 K_nu below: Temme's series (N. M. Temme,
-// J. Comput. Phys. 19 (1975) 324-337) for x <= 2 with upward recurrence,
-// and the trapezoidal rule on K_nu(x) = int_0^inf exp(-x cosh t) cosh(nu t) dt
-// for x > 2 (exponentially convergent: the integrand is analytic in
-// |Im t| < pi/2).
+// General nu uses the FP64 K_nu below, by the methods GSL's K_nu uses: for
+// nu = mu + n, |mu| <= 1/2, Temme's series for K_mu, K_mu+1 at x < 2 and
+// Steed's algorithm for Temme's continued fraction at x >= 2 (N. M. Temme,
+// J. Comput. Phys. 19 (1975) 324-337), then upward recurrence in the order.
+// Everything that depends on mu only (Gamma-function combinations, the
+// series' constant factors) is computed on the host once per evaluation.
 #pragma once
 
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <cmath>
 
 namespace bv {
 
@@ -32,73 +35,89 @@ struct MaternParams {
     double inv_ds;      // RN(1 / dist_scale), host-computed
     int nu_kind;        // NuKind
     int scale_is_one;   // dist_scale == 1.0: the second division is exact and skipped
+    // General nu (matern_prepare): nu = mu + nn, |mu| <= 1/2.
+    int nn;
+    double mu;
+    double g1, g2;      // Temme's gamma_1(mu), gamma_2(mu)
+    double gam_p;       // Gamma(1 + mu)
+    double gam_m;       // Gamma(1 - mu)
+    double fact;        // pi mu / sin(pi mu)
 };
 
-// Taylor coefficients of 1/Gamma(1+z) at 0 (mpmath, 40 digits; the same
-// table oracle/gen_rgamma_coeffs.py prints).
-__device__ __constant__ static const double kRGammaA[30] = {
-    1.0,
-    5.77215664901532860607e-1,
-    -6.55878071520253881077e-1,
-    -4.2002635034095235529e-2,
-    1.66538611382291489502e-1,
-    -4.21977345555443367482e-2,
-    -9.62197152787697356211e-3,
-    7.2189432466630995424e-3,
-    -1.16516759185906511211e-3,
-    -2.15241674114950972816e-4,
-    1.28050282388116186153e-4,
-    -2.01348547807882386557e-5,
-    -1.25049348214267065735e-6,
-    1.13302723198169588237e-6,
-    -2.05633841697760710345e-7,
-    6.11609510448141581786e-9,
-    5.00200764446922293006e-9,
-    -1.18127457048702014459e-9,
-    1.04342671169110051049e-10,
-    7.78226343990507125405e-12,
-    -3.69680561864220570819e-12,
-    5.10037028745447597902e-13,
-    -2.05832605356650678322e-14,
-    -5.34812253942301798237e-15,
-    1.22677862823826079016e-15,
-    -1.18125930169745876951e-16,
-    1.18669225475160033258e-18,
-    1.41238065531803178156e-18,
-    -2.29874568443537020659e-19,
-    1.71440632192733743338e-20,
-};
-
-// K_mu(x), K_{mu+1}(x) for |mu| <= 1/2 and 0 < x <= 2 (Temme's series).
-__device__ __forceinline__ void temme_series(double mu, double x, double &kmu, double &kmu1)
+// Host: the mu-only constants of the general-nu K_nu.  1/Gamma(1+z) by its
+// Taylor series at 0 (coefficients from mpmath, 40 digits; the same table
+// oracle/gen_rgamma_coeffs.py prints), which keeps gamma_1 = (1/Gamma(1-mu) -
+// 1/Gamma(1+mu)) / (2 mu) accurate as mu -> 0.
+inline void matern_prepare(MaternParams &p)
 {
+    static const double a[30] = {
+        1.0, 5.77215664901532860607e-1, -6.55878071520253881077e-1, -4.2002635034095235529e-2,
+        1.66538611382291489502e-1, -4.21977345555443367482e-2, -9.62197152787697356211e-3,
+        7.2189432466630995424e-3, -1.16516759185906511211e-3, -2.15241674114950972816e-4,
+        1.28050282388116186153e-4, -2.01348547807882386557e-5, -1.25049348214267065735e-6,
+        1.13302723198169588237e-6, -2.05633841697760710345e-7, 6.11609510448141581786e-9,
+        5.00200764446922293006e-9, -1.18127457048702014459e-9, 1.04342671169110051049e-10,
+        7.78226343990507125405e-12, -3.69680561864220570819e-12, 5.10037028745447597902e-13,
+        -2.05832605356650678322e-14, -5.34812253942301798237e-15, 1.22677862823826079016e-15,
+        -1.18125930169745876951e-16, 1.18669225475160033258e-18, 1.41238065531803178156e-18,
+        -2.29874568443537020659e-19, 1.71440632192733743338e-20};
+    const double nu = p.nu < 0 ? -p.nu : p.nu;
+    p.nn = (int)std::floor(nu + 0.5);
+    const double mu = nu - (double)p.nn;
+    p.mu = mu;
     const double m2 = mu * mu;
     double odd = 0.0, even = 0.0;
-#pragma unroll
-    for (int j = 29; j >= 1; j -= 2) odd = fma(odd, m2, kRGammaA[j]);
-#pragma unroll
-    for (int j = 28; j >= 0; j -= 2) even = fma(even, m2, kRGammaA[j]);
-    const double g1 = -odd, g2 = even;
-    const double rg_p = g2 - mu * g1;  // 1/Gamma(1+mu)
-    const double rg_m = g2 + mu * g1;  // 1/Gamma(1-mu)
-    const double lx = log(2.0 / x);
-    const double sigma = mu * lx;
+    for (int j = 29; j >= 1; j -= 2) odd = std::fma(odd, m2, a[j]);
+    for (int j = 28; j >= 0; j -= 2) even = std::fma(even, m2, a[j]);
+    p.g1 = -odd;
+    p.g2 = even;
+    p.gam_p = 1.0 / (p.g2 - mu * p.g1);  // 1 / (1/Gamma(1+mu))
+    p.gam_m = 1.0 / (p.g2 + mu * p.g1);
     const double pimu = 3.141592653589793 * mu;
-    const double fact = (fabs(pimu) < 1e-300) ? 1.0 : pimu / sin(pimu);
-    const double shs = (fabs(sigma) < 1e-300) ? 1.0 : sinh(sigma) / sigma;
-    double f = fact * (g1 * cosh(sigma) + g2 * lx * shs);
+    p.fact = (std::fabs(pimu) < 1e-300) ? 1.0 : pimu / std::sin(pimu);
+}
+
+// K_mu(x), K_{mu+1}(x) for |mu| <= 1/2 and 0 < x < 2 (Temme's series), with
+// lx = log(2/x) and ix = 1/x from the caller.  One reciprocal per term:
+// 1/(k - mu) = (k + mu) / (k^2 - mu^2) and likewise 1/(k + mu).
+__device__ __forceinline__ void temme_series(double x, double lx, double ix, const MaternParams &mp,
+                                             double &kmu, double &kmu1)
+{
+    const double mu = mp.mu;
+    const double m2 = mu * mu;
+    const double sigma = mu * lx;
     const double e = exp(sigma);  // (x/2)^(-mu)
-    double p = 0.5 * e / rg_p;
-    double q = 0.5 / (e * rg_m);
+    const double ie = 1.0 / e;
+    const double ch = 0.5 * (e + ie);
+    double shs;                   // sinh(sigma) / sigma
+    if (fabs(sigma) < 0.5) {
+        // sum_k sigma^(2k) / (2k+1)!, truncated below 1e-19 relative
+        const double s2 = sigma * sigma;
+        double t = 1.0 / 355687428096000.0;  // 1/17!
+        t = fma(t, s2, 1.0 / 1307674368000.0);
+        t = fma(t, s2, 1.0 / 6227020800.0);
+        t = fma(t, s2, 1.0 / 39916800.0);
+        t = fma(t, s2, 1.0 / 362880.0);
+        t = fma(t, s2, 1.0 / 5040.0);
+        t = fma(t, s2, 1.0 / 120.0);
+        t = fma(t, s2, 1.0 / 6.0);
+        shs = fma(t, s2, 1.0);
+    } else {
+        shs = 0.5 * (e - ie) / sigma;
+    }
+    double f = mp.fact * (mp.g1 * ch + mp.g2 * lx * shs);
+    double p = 0.5 * e * mp.gam_p;
+    double q = 0.5 * ie * mp.gam_m;
     double c = 1.0;
     const double d = 0.25 * x * x;
     double s0 = f, s1 = p;
     for (int k = 1; k < 200; ++k) {
         const double kk = (double)k;
-        f = (kk * f + p + q) / (kk * kk - m2);
+        const double r = 1.0 / fma(kk, kk, -m2);
+        f = (kk * f + p + q) * r;
         c *= d / kk;
-        p /= (kk - mu);
-        q /= (kk + mu);
+        p *= (kk + mu) * r;
+        q *= (kk - mu) * r;
         const double t0 = c * f;
         const double t1 = c * (p - kk * f);
         s0 += t0;
@@ -106,47 +125,61 @@ __device__ __forceinline__ void temme_series(double mu, double x, double &kmu, d
         if (fabs(t0) < 1e-17 * fabs(s0) && fabs(t1) < 1e-17 * fabs(s1)) break;
     }
     kmu = s0;
-    kmu1 = s1 * 2.0 / x;
+    kmu1 = s1 * 2.0 * ix;
 }
 
-// exp(x) K_nu(x), x > 2, trapezoidal rule (step follows the 1/sqrt(x) peak).
-__device__ __forceinline__ double besselk_scaled_trap(double nu, double x)
+// K_mu(x) and K_{mu+1}(x) for x >= 2, |mu| <= 1/2: Steed's algorithm for
+// Temme's continued fraction (N. M. Temme, J. Comput. Phys. 19 (1975)
+// 324-337), the method GSL's K_nu uses for x >= 2.  The fraction for
+// K_{mu+1}/K_mu and the series normalising K_mu are summed together; a few
+// dozen iterations of plain arithmetic, one exp and one sqrt.
+__device__ __forceinline__ void steed_cf2(double mu, double x, double &kmu, double &kmu1)
 {
-    double h = 0.6 * rsqrt(x);
-    if (h > 0.125) h = 0.125;
-    double sum = 0.5;
-    for (int k = 1; k < 4000; ++k) {
-        const double t = h * (double)k;
-        const double sh = sinh(0.5 * t);
-        const double expo = -2.0 * x * sh * sh;
-        const double a = expo + nu * t;
-        sum += exp(a) * 0.5 * (1.0 + exp(-2.0 * nu * t));
-        if (a < -45.0) break;
+    const double a1 = 0.25 - mu * mu;
+    double b = 2.0 * (1.0 + x);
+    double d = 1.0 / b;
+    double h = d, delh = d;
+    double q1 = 0.0, q2 = 1.0;
+    double q = a1, c = a1, a = -a1;
+    double s = 1.0 + q * delh;
+    for (int i = 2; i < 20000; ++i) {
+        a -= 2.0 * (double)(i - 1);
+        c = -a * c / (double)i;
+        const double qn = (q1 - b * q2) / a;
+        q1 = q2;
+        q2 = qn;
+        q += c * qn;
+        b += 2.0;
+        d = 1.0 / (b + a * d);
+        delh = (b * d - 1.0) * delh;
+        h += delh;
+        const double dels = q * delh;
+        s += dels;
+        if (fabs(dels) < 1e-17 * fabs(s)) break;
     }
-    return h * sum;
+    h = a1 * h;
+    kmu = sqrt(3.14159265358979323846 / (2.0 * x)) * exp(-x) / s;
+    kmu1 = kmu * (mu + x + 0.5 - h) / x;
 }
 
-static __device__ __noinline__ double besselk(double nu, double x)
+// con * r^nu * K_nu(r) for general nu (out of line: long and rare).
+static __device__ __noinline__ double matern_general(double r, const MaternParams &mp)
 {
-    nu = fabs(nu);
-    if (x > 2.0) return besselk_scaled_trap(nu, x) * exp(-x);
-    const int nn = (int)floor(nu + 0.5);
-    const double mu = nu - (double)nn;
+    const double lr = log(r);
+    const double ix = 1.0 / r;
     double k0, k1;
-    temme_series(mu, x, k0, k1);
-    for (int j = 1; j <= nn; ++j) {
-        const double m = mu + (double)j;
-        const double k2 = 2.0 * m / x * k1 + k0;
+    if (r < 2.0)
+        temme_series(r, 0.6931471805599453094 - lr, ix, mp, k0, k1);
+    else
+        steed_cf2(mp.mu, r, k0, k1);
+    for (int j = 1; j <= mp.nn; ++j) {
+        const double m = mp.mu + (double)j;
+        const double k2 = 2.0 * m * ix * k1 + k0;
         k0 = k1;
         k1 = k2;
     }
-    return k0;
-}
-
-// General nu: con * r^nu * K_nu(r) (kept out of line; it is long and rare).
-static __device__ __noinline__ double matern_general(double r, double con, double nu)
-{
-    return con * pow(r, nu) * besselk(nu, r);
+    const double nu = mp.nu < 0 ? -mp.nu : mp.nu;
+    return mp.con * exp(nu * lr) * k0;
 }
 
 // a / b from the correctly rounded reciprocal y = RN(1/b) with one
@@ -184,7 +217,7 @@ __device__ __forceinline__ double matern_from_r(double r, const MaternParams &p)
     case kNuFiveHalves:
         return p.sigma2 * (fma(r, r * (1.0 / 3.0), 1.0 + r) * exp(-r));
     default:
-        return matern_general(r, p.con, p.nu);
+        return matern_general(r, p);
     }
 }
 
@@ -192,28 +225,6 @@ __device__ __forceinline__ double matern(double x1, double y1, double x2, double
                                          const MaternParams &p)
 {
     return matern_from_r(matern_r(x1, y1, x2, y2, p), p);
-}
-
-// FP32 variant for the mixed path (diagonal scaled by 1/sigma2: returns C/sigma2).
-__device__ __forceinline__ float matern_unit_f32(float x1, float y1, float x2, float y2,
-                                                 float inv_range, const MaternParams &p)
-{
-    const float dx = x2 - x1;
-    const float dy = y2 - y1;
-    const float r = sqrtf(fmaf(dx, dx, dy * dy)) * inv_range;
-    if (r == 0.0f) return 1.0f;
-    switch (p.nu_kind) {
-    case kNuHalf:
-        return __expf(-r);
-    case kNuThreeHalves:
-        return (1.0f + r) * __expf(-r);
-    case kNuFiveHalves:
-        return fmaf(r, r * (1.0f / 3.0f), 1.0f + r) * __expf(-r);
-    default: {
-        const double rd = (double)r;
-        return (float)(p.con / p.sigma2 * pow(rd, p.nu) * besselk(p.nu, rd));
-    }
-    }
 }
 
 }  // namespace bv

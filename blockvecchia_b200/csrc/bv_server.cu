@@ -272,6 +272,7 @@ void fill_params(MaternParams &p, const double *theta, double dist_scale)
     p.inv_ds = 1.0 / dist_scale;
     p.nu_kind = (nu == 0.5) ? kNuHalf : (nu == 1.5) ? kNuThreeHalves : (nu == 2.5) ? kNuFiveHalves
                                                                                   : kNuGeneral;
+    matern_prepare(p);
 }
 
 // Requests of admitted jobs are ready to run.

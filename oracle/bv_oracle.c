@@ -112,36 +112,51 @@ static void bvo_temme_series(double mu, double x, double *kmu, double *kmu1)
     *kmu1 = sum1 * 2.0 / x;
 }
 
-/* exp(x) K_nu(x) for x > 2 by the trapezoidal rule with step h on
- * int_0^inf exp(-x (cosh t - 1)) cosh(nu t) dt.  The integrand is analytic in
- * |Im t| < pi/2, so the rule converges like exp(-pi^2 / h); for large x the
- * peak at t = 0 narrows like 1/sqrt(x) and the step follows it
- * (aliasing error ~ exp(-2 pi^2 / (x h^2))). */
-static double bvo_besselk_scaled_trap(double nu, double x)
+/* K_mu(x) and K_{mu+1}(x) for x >= 2, |mu| <= 1/2, by Steed's algorithm for
+ * Temme's continued fraction (N. M. Temme, J. Comput. Phys. 19 (1975)
+ * 324-337; the method GSL's gsl_sf_bessel_Knu uses for x >= 2): the CF for
+ * K_{mu+1}/K_mu is summed by Steed's recurrence together with the series
+ * that normalises K_mu, so K_mu = sqrt(pi / (2x)) exp(-x) / s. */
+static void bvo_steed_cf2(double mu, double x, double *kmu, double *kmu1)
 {
-    double h = 0.6 / sqrt(x);
-    if (h > 0.125) h = 0.125;
-    double sum = 0.5; /* t = 0 term: exp(0) cosh(0) / 2 */
-    for (int k = 1; k < 4000; ++k) {
-        double t = h * (double)k;
-        double sh = sinh(0.5 * t);
-        double expo = -2.0 * x * sh * sh; /* -x (cosh t - 1) */
-        double term = exp(expo + nu * t) * 0.5 * (1.0 + exp(-2.0 * nu * t));
-        sum += term;
-        if (expo + nu * t < -45.0) break;
+    const double a1 = 0.25 - mu * mu;
+    double b = 2.0 * (1.0 + x);
+    double d = 1.0 / b;
+    double h = d, delh = d;
+    double q1 = 0.0, q2 = 1.0;
+    double q = a1, c = a1, a = -a1;
+    double s = 1.0 + q * delh;
+    for (int i = 2; i < 20000; ++i) {
+        a -= 2.0 * (double)(i - 1);
+        c = -a * c / (double)i;
+        const double qn = (q1 - b * q2) / a;
+        q1 = q2;
+        q2 = qn;
+        q += c * qn;
+        b += 2.0;
+        d = 1.0 / (b + a * d);
+        delh = (b * d - 1.0) * delh;
+        h += delh;
+        const double dels = q * delh;
+        s += dels;
+        if (fabs(dels) < 1e-17 * fabs(s)) break;
     }
-    return h * sum;
+    h = a1 * h;
+    *kmu = sqrt(3.14159265358979323846 / (2.0 * x)) * exp(-x) / s;
+    *kmu1 = *kmu * (mu + x + 0.5 - h) / x;
 }
 
 double bvo_besselk(double nu, double x)
 {
     if (!(x > 0.0)) return (x == 0.0) ? INFINITY : NAN;
     nu = fabs(nu);
-    if (x > 2.0) return bvo_besselk_scaled_trap(nu, x) * exp(-x);
     int nn = (int)floor(nu + 0.5);
     double mu = nu - (double)nn;
     double k0, k1;
-    bvo_temme_series(mu, x, &k0, &k1);
+    if (x < 2.0)
+        bvo_temme_series(mu, x, &k0, &k1);
+    else
+        bvo_steed_cf2(mu, x, &k0, &k1);
     /* Upward recurrence K_{m+1} = 2 m / x K_m + K_{m-1}, m = mu+1 .. nu-1. */
     for (int j = 1; j <= nn; ++j) {
         double m = mu + (double)j;
