@@ -171,50 +171,89 @@ __device__ __forceinline__ void init_block_sync(BlockShared &sh)
 // Matern generation.
 // ---------------------------------------------------------------------------
 
-// Lower triangle of rows 0..M-1 with columns paired (q, M-1-q) so each pair
-// holds M+1 entries; warp w takes pairs w, w+16, ...; a lane computes four
-// entries of a pair at a time.
-__device__ __forceinline__ void generate(double *A, const double *X, const double *Y, int M,
-                                         const MaternParams &mp)
+// Lower triangle of rows 0..M-1 with columns paired (q, M-1-q), so each pair
+// holds M+1 entries (the middle column of an odd M only M-q).  The pairs'
+// entries form one flat index space dealt to the warps in chunks of 32 x
+// kGenU, so only the last chunk is partial; a lane computes kGenU entries at a
+// time, branch-free (entries past the end are clamped and dropped) and with
+// the smoothness dispatch hoisted out of the loop, so the independent exp
+// chains interleave.
+constexpr int kGenU = 6;
+
+template <int KIND>
+__device__ __forceinline__ double matern_kind(double x1, double y1, double x2, double y2,
+                                              const MaternParams &mp)
+{
+    const double r = matern_r(x1, y1, x2, y2, mp);
+    if (KIND == kNuGeneral) return (r == 0.0) ? mp.sigma2 : matern_general(r, mp);
+    const double e = exp(-r);
+    double c;
+    if (KIND == kNuHalf)
+        c = e;
+    else if (KIND == kNuThreeHalves)
+        c = (1.0 + r) * e;
+    else
+        c = fma(r, r * (1.0 / 3.0), 1.0 + r) * e;
+    return (r == 0.0) ? mp.sigma2 : mp.sigma2 * c;
+}
+
+template <int KIND>
+__device__ __forceinline__ void generate_t(double *A, const double *X, const double *Y, int M,
+                                           const MaternParams &mp)
 {
     const int Mp = M + 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int half = (M + 1) >> 1;
-    for (int q = warp; q < half; q += kWarps) {
-        const int jb = M - 1 - q;          // partner column
-        const int na = M - q;              // rows q..M-1 of column q
-        const int nt = (jb == q) ? na : M + 1;
-        const int oa = poff(q, Mp), ob = poff(jb, Mp);
-        const double xq = X[q], yq = Y[q], xb = X[jb], yb = Y[jb];
-        for (int r0 = lane; r0 < nt; r0 += 128) {
-            double v[4];
-            int dst[4];
+    const int total = half * Mp;
+    for (int e0 = (warp * kGenU * 32) + lane; e0 < total; e0 += kWarps * kGenU * 32) {
+        int q = e0 / Mp;
+        int rr0 = e0 - q * Mp;
+        double v[kGenU];
+        int dst[kGenU];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int rr = r0 + 32 * u;
-                dst[u] = -1;
-                v[u] = 0.0;
-                if (rr < nt) {
-                    int i;
-                    double xj, yj;
-                    if (rr < na) {
-                        i = q + rr;
-                        xj = xq;
-                        yj = yq;
-                        dst[u] = oa + i;
-                    } else {
-                        i = jb + (rr - na);
-                        xj = xb;
-                        yj = yb;
-                        dst[u] = ob + i;
-                    }
-                    v[u] = matern(X[i], Y[i], xj, yj, mp);
+        for (int u = 0; u < kGenU; ++u) {
+            if (u > 0) {
+                rr0 += 32;
+                while (rr0 >= Mp) {
+                    rr0 -= Mp;
+                    ++q;
                 }
             }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (dst[u] >= 0) A[dst[u]] = v[u];
+            const int jb = M - 1 - q;
+            const int na = M - q;  // rows q..M-1 of column q
+            const int nt = (jb == q) ? na : Mp;
+            const bool valid = q < half && rr0 < nt;
+            const int qq = valid ? q : 0;
+            const int rr = valid ? rr0 : 0;
+            const int jbb = M - 1 - qq, naa = M - qq;
+            const bool first = rr < naa;
+            const int i = first ? qq + rr : jbb + (rr - naa);
+            const int j = first ? qq : jbb;
+            dst[u] = valid ? poff(j, Mp) + i : -1;
+            v[u] = matern_kind<KIND>(X[i], Y[i], X[j], Y[j], mp);
         }
+#pragma unroll
+        for (int u = 0; u < kGenU; ++u)
+            if (dst[u] >= 0) A[dst[u]] = v[u];
+    }
+}
+
+__device__ __forceinline__ void generate(double *A, const double *X, const double *Y, int M,
+                                         const MaternParams &mp)
+{
+    switch (mp.nu_kind) {
+    case kNuHalf:
+        generate_t<kNuHalf>(A, X, Y, M, mp);
+        break;
+    case kNuThreeHalves:
+        generate_t<kNuThreeHalves>(A, X, Y, M, mp);
+        break;
+    case kNuFiveHalves:
+        generate_t<kNuFiveHalves>(A, X, Y, M, mp);
+        break;
+    default:
+        generate_t<kNuGeneral>(A, X, Y, M, mp);
+        break;
     }
 }
 
