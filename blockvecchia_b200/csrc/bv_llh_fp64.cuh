@@ -464,7 +464,8 @@ __device__ __forceinline__ void update_diag_block(double *A, int Mp, int k0, int
 // Lanes < nl solve rows base+lane of panel p against L_pp (sh.Lt, sh.inv):
 // forward substitution, column q of L_pp read per stage as eight 16-byte
 // broadcasts behind a compiler fence so the factor values are not all
-// hoisted into registers.
+// hoisted into registers.  The two values on the dependent chain of step
+// q + 1 (1 / L_{q+1,q+1} and L_{q+2,q+1}) are read one step ahead.
 __device__ __forceinline__ void solve_rows(double *A, int Mp, int k0, int kb, int base, int nl,
                                            const BlockShared &sh)
 {
@@ -477,17 +478,24 @@ __device__ __forceinline__ void solve_rows(double *A, int Mp, int k0, int kb, in
     double w[kNB];
 #pragma unroll
     for (int c = 0; c < kNB; ++c) w[c] = (c < kb) ? A[cof[c] + r] : 0.0;
+    double inv_q = sh.inv[0];
+    double l_next = sh.Lt[0][1];
 #pragma unroll
     for (int q = 0; q < kNB; ++q) {
         if (q < kb) {
             asm volatile("" ::: "memory");
+            const double inv_cur = inv_q;
+            const double l_cur = l_next;
+            if (q + 1 < kNB) inv_q = sh.inv[q + 1];
+            if (q + 2 < kNB) l_next = sh.Lt[q + 1][q + 2];
             double2 col[kNB / 2];
             const double2 *src = reinterpret_cast<const double2 *>(sh.Lt[q]);
 #pragma unroll
-            for (int h = 0; h < kNB / 2; ++h) col[h] = src[h];
-            w[q] *= sh.inv[q];
+            for (int h = (q + 2) >> 1; h < kNB / 2; ++h) col[h] = src[h];
+            w[q] *= inv_cur;
+            if (q + 1 < kNB) w[q + 1] = fma(-w[q], l_cur, w[q + 1]);
 #pragma unroll
-            for (int c = q + 1; c < kNB; ++c) {
+            for (int c = q + 2; c < kNB; ++c) {
                 const double l = (c & 1) ? col[c >> 1].y : col[c >> 1].x;
                 w[c] = fma(-w[q], l, w[c]);
             }
