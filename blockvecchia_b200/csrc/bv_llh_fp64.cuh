@@ -150,6 +150,7 @@ struct alignas(16) BlockShared {
     uint64_t bar_crit;          // warp 1 -> warp 0: the rows warp 0 needs next are done
     uint64_t bar_free;          // warps 1..15 -> warp 0: Lt/Lnx/inv may be overwritten
     unsigned phase_base;        // panels completed by this CTA (parity of the barriers)
+    int bulk_next[2];           // next bulk work item of panels with even / odd index
     unsigned status;
     int task;
 };
@@ -162,6 +163,7 @@ __device__ __forceinline__ void init_block_sync(BlockShared &sh)
         mbar_init(&sh.bar_crit, 1);
         mbar_init(&sh.bar_free, 1);
         sh.phase_base = 0;
+        sh.bulk_next[0] = sh.bulk_next[1] = 0;
         fence_mbar_init();
     }
     __syncthreads();
@@ -638,7 +640,7 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
             if (lane == 0) mbar_arrive(&sh.bar_crit);
         }
     } else if ((warp & 3) != 0) {
-        const int wb = warp - (warp >> 2) - 1, nwb = kBulkWarps;
+        const int wb = warp - (warp >> 2) - 1;
         for (int p = 0; p < P; ++p) {
             const int k0 = p * kNB, kb = min(kNB, M - k0);
             const int n0 = k0 + kb;
@@ -654,32 +656,40 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
                     if (c < kb && r < kb && r >= c) A[poff(k0 + c, Mp) + k0 + r] = sh.Lt[c][r];
                 }
             }
-            // Rows >= n2 in 32-row groups (solve, then panel p+1's columns take
-            // panels p and p-1), then panel p-1 on the columns beyond panel p+1.
+            // Work items, taken by the warps in turn from a shared counter (the
+            // next index is fetched while the current item runs): first the
+            // rows >= n2 in 32-row groups (solve, then panel p+1's columns take
+            // panels p and p-1; the longest items), then panel p-1 on the
+            // columns beyond panel p+1 in 32 x 16 tiles, column tile tc
+            // covering row tiles tc/2 .. TR-1.
             const int G = (Mp > n2) ? (Mp - n2 + 31) >> 5 : 0;
-            int item = 0;
-            for (int g = 0; g < G; ++g, ++item) {
-                if (item % nwb != wb) continue;
-                const int rb = n2 + 32 * g;
-                solve_rows(A, Mp, k0, kb, rb, 32, sh);
-                __syncwarp();
-                if (kb1 > 0) {
-                    update_next_rows16(A, Mp, k0, kb, n0, kb1, rb, p > 0, sh);
-                    if (rb + 16 < Mp) update_next_rows16(A, Mp, k0, kb, n0, kb1, rb + 16, p > 0, sh);
-                }
-            }
-            if (p > 0 && M > n1) {
-                const int TR = (Mp - n1 + 31) >> 5, TC = (M - n1 + 15) >> 4;
-                for (int tc = 0; tc < TC; ++tc) {
-                    const int j0 = n1 + tc * 16;
-                    for (int tr = (j0 - n1) >> 5; tr < TR; ++tr, ++item) {
-                        if (item % nwb != wb) continue;
-                        mma_tile<4, 2, kNB>(A, Mp, k0 - kNB, kNB, n1 + (tr << 5), j0, M, 0);
+            const int TR = (Mp - n1 + 31) >> 5;
+            const int TC = (p > 0 && M > n1) ? (M - n1 + 15) >> 4 : 0;
+            const int total = G + TC * TR - ((TC - 1) * (TC - 1)) / 4;
+            int *ctr = &sh.bulk_next[p & 1];
+            int item = __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(ctr, 1) : 0, 0);
+            while (item < total) {
+                const int raw = (lane == 0) ? atomicAdd(ctr, 1) : 0;
+                if (item < G) {
+                    const int rb = n2 + 32 * item;
+                    solve_rows(A, Mp, k0, kb, rb, 32, sh);
+                    __syncwarp();
+                    if (kb1 > 0) {
+                        update_next_rows16(A, Mp, k0, kb, n0, kb1, rb, p > 0, sh);
+                        if (rb + 16 < Mp) update_next_rows16(A, Mp, k0, kb, n0, kb1, rb + 16, p > 0, sh);
                     }
+                } else {
+                    int t = item - G, tc = 0;
+                    while (t >= TR - (tc >> 1)) t -= TR - (tc++ >> 1);
+                    mma_tile<4, 2, kNB>(A, Mp, k0 - kNB, kNB, n1 + (((tc >> 1) + t) << 5), n1 + tc * 16, M, 0);
                 }
+                item = __shfl_sync(0xffffffffu, raw, 0);
             }
             asm volatile("bar.sync 1, %0;" ::"n"(kBulkWarps * 32) : "memory");
-            if (tid == 32) mbar_arrive(&sh.bar_free);
+            if (tid == 32) {
+                *ctr = 0;  // every bulk warp is done with it; reused two panels on
+                mbar_arrive(&sh.bar_free);
+            }
         }
     }
     if (timed_out) atomicOr(&sh.status, kStDeviceTimeout);
