@@ -151,6 +151,10 @@ struct alignas(16) BlockShared {
     uint64_t bar_free;          // warps 1..15 -> warp 0: Lt/Lnx/inv may be overwritten
     unsigned phase_base;        // panels completed by this CTA (parity of the barriers)
     int bulk_next[2];           // next bulk work item of panels with even / odd index
+    uint64_t bar_ls[2];         // chain warps -> bulk warps: panel p's L is stored (by p's parity)
+    uint64_t bar_nc[2];         // bulk warps -> chain warps: panel p+1's columns took panel p-1
+    unsigned ph_ls[2], ph_nc[2];  // phases those four barriers completed before this block
+    int work_next[4];           // next bulk work item, by (2 p + stage) mod 4
     unsigned status;
     int task;
 };
@@ -164,6 +168,12 @@ __device__ __forceinline__ void init_block_sync(BlockShared &sh)
         mbar_init(&sh.bar_free, 1);
         sh.phase_base = 0;
         sh.bulk_next[0] = sh.bulk_next[1] = 0;
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&sh.bar_ls[i], 1);
+            mbar_init(&sh.bar_nc[i], 1);
+            sh.ph_ls[i] = sh.ph_nc[i] = 0;
+        }
+        for (int i = 0; i < 4; ++i) sh.work_next[i] = 0;
         fence_mbar_init();
     }
     __syncthreads();
@@ -324,6 +334,92 @@ __device__ __forceinline__ unsigned factor_diag_regs(const double *A, int Mp, in
         }
     }
     return st;
+}
+
+// Left-looking (Crout) factorization of the kb x kb diagonal block of panel
+// p with 16 rows below it solved in the same pass (one warp, registers):
+// lane r < 16 holds row k0+r of the diagonal block (columns <= r), lane 16+r
+// a row below.  At pivot q every lane forms a_rq - sum_{k<q} L_rk L_qk with
+// row q of L by shuffles from lane q; lane q's value is the pivot and one
+// rsqrt scales the column.  The sum over k < q-1 is formed while pivot
+// q-1's rsqrt is in flight (four partial sums), and every lane forms the
+// pivot itself from lane q's early-broadcast partial sum, so one shuffle
+// sits on the dependent chain per pivot.  A non-positive or NaN pivot is
+// kept on the diagonal and its column is zeroed below (the block is
+// reported; its log-determinant skips the pivot, as core_Xlogdet does).
+// Warps that run it on the same diagonal block form identical factors.
+__device__ __forceinline__ unsigned factor_rows(int k0, int kb, int mc, double (&v)[kNB], double &myinv)
+{
+    const int lane = threadIdx.x & 31;
+    const bool low = lane < kNB;
+    const int r = low ? lane : lane - kNB;
+    unsigned st = 0;
+    myinv = 0.0;
+    double pre = v[0];
+#pragma unroll
+    for (int q = 0; q < kNB; ++q) {
+        if (q < kb) {
+            const double preq = __shfl_sync(0xffffffffu, pre, q);
+            double s = pre, piv = preq;
+            if (q > 0) {
+                const double l = __shfl_sync(0xffffffffu, v[q - 1], q);
+                s = fma(-v[q - 1], l, s);
+                piv = fma(-l, l, preq);
+            }
+            const bool ok = piv > 0.0;
+            const double inv = ok ? rsqrt(piv) : 0.0;
+            if (q + 1 < kNB) {
+                double s4[4] = {v[q + 1], 0.0, 0.0, 0.0};
+#pragma unroll
+                for (int k = 0; k < q; ++k) {
+                    const double lk = __shfl_sync(0xffffffffu, v[k], q + 1);
+                    s4[k & 3] = fma(-v[k], lk, s4[k & 3]);
+                }
+                pre = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+            }
+            if (!ok) st |= (k0 + q < mc) ? 1u : 2u;
+            if (low && r == q) {
+                v[q] = ok ? piv * inv : piv;
+                myinv = inv;
+            } else if (!low || r > q) {
+                v[q] = s * inv;
+            }
+        }
+    }
+    return st;
+}
+
+// Another 16 rows below the same diagonal block, after factor_rows: the
+// lower lanes keep the factor (L rows in v, the scale of their pivot in
+// myinv) and only the upper lanes' rows change, by the same operations in
+// the same order as in factor_rows (so the results are identical), without
+// the pivot chain.
+__device__ __forceinline__ void solve_more_rows(int kb, double (&v)[kNB], double myinv)
+{
+    const int lane = threadIdx.x & 31;
+    const bool low = lane < kNB;
+    double pre = v[0];
+#pragma unroll
+    for (int q = 0; q < kNB; ++q) {
+        if (q < kb) {
+            const double inv = __shfl_sync(0xffffffffu, myinv, q);
+            double s = pre;
+            if (q > 0) {
+                const double l = __shfl_sync(0xffffffffu, v[q - 1], q);
+                s = fma(-v[q - 1], l, s);
+            }
+            if (q + 1 < kNB) {
+                double s4[4] = {v[q + 1], 0.0, 0.0, 0.0};
+#pragma unroll
+                for (int k = 0; k < q; ++k) {
+                    const double lk = __shfl_sync(0xffffffffu, v[k], q + 1);
+                    s4[k & 3] = fma(-v[k], lk, s4[k & 3]);
+                }
+                pre = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+            }
+            if (!low) v[q] = s * inv;
+        }
+    }
 }
 
 // The factored diagonal block to sh.Lt (transposed), its reciprocal pivots
@@ -697,6 +793,176 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
     if (tid == 0) sh.phase_base = base + (unsigned)P;
 }
 
+// ---------------------------------------------------------------------------
+// Panel-parallel Cholesky of the first M columns of the packed (M+1)-row
+// system, right-looking with a look-ahead of one panel.
+//
+// Chain warps (0-7): for panel p each runs the 16-pivot factorization of the
+// diagonal block together with 32 rows of its own below it (rows c1 + 32 w
+// ..., c1 = first row below the block), so the whole panel column is factored
+// and solved in one pass of the dependent chain with no separate triangular
+// solve; every warp forms the same pivots.  They store their rows, meet at a
+// barrier (warp 0 then stores the diagonal block and signals the bulk warps),
+// wait until panel p+1's columns have taken panel p-1, apply panel p to their
+// own rows in panel p+1's columns (the look-ahead; panel p+1's rows are warp
+// 0's first 16) and meet again: panel p+1's columns are then final for the
+// next factorization.  Bulk warps (8-15): for panel p they apply panel p-1
+// to panel p+1's columns, signal, then apply it to the columns beyond, in
+// 32 x 16 tiles taken from a shared counter.  Every element of panel c's
+// columns receives panel q's contribution exactly once: q = c-1 from the
+// look-ahead of iteration c-1, q <= c-2 from the bulk work of iteration q+1.
+// The two signals are mbarriers with bounded waits, one per parity of p, so
+// neither side can run two phases ahead of the other.
+// ---------------------------------------------------------------------------
+constexpr int kChainWarps = 8;
+#ifndef BV_PP_MAX_M
+#define BV_PP_MAX_M 150
+#endif
+constexpr int kPpMaxM = BV_PP_MAX_M;
+constexpr int kPpBulkWarps = kWarps - kChainWarps;
+
+__device__ __forceinline__ void cholesky_pp(double *A, int M, int mc, BlockShared &sh)
+{
+    const int Mp = M + 1;
+    const int P = (M + kNB - 1) / kNB;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const unsigned bl[2] = {sh.ph_ls[0], sh.ph_ls[1]};
+    const unsigned bn[2] = {sh.ph_nc[0], sh.ph_nc[1]};
+    bool timed_out = false;
+    if (warp < kChainWarps) {
+        const bool low = lane < kNB;
+        const int r = low ? lane : lane - kNB;
+        for (int p = 0; p < P; ++p) {
+            const int k0 = p * kNB, kb = min(kNB, M - k0);
+            const int c1 = k0 + kb;
+            const int kb1 = max(0, min(kNB, M - c1));
+            // Slices of 16 rows below the diagonal block: w, w + 8, ... (the
+            // first is panel p+1's rows, warp 0's, and warp 0 always runs).
+            // The first slice of a warp runs with the factorization, the
+            // others reuse the factor it leaves in the lower lanes.
+            unsigned st = 0;
+            if (warp == 0 || c1 + kNB * warp < Mp) {
+                double v[kNB], myinv;
+                {
+                    const int row = c1 + kNB * warp + r;
+                    const bool valid = !low && row < Mp;
+#pragma unroll
+                    for (int c = 0; c < kNB; ++c) {
+                        const bool in = low ? (r < kb && c <= r) : valid;
+                        v[c] = (in && c < kb) ? A[poff(k0 + c, Mp) + (low ? k0 + r : row)] : 0.0;
+                    }
+                    st = factor_rows(k0, kb, mc, v, myinv);
+                    if (warp == 0 && low) {
+                        // Warp 0's diagonal factor waits in sh.Lt (transposed)
+                        // until every chain warp has read the block from A.
+#pragma unroll
+                        for (int c = 0; c < kNB; ++c) sh.Lt[c][r] = v[c];
+                    }
+                    if (valid) {
+#pragma unroll
+                        for (int c = 0; c < kNB; ++c)
+                            if (c < kb) A[poff(k0 + c, Mp) + row] = v[c];
+                    }
+                }
+#pragma unroll 1
+                for (int sl = warp + kChainWarps; c1 + kNB * sl < Mp; sl += kChainWarps) {
+                    const int row = c1 + kNB * sl + r;
+                    const bool valid = !low && row < Mp;
+                    if (!low) {
+#pragma unroll
+                        for (int c = 0; c < kNB; ++c) v[c] = (valid && c < kb) ? A[poff(k0 + c, Mp) + row] : 0.0;
+                    }
+                    solve_more_rows(kb, v, myinv);
+                    if (valid) {
+#pragma unroll
+                        for (int c = 0; c < kNB; ++c)
+                            if (c < kb) A[poff(k0 + c, Mp) + row] = v[c];
+                    }
+                }
+            }
+            // Every chain warp has read the diagonal block and stored its rows.
+            asm volatile("bar.sync 2, %0;" ::"n"(kChainWarps * 32) : "memory");
+            if (warp == 0 && lane == 0) {
+                if (st) atomicOr(&sh.status, st);
+                mbar_arrive(&sh.bar_ls[p & 1]);
+            }
+            if (warp == kChainWarps - 1) {
+                // The diagonal factor into A (off warp 0's path; the last
+                // chain warp has the least look-ahead work).
+                double l[kNB * kNB / 32];
+#pragma unroll
+                for (int i = 0; i < kNB * kNB / 32; ++i) {
+                    const int t = lane + 32 * i;
+                    l[i] = sh.Lt[t >> 4][t & 15];
+                }
+#pragma unroll
+                for (int i = 0; i < kNB * kNB / 32; ++i) {
+                    const int t = lane + 32 * i, c = t >> 4, rr = t & 15;
+                    if (c < kb && rr < kb && rr >= c) A[poff(k0 + c, Mp) + k0 + rr] = l[i];
+                }
+            }
+            if (!mbar_wait_bounded(&sh.bar_nc[p & 1], (bn[p & 1] + (p >> 1)) & 1u)) timed_out = true;
+            if (kb1 > 0) {
+                for (int sl = warp; c1 + kNB * sl < Mp; sl += kChainWarps)
+                    mma_tile<2, 2, kNB>(A, Mp, k0, kNB, c1 + kNB * sl, c1, c1 + kb1, 0);
+            }
+            asm volatile("bar.sync 2, %0;" ::"n"(kChainWarps * 32) : "memory");
+        }
+    } else {
+        const int first = kChainWarps * 32;
+        for (int p = 0; p < P; ++p) {
+            const int k0 = p * kNB, kb = min(kNB, M - k0);
+            const int c1 = k0 + kb;
+            const int kb1 = max(0, min(kNB, M - c1));
+            const int c2 = c1 + kb1;
+            if (p > 0 && !mbar_wait_bounded(&sh.bar_ls[(p - 1) & 1], (bl[(p - 1) & 1] + ((p - 1) >> 1)) & 1u))
+                timed_out = true;
+            // Panel p-1 on panel p+1's columns, 32-row tiles from its diagonal down.
+            {
+                const int total = (p > 0 && kb1 > 0) ? (Mp - c1 + 31) >> 5 : 0;
+                int *ctr = &sh.work_next[(2 * p) & 3];
+                int item = __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(ctr, 1) : 0, 0);
+                while (item < total) {
+                    const int raw = (lane == 0) ? atomicAdd(ctr, 1) : 0;
+                    mma_tile<4, 2, kNB>(A, Mp, k0 - kNB, kNB, c1 + 32 * item, c1, c2, 0);
+                    item = __shfl_sync(0xffffffffu, raw, 0);
+                }
+            }
+            asm volatile("bar.sync 1, %0;" ::"n"(kPpBulkWarps * 32) : "memory");
+            if (tid == first) {
+                sh.work_next[(2 * p) & 3] = 0;
+                mbar_arrive(&sh.bar_nc[p & 1]);
+            }
+            // Panel p-1 on the columns beyond panel p+1: column tile tc covers
+            // row tiles tc/2 .. TR-1.
+            {
+                const int TR = (Mp - c2 + 31) >> 5;
+                const int TC = (p > 0 && M > c2) ? (M - c2 + 15) >> 4 : 0;
+                const int total = TC * TR - ((TC - 1) * (TC - 1)) / 4;
+                int *ctr = &sh.work_next[(2 * p + 1) & 3];
+                int item = __shfl_sync(0xffffffffu, lane == 0 ? atomicAdd(ctr, 1) : 0, 0);
+                while (item < total) {
+                    const int raw = (lane == 0) ? atomicAdd(ctr, 1) : 0;
+                    int t = item, tc = 0;
+                    while (t >= TR - (tc >> 1)) t -= TR - (tc++ >> 1);
+                    mma_tile<4, 2, kNB>(A, Mp, k0 - kNB, kNB, c2 + (((tc >> 1) + t) << 5), c2 + tc * 16, M, 0);
+                    item = __shfl_sync(0xffffffffu, raw, 0);
+                }
+            }
+            asm volatile("bar.sync 1, %0;" ::"n"(kPpBulkWarps * 32) : "memory");
+            if (tid == first) sh.work_next[(2 * p + 1) & 3] = 0;
+        }
+    }
+    if (timed_out) atomicOr(&sh.status, kStDeviceTimeout);
+    __syncthreads();
+    if (tid == 0) {
+        sh.ph_ls[0] = bl[0] + (unsigned)((P + 1) >> 1);
+        sh.ph_ls[1] = bl[1] + (unsigned)(P >> 1);
+        sh.ph_nc[0] = bn[0] + (unsigned)((P + 1) >> 1);
+        sh.ph_nc[1] = bn[1] + (unsigned)(P >> 1);
+    }
+}
+
 // One block, with its matrix at A (shared memory or the global slab).
 __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternParams &mp, int b,
                                               double *X, double *Y, double *A, BlockShared &sh)
@@ -722,7 +988,10 @@ __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternPara
 
     // Cholesky of the first M columns; row M rides along as the
     // forward-substitution right-hand side.
-    cholesky_ws(A, M, mc, sh);
+    if (M <= kPpMaxM)
+        cholesky_pp(A, M, mc, sh);
+    else
+        cholesky_ws(A, M, mc, sh);
 
     // log det of the conditional factor (positive pivots only, as
     // core_Xlogdet) and |u|^2 from row M.
