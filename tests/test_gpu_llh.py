@@ -229,3 +229,55 @@ def test_large_blocks_deterministic_and_served(bvlib):
     with bvlib.Server(on_failure="continue") as srv:
         j = srv.open_job(L)
         assert srv.evaluate(j, th) == v[0]
+
+
+@pytest.mark.parametrize("cs", [180, 200])
+def test_large_shared_memory_blocks(bvlib, oracle, cs):
+    """Blocks of M = cs + bs ~ 190-230, which run the warp-specialised
+    schedule in shared memory (the headline workload's path)."""
+    L = _gen(bvlib, 3000, 200, cs)
+    M = L.batchNum[1:] + cs
+    assert M.min() > 150 and M.max() <= 230
+    _check(bvlib, oracle, L, thetas=THETAS[:4])
+
+
+def test_both_schedules_in_one_launch(bvlib, oracle):
+    """cs = 140: blocks on both sides of the size at which the kernel switches
+    from the panel-parallel to the warp-specialised schedule."""
+    L = _gen(bvlib, 4000, 300, 140)
+    M = L.batchNum[1:] + 140
+    assert (M <= 150).any() and (M > 150).any()
+    _check(bvlib, oracle, L, thetas=THETAS[:3])
+
+
+def test_failure_policy_large_blocks(bvlib):
+    """Singular covariances (duplicated locations) in blocks of M = 180-190,
+    which run the warp-specialised schedule: reported, -inf by default,
+    finite under 'continue', and the same on a second evaluation."""
+    rng = np.random.default_rng(5)
+    cs = 170
+    first = rng.random((160, 2))
+    block0 = np.concatenate([first, first[:20]])     # 20 locations twice in block 0
+    rest = rng.random((60, 2))
+    pts = np.concatenate([block0, rest])
+    x, y = pts[:, 0].copy(), pts[:, 1].copy()
+    n = len(x)
+    bn = np.array([180, 20, 20, 20], dtype=np.int32)   # block 0 must hold >= cs points
+    acc = np.concatenate([[0], np.cumsum(bn)]).astype(np.int32)
+    assert acc[-1] == n
+    # conditioning sets from the earlier blocks, as the layout requires
+    knn = np.zeros(len(bn) * cs, dtype=np.int32)
+    knn[:cs] = np.arange(cs)
+    for b in range(1, len(bn)):
+        knn[b * cs:(b + 1) * cs] = rng.choice(int(acc[b]), cs, replace=False)
+    L = bvlib.Layout(bn, acc, x, y, rng.standard_normal(n), cs, knn_idx=knn)
+    th = (1.0, 0.1, 0.5)
+    with bvlib.LlhData(L) as D:
+        v = D(th)
+        st = D.status()
+    nfail = st["cond_fail"] + st["schur_fail"]
+    assert v == -np.inf and nfail >= 1
+    with bvlib.LlhData(L, on_failure="continue") as D:
+        a, b = D(th), D(th)
+        st2 = D.status()
+    assert np.isfinite(a) and a == b and st2["cond_fail"] + st2["schur_fail"] == nfail
