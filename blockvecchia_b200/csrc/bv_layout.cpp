@@ -298,14 +298,19 @@ extern "C" int bv_layout_from_clusters(const double *x, const double *y, const d
     }
     // reorderIndex (include/vecchia_helper_method.h:128-160): index of the
     // first original centroid at zero distance = lowest index with the same
-    // coordinates.
+    // coordinates.  Where several centroids coincide (clusters of duplicated
+    // locations) the reference maps all of them to that lowest index, so one
+    // cluster's points are taken twice and the other's are lost; here the
+    // k-th shuffled occurrence of a coordinate pair maps to the k-th original
+    // with it, which is the same map whenever the centroids are distinct and
+    // otherwise puts every point in exactly one block.
     struct PairHash {
         size_t operator()(const std::pair<uint64_t, uint64_t> &p) const
         {
             return std::hash<uint64_t>()(p.first * 0x9E3779B97F4A7C15ull ^ p.second);
         }
     };
-    std::unordered_map<std::pair<uint64_t, uint64_t>, int, PairHash> first_at;
+    std::unordered_map<std::pair<uint64_t, uint64_t>, std::vector<int>, PairHash> first_at;
     first_at.reserve((size_t)k * 2);
     auto keyof = [](double a, double b) {
         uint64_t ua, ub;
@@ -315,9 +320,13 @@ extern "C" int bv_layout_from_clusters(const double *x, const double *y, const d
         std::memcpy(&ub, &b, 8);
         return std::make_pair(ua, ub);
     };
-    for (int j = 0; j < k; ++j) first_at.emplace(keyof(ccx[j], ccy[j]), j);
+    for (int j = 0; j < k; ++j) first_at[keyof(ccx[j], ccy[j])].push_back(j);  // ascending j
+    std::unordered_map<std::pair<uint64_t, uint64_t>, int, PairHash> taken;
     std::vector<int> perm(k);
-    for (int i = 0; i < k; ++i) perm[i] = first_at.at(keyof(px[i], py[i]));
+    for (int i = 0; i < k; ++i) {
+        const auto key = keyof(px[i], py[i]);
+        perm[i] = first_at.at(key)[taken[key]++];
+    }
     // firstbatch (:95-108)
     int fcs = 0, fcc = 0, acc_sz = 0;
     for (int i = 0; i < k; ++i) {

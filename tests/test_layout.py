@@ -78,3 +78,35 @@ def test_layout_rejects_too_few_points(bvlib):
     x, y, z = rng.random(20), rng.random(20), rng.random(20)
     with pytest.raises(bvlib.BvError):
         bvlib.build_layout(x, y, z, 5, 30)
+
+
+def test_layout_with_coinciding_centroids_covers_every_point(bvlib):
+    """Clusters whose centroids coincide (duplicated locations) each become
+    their own block: every point lands in exactly one block.  (The reference's
+    reorderIndex maps coinciding centroids to one cluster, which takes that
+    cluster's points twice and drops the other's.)"""
+    rng = np.random.default_rng(3)
+    k = 12
+    ccx, ccy = rng.random(k), rng.random(k)
+    ccx[7], ccy[7] = ccx[2], ccy[2]          # clusters 2 and 7 share a centroid
+    ccx[10], ccy[10] = ccx[2], ccy[2]        # and so does cluster 10
+    sizes = rng.integers(3, 9, k)
+    labels = np.repeat(np.arange(k), sizes)
+    rng.shuffle(labels)
+    n = len(labels)
+    x = ccx[labels] + 1e-3 * rng.standard_normal(n)
+    y = ccy[labels] + 1e-3 * rng.standard_normal(n)
+    L = bvlib.layout_from_clusters(x, y, np.arange(n, dtype=np.float64), labels, ccx, ccy, 4)
+    assert int(L.batchNumAccum[-1]) == n
+    assert np.array_equal(np.sort(L.obs.astype(np.int64)), np.arange(n))
+
+
+def test_layout_with_many_duplicated_locations(bvlib):
+    """Locations clipped to the unit square (many exact duplicates on the
+    edges) still give a layout that covers every point once."""
+    rng = np.random.default_rng(4)
+    n = 30000
+    x = np.clip(0.5 + 0.4 * rng.standard_normal(n), 0, 1)
+    y = np.clip(0.5 + 0.4 * rng.standard_normal(n), 0, 1)
+    L = bvlib.build_layout(x, y, np.arange(n, dtype=np.float64), 3000, 40, seed=0, epochs=5)
+    assert np.array_equal(np.sort(L.obs.astype(np.int64)), np.arange(n))
