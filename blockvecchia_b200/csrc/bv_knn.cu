@@ -18,6 +18,10 @@
 // whatever S member occupied position t moves to the winner's old position.
 // Members outside S never win and never change the relative positions of S
 // members, so the replay reproduces the reference's output, ties included.
+// A block whose ties at the k-th key overflow the warp's buffer (hundreds of
+// exactly repeated locations at one distance) is listed and redone by
+// knn_heavy_kernel: one CTA, keys recomputed on every pass instead of
+// buffered, S in a global scratch array, the same replay.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -48,6 +52,8 @@ struct KnnArgs {
     int *out;
     unsigned *counter;
     int *error;  // first failing block + 1, or 0
+    int *heavy;  // blocks whose ties overflow the buffer, for knn_heavy_kernel
+    unsigned *heavy_count;
 };
 
 __device__ __forceinline__ unsigned lanemask_lt()
@@ -215,7 +221,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
             }
         }
         if (overflow) {
-            if (lane == 0) atomicCAS(a.error, 0, i + 1);
+            if (lane == 0) a.heavy[atomicAdd(a.heavy_count, 1u)] = i;
             continue;
         }
         __syncwarp();
@@ -289,6 +295,144 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
     }
 }
 
+
+// Blocks listed by knn_kernel, one after another on one CTA.  scratch holds
+// S (distance bits, index, current position) for one block at a time; n
+// entries suffice (S is a subset of the block's candidates).
+constexpr int kHeavyThreads = 1024;
+
+struct KnnHeavyScratch {
+    unsigned long long *key;
+    int *idx;
+    int *pos;
+};
+
+__device__ __forceinline__ unsigned long long knn_skey(const double *x, const double *y, int p, double cx,
+                                                       double cy)
+{
+    const double dx = __ldg(x + p) - cx;
+    const double dy = __ldg(y + p) - cy;
+    return (unsigned long long)__double_as_longlong(__fma_rn(dx, dx, __dmul_rn(dy, dy)));
+}
+
+__global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int nheavy, KnnHeavyScratch sc)
+{
+    __shared__ unsigned hist[256];
+    __shared__ unsigned long long s_prefix;
+    __shared__ int s_kk, s_count, s_occ;
+    __shared__ unsigned long long w_key[kHeavyThreads / 32];
+    __shared__ int w_pos[kHeavyThreads / 32], w_slot[kHeavyThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int k = a.cs;
+    for (int h = 0; h < nheavy; ++h) {
+        const int i = a.heavy[h];
+        const int P = a.acc[i];
+        const double cx = a.cx[i], cy = a.cy[i];
+        int *out = a.out + (size_t)i * k;
+        // 1. Exact k-th smallest squared distance, MSB-first radix select.
+        if (tid == 0) {
+            s_prefix = 0ull;
+            s_kk = k;
+        }
+        unsigned long long mask = 0ull;
+        for (int shift = 56; shift >= 0; shift -= 8) {
+            if (tid < 256) hist[tid] = 0u;
+            __syncthreads();
+            const unsigned long long prefix = s_prefix;
+            for (int p = tid; p < P; p += kHeavyThreads) {
+                const unsigned long long key = knn_skey(a.x, a.y, p, cx, cy);
+                if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255ull], 1u);
+            }
+            __syncthreads();
+            if (tid == 0) {
+                unsigned run = 0;
+                int bin = 255;
+                for (int b = 0; b < 256; ++b) {
+                    if (run + hist[b] >= (unsigned)s_kk) {
+                        bin = b;
+                        break;
+                    }
+                    run += hist[b];
+                }
+                s_prefix = prefix | ((unsigned long long)bin << shift);
+                s_kk -= (int)run;
+            }
+            mask |= 255ull << shift;
+            __syncthreads();
+        }
+        const unsigned long long kth = s_prefix;
+        // 2. S = candidates whose distance equals or beats the k-th.
+        const unsigned long long hi = window_hi(kth);
+        const double dk = __dsqrt_rn(__longlong_as_double((long long)kth));
+        if (tid == 0) s_count = 0;
+        __syncthreads();
+        for (int p = tid; p < P; p += kHeavyThreads) {
+            const unsigned long long key = knn_skey(a.x, a.y, p, cx, cy);
+            if (key <= hi) {
+                const double d = __dsqrt_rn(__longlong_as_double((long long)key));
+                if (d <= dk) {
+                    const int slot = atomicAdd(&s_count, 1);
+                    sc.key[slot] = (unsigned long long)__double_as_longlong(d);
+                    sc.idx[slot] = p;
+                    sc.pos[slot] = p;  // initial position = index
+                }
+            }
+        }
+        __syncthreads();
+        const int count = s_count;
+        // 3. Replay the selection sort on S.
+        for (int t = 0; t < k; ++t) {
+            unsigned long long bkey = ~0ull;
+            int bpos = 0x7fffffff, bslot = -1;
+            if (tid == 0) s_occ = -1;
+            __syncthreads();
+            for (int j = tid; j < count; j += kHeavyThreads) {
+                const int pj = sc.pos[j];
+                if (pj < 0) continue;  // already selected
+                const unsigned long long kj = sc.key[j];
+                if (kj < bkey || (kj == bkey && pj < bpos)) {
+                    bkey = kj;
+                    bpos = pj;
+                    bslot = j;
+                }
+                if (pj == t) s_occ = j;  // positions are distinct: one writer
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long ok = __shfl_xor_sync(0xffffffffu, bkey, o);
+                const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
+                const int os = __shfl_xor_sync(0xffffffffu, bslot, o);
+                if (ok < bkey || (ok == bkey && op < bpos)) {
+                    bkey = ok;
+                    bpos = op;
+                    bslot = os;
+                }
+            }
+            if (lane == 0) {
+                w_key[warp] = bkey;
+                w_pos[warp] = bpos;
+                w_slot[warp] = bslot;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                for (int w = 1; w < kHeavyThreads / 32; ++w) {
+                    if (w_key[w] < bkey || (w_key[w] == bkey && w_pos[w] < bpos)) {
+                        bkey = w_key[w];
+                        bpos = w_pos[w];
+                        bslot = w_slot[w];
+                    }
+                }
+                if (bslot >= 0) {  // |S| >= k makes bslot >= 0
+                    out[t] = sc.idx[bslot];
+                    if (s_occ >= 0 && s_occ != bslot) sc.pos[s_occ] = bpos;
+                    sc.pos[bslot] = -1;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, const int *d_acc,
                const double *cx, const double *cy, int *d_knn, cudaStream_t s)
 {
@@ -312,17 +456,21 @@ int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, cons
         fail(e, "cudaMalloc");
         return rc;
     }
-    if ((e = cudaMalloc(&d_counter, sizeof(unsigned) + sizeof(int))) != cudaSuccess) {
+    // counter, error, heavy_count, then the heavy list (bc entries)
+    if ((e = cudaMalloc(&d_counter, sizeof(unsigned) * 3 + sizeof(int) * (size_t)bc)) != cudaSuccess) {
         cudaFree(d_c);
         fail(e, "cudaMalloc");
         return rc;
     }
     d_err = reinterpret_cast<int *>(d_counter + 1);
+    unsigned *d_heavy_count = d_counter + 2;
+    int *d_heavy = reinterpret_cast<int *>(d_counter + 3);
+    KnnHeavyScratch sc{nullptr, nullptr, nullptr};
     do {
         if ((e = cudaMemcpyAsync(d_c, cx, sizeof(double) * bc, cudaMemcpyHostToDevice, s)) ||
             (e = cudaMemcpyAsync(d_c + bc, cy, sizeof(double) * bc, cudaMemcpyHostToDevice, s)) ||
             (e = cudaMemcpyAsync(d_knn, first.data(), sizeof(int) * cs, cudaMemcpyHostToDevice, s)) ||
-            (e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned) + sizeof(int), s))) {
+            (e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned) * 3, s))) {
             fail(e, "copy");
             break;
         }
@@ -337,6 +485,8 @@ int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, cons
         ka.out = d_knn;
         ka.counter = d_counter;
         ka.error = d_err;
+        ka.heavy = d_heavy;
+        ka.heavy_count = d_heavy_count;
         const size_t smem = sizeof(KnnWarpSmem) * kKnnWarps;
         if ((e = cudaFuncSetAttribute(knn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem))) {
@@ -356,21 +506,39 @@ int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, cons
             fail(e, "launch");
             break;
         }
-        int herr = 0;
-        if ((e = cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, s)) ||
+        unsigned hbuf[2] = {0u, 0u};  // error, heavy_count
+        if ((e = cudaMemcpyAsync(hbuf, d_err, sizeof(unsigned) * 2, cudaMemcpyDeviceToHost, s)) ||
             (e = cudaStreamSynchronize(s))) {
             fail(e, "sync");
             break;
         }
-        if (herr) {
-            set_error("bv_knn: block %d has fewer than cs=%d earlier points or more than %d "
-                      "candidates tie at its cs-th distance",
-                      herr - 1, cs, kKnnCap - 128);
+        if (hbuf[0]) {
+            set_error("bv_knn: block %d has fewer than cs=%d earlier points", (int)hbuf[0] - 1, cs);
             rc = BV_E_TOOLARGE;
+            break;
+        }
+        const int nheavy = (int)hbuf[1];
+        if (nheavy > 0) {
+            // Blocks with more ties than the warp buffer holds: S can hold up
+            // to every earlier point, so the scratch has n entries.
+            if ((e = cudaMalloc(&sc.key, sizeof(unsigned long long) * (size_t)n)) ||
+                (e = cudaMalloc(&sc.idx, sizeof(int) * (size_t)n)) ||
+                (e = cudaMalloc(&sc.pos, sizeof(int) * (size_t)n))) {
+                fail(e, "cudaMalloc (tie scratch)");
+                break;
+            }
+            knn_heavy_kernel<<<1, kHeavyThreads, 0, s>>>(ka, nheavy, sc);
+            if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(s))) {
+                fail(e, "tie pass");
+                break;
+            }
         }
     } while (0);
     cudaFree(d_c);
     cudaFree(d_counter);
+    cudaFree(sc.key);
+    cudaFree(sc.idx);
+    cudaFree(sc.pos);
     return rc;
 }
 

@@ -58,3 +58,26 @@ def test_knn_rejects_short_prefix(bvlib):
                      np.random.rand(10), np.zeros(10), 8, np.zeros(2), np.zeros(2))
     with pytest.raises(bvlib.BvError):
         bvlib.knn(L)
+
+
+def test_ties_beyond_the_warp_buffer(bvlib, oracle):
+    """1,200 copies of one location, all at the cs-th distance of two blocks'
+    centroids: more ties than the per-warp candidate buffer holds, so those
+    blocks take the block-wide pass; the order must still be the
+    reference's, bit for bit."""
+    rng = np.random.default_rng(9)
+    cs = 100
+    dup = np.full(1200, 0.5)
+    x = np.concatenate([dup, rng.random(2000), [0.2, 0.8]])
+    y = np.concatenate([dup, rng.random(2000), [0.3, 0.6]])
+    perm = np.concatenate([rng.permutation(3200), [3200, 3201]])
+    x, y = x[perm].copy(), y[perm].copy()
+    bn = np.array([3200, 1, 1], np.int32)
+    acc = np.array([0, 3200, 3201, 3202], np.int32)
+    cx = np.array([0.0, 0.5 + 1e-3, 0.5])       # block 2: centroid on the duplicates
+    cy = np.array([0.0, 0.5, 0.5 - 2e-3])
+    L = bvlib.Layout(bn, acc, x, y, np.zeros(len(x)), cs, cx, cy)
+    got = bvlib.knn(L)
+    ref = oracle.knn_all(L.x, L.y, cs, L.batchNumAccum, L.cx, L.cy)
+    assert np.array_equal(got, ref)
+    assert set(got[cs:2 * cs].tolist()) <= set(np.nonzero(L.x[:3200] == 0.5)[0].tolist())
