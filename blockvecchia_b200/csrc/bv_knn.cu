@@ -24,6 +24,7 @@
 // buffered, S in a global scratch array, the same replay.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <vector>
 
@@ -296,9 +297,9 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
 }
 
 
-// Blocks listed by knn_kernel, one after another on one CTA.  scratch holds
-// S (distance bits, index, current position) for one block at a time; n
-// entries suffice (S is a subset of the block's candidates).
+// Blocks listed by knn_kernel, dealt round-robin to the CTAs.  Each CTA has
+// n entries of scratch for S (distance bits, index, current position) of the
+// block it works on (S is a subset of the block's candidates, so n suffice).
 constexpr int kHeavyThreads = 1024;
 
 struct KnnHeavyScratch {
@@ -315,8 +316,11 @@ __device__ __forceinline__ unsigned long long knn_skey(const double *x, const do
     return (unsigned long long)__double_as_longlong(__fma_rn(dx, dx, __dmul_rn(dy, dy)));
 }
 
-__global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int nheavy, KnnHeavyScratch sc)
+__global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int nheavy, KnnHeavyScratch scr,
+                                                                  size_t stride)
 {
+    KnnHeavyScratch sc{scr.key + blockIdx.x * stride, scr.idx + blockIdx.x * stride,
+                       scr.pos + blockIdx.x * stride};
     __shared__ unsigned hist[256];
     __shared__ unsigned long long s_prefix;
     __shared__ int s_kk, s_count, s_occ;
@@ -324,7 +328,7 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
     __shared__ int w_pos[kHeavyThreads / 32], w_slot[kHeavyThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int k = a.cs;
-    for (int h = 0; h < nheavy; ++h) {
+    for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
         const int i = a.heavy[h];
         const int P = a.acc[i];
         const double cx = a.cx[i], cy = a.cy[i];
@@ -520,14 +524,18 @@ int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, cons
         const int nheavy = (int)hbuf[1];
         if (nheavy > 0) {
             // Blocks with more ties than the warp buffer holds: S can hold up
-            // to every earlier point, so the scratch has n entries.
-            if ((e = cudaMalloc(&sc.key, sizeof(unsigned long long) * (size_t)n)) ||
-                (e = cudaMalloc(&sc.idx, sizeof(int) * (size_t)n)) ||
-                (e = cudaMalloc(&sc.pos, sizeof(int) * (size_t)n))) {
+            // to every earlier point, so each CTA gets n entries (16 bytes
+            // each); at most one CTA per SM and 4 GB of scratch in all.
+            const size_t per = (size_t)n * 16;
+            int g = (int)std::min<size_t>((size_t)nheavy, std::max<size_t>(1, ((size_t)4 << 30) / per));
+            g = std::min(g, sms > 0 ? sms : 1);
+            const size_t cnt = (size_t)n * (size_t)g;
+            if ((e = cudaMalloc(&sc.key, sizeof(unsigned long long) * cnt)) ||
+                (e = cudaMalloc(&sc.idx, sizeof(int) * cnt)) || (e = cudaMalloc(&sc.pos, sizeof(int) * cnt))) {
                 fail(e, "cudaMalloc (tie scratch)");
                 break;
             }
-            knn_heavy_kernel<<<1, kHeavyThreads, 0, s>>>(ka, nheavy, sc);
+            knn_heavy_kernel<<<g, kHeavyThreads, 0, s>>>(ka, nheavy, sc, (size_t)n);
             if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(s))) {
                 fail(e, "tie pass");
                 break;
