@@ -797,16 +797,17 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
 // Panel-parallel Cholesky of the first M columns of the packed (M+1)-row
 // system, right-looking with a look-ahead of one panel.
 //
-// Chain warps (0-7): for panel p each runs the 16-pivot factorization of the
-// diagonal block together with 32 rows of its own below it (rows c1 + 32 w
-// ..., c1 = first row below the block), so the whole panel column is factored
-// and solved in one pass of the dependent chain with no separate triangular
-// solve; every warp forms the same pivots.  They store their rows, meet at a
+// Chain warps (0-11): for panel p each runs the 16-pivot factorization of the
+// diagonal block together with 16 rows of its own below it (slice w of the
+// rows from c1, the first row below the block; slices w + 12, ... reuse the
+// factor by substitution), so the whole panel column is factored and solved
+// in one pass of the dependent chain with no separate triangular solve;
+// every warp forms the same pivots.  They store their rows, meet at a
 // barrier (warp 0 then stores the diagonal block and signals the bulk warps),
 // wait until panel p+1's columns have taken panel p-1, apply panel p to their
 // own rows in panel p+1's columns (the look-ahead; panel p+1's rows are warp
 // 0's first 16) and meet again: panel p+1's columns are then final for the
-// next factorization.  Bulk warps (8-15): for panel p they apply panel p-1
+// next factorization.  Bulk warps (12-15): for panel p they apply panel p-1
 // to panel p+1's columns, signal, then apply it to the columns beyond, in
 // 32 x 16 tiles taken from a shared counter.  Every element of panel c's
 // columns receives panel q's contribution exactly once: q = c-1 from the
@@ -814,9 +815,9 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
 // The two signals are mbarriers with bounded waits, one per parity of p, so
 // neither side can run two phases ahead of the other.
 // ---------------------------------------------------------------------------
-constexpr int kChainWarps = 8;
+constexpr int kChainWarps = 12;
 #ifndef BV_PP_MAX_M
-#define BV_PP_MAX_M 150
+#define BV_PP_MAX_M 190
 #endif
 constexpr int kPpMaxM = BV_PP_MAX_M;
 constexpr int kPpBulkWarps = kWarps - kChainWarps;
@@ -836,7 +837,7 @@ __device__ __forceinline__ void cholesky_pp(double *A, int M, int mc, BlockShare
             const int k0 = p * kNB, kb = min(kNB, M - k0);
             const int c1 = k0 + kb;
             const int kb1 = max(0, min(kNB, M - c1));
-            // Slices of 16 rows below the diagonal block: w, w + 8, ... (the
+            // Slices of 16 rows below the diagonal block: w, w + 12, ... (the
             // first is panel p+1's rows, warp 0's, and warp 0 always runs).
             // The first slice of a warp runs with the factorization, the
             // others reuse the factor it leaves in the lower lanes.

@@ -231,31 +231,31 @@ def test_large_blocks_deterministic_and_served(bvlib):
         assert srv.evaluate(j, th) == v[0]
 
 
-@pytest.mark.parametrize("cs", [180, 200])
+@pytest.mark.parametrize("cs", [195, 205])
 def test_large_shared_memory_blocks(bvlib, oracle, cs):
-    """Blocks of M = cs + bs ~ 190-230, which run the warp-specialised
+    """Blocks of M = cs + bs ~ 200-230, which run the warp-specialised
     schedule in shared memory (the headline workload's path)."""
     L = _gen(bvlib, 3000, 200, cs)
     M = L.batchNum[1:] + cs
-    assert M.min() > 150 and M.max() <= 230
+    assert M.min() > 190 and M.max() <= 230
     _check(bvlib, oracle, L, thetas=THETAS[:4])
 
 
 def test_both_schedules_in_one_launch(bvlib, oracle):
-    """cs = 140: blocks on both sides of the size at which the kernel switches
-    from the panel-parallel to the warp-specialised schedule."""
-    L = _gen(bvlib, 4000, 300, 140)
-    M = L.batchNum[1:] + 140
-    assert (M <= 150).any() and (M > 150).any()
+    """cs = 180: blocks on both sides of the size (M = 190) at which the kernel
+    switches from the panel-parallel to the warp-specialised schedule."""
+    L = _gen(bvlib, 3000, 200, 180)
+    M = L.batchNum[1:] + 180
+    assert (M <= 190).any() and (M > 190).any()
     _check(bvlib, oracle, L, thetas=THETAS[:3])
 
 
 def test_failure_policy_large_blocks(bvlib):
-    """Singular covariances (duplicated locations) in blocks of M = 180-190,
+    """Singular covariances (duplicated locations) in blocks of M = 195,
     which run the warp-specialised schedule: reported, -inf by default,
     finite under 'continue', and the same on a second evaluation."""
     rng = np.random.default_rng(5)
-    cs = 170
+    cs = 175
     first = rng.random((160, 2))
     block0 = np.concatenate([first, first[:20]])     # 20 locations twice in block 0
     rest = rng.random((60, 2))
