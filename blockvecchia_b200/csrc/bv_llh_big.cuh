@@ -335,23 +335,32 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
             }
         }
         __syncthreads();
-        // Rows below the diagonal block: forward substitution against L_kk.
+        // Rows below the diagonal block: forward substitution against L_kk,
+        // the two operands on step q+1's dependent chain (1 / L_{q+1,q+1} and
+        // L_{q+2,q+1}) read one step ahead.
         for (int r = k0 + kb + tid; r < Mp; r += kThreads) {
             double *row = cur + (r - k0) * 16;
             double w[kNB];
 #pragma unroll
             for (int c = 0; c < kNB; ++c) w[c] = (c < kb) ? row[swz(r, c)] : 0.0;
+            double inv_q = sh.inv[0];
+            double l_next = sh.Lt[0][1];
 #pragma unroll
             for (int q = 0; q < kNB; ++q) {
                 if (q < kb) {
                     asm volatile("" ::: "memory");
+                    const double inv_cur = inv_q;
+                    const double l_cur = l_next;
+                    if (q + 1 < kNB) inv_q = sh.inv[q + 1];
+                    if (q + 2 < kNB) l_next = sh.Lt[q + 1][q + 2];
                     double2 col[kNB / 2];
                     const double2 *srcp = reinterpret_cast<const double2 *>(sh.Lt[q]);
 #pragma unroll
-                    for (int h = 0; h < kNB / 2; ++h) col[h] = srcp[h];
-                    w[q] *= sh.inv[q];
+                    for (int h = (q + 2) >> 1; h < kNB / 2; ++h) col[h] = srcp[h];
+                    w[q] *= inv_cur;
+                    if (q + 1 < kNB) w[q + 1] = fma(-w[q], l_cur, w[q + 1]);
 #pragma unroll
-                    for (int c = q + 1; c < kNB; ++c) {
+                    for (int c = q + 2; c < kNB; ++c) {
                         const double lc = (c & 1) ? col[c >> 1].y : col[c >> 1].x;
                         w[c] = fma(-w[q], lc, w[c]);
                     }
