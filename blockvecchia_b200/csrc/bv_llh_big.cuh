@@ -228,36 +228,15 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         const int n0 = k0 + kb;                       // first row / column of panel p+1
         const int kb1 = max(0, min(kNB, M - n0));     // its width
         if (warp == 0) {
-            // Crout factorization of the diagonal block (lane r < kb owns row k0+r).
+            // Lagged Crout factorization of the diagonal block (lane r < kb
+            // owns row k0+r; factor_rows, the upper lanes idle).
             const bool valid = lane < kb;
             const int row = k0 + lane;
-            double v[kNB];
+            double v[kNB], myinv;
 #pragma unroll
             for (int c = 0; c < kNB; ++c)
                 v[c] = (valid && c < kb && c <= lane) ? cur[lane * 16 + swz(row, c)] : 0.0;
-            unsigned fst = 0;
-#pragma unroll
-            for (int q = 0; q < kNB; ++q) {
-                if (q < kb) {
-                    double s4[4] = {v[q], 0.0, 0.0, 0.0};
-#pragma unroll
-                    for (int k = 0; k < q; ++k) {
-                        const double lqk = __shfl_sync(0xffffffffu, v[k], q);
-                        s4[k & 3] = fma(-v[k], lqk, s4[k & 3]);
-                    }
-                    const double s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
-                    const double piv = __shfl_sync(0xffffffffu, s, q);
-                    const bool ok = piv > 0.0;
-                    const double inv = ok ? rsqrt(piv) : 0.0;
-                    if (!ok) fst |= (k0 + q < mc) ? BV_ST_COND_FAIL : BV_ST_SCHUR_FAIL;
-                    if (lane == q) {
-                        v[q] = ok ? piv * inv : piv;
-                        sh.inv[q] = inv;
-                    } else if (lane > q) {
-                        v[q] = s * inv;
-                    }
-                }
-            }
+            const unsigned fst = factor_rows(k0, kb, mc, v, myinv);
             if (valid) {
 #pragma unroll
                 for (int c = 0; c < kNB; ++c)
@@ -265,11 +244,8 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
             }
             if (lane < kNB) {
 #pragma unroll
-                for (int c = 0; c < kNB; ++c) {
-                    const double lv = (c <= lane && lane < kb) ? v[c] : 0.0;
-                    sh.Lt[c][lane] = lv;
-                }
-                if (lane >= kb) sh.inv[lane] = 0.0;
+                for (int c = 0; c < kNB; ++c) sh.Lt[c][lane] = (c <= lane && lane < kb) ? v[c] : 0.0;
+                sh.inv[lane] = (lane < kb) ? myinv : 0.0;
             }
             if (lane == 0) st |= fst;
         } else if (kb1 > 0) {
