@@ -430,18 +430,14 @@ __device__ __forceinline__ void publish_diag(BlockShared &sh, const double (&v)[
     const int lane = threadIdx.x & 31;
     const bool low = lane < kNB;
     const int r = low ? lane : lane - kNB;
-    if (low) {
+    // One store per column for both halves of the warp (per-lane address).
 #pragma unroll
-        for (int c = 0; c < kNB; ++c) {
-            const double l = (c <= r && r < kb) ? v[c] : 0.0;
-            sh.Lt[c][r] = l;
-        }
-        sh.inv[r] = (r < kb) ? myinv : 0.0;
-    } else {
-        const bool valid = r < kb1;
-#pragma unroll
-        for (int c = 0; c < kNB; ++c) sh.Lnx[r][c] = (valid && c < kb) ? v[c] : 0.0;
+    for (int c = 0; c < kNB; ++c) {
+        const bool keep = low ? (c <= r && r < kb) : (r < kb1 && c < kb);
+        double *dst = low ? &sh.Lt[c][r] : &sh.Lnx[r][c];
+        *dst = keep ? v[c] : 0.0;
     }
+    if (low) sh.inv[r] = (r < kb) ? myinv : 0.0;
 }
 
 __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b)
