@@ -155,6 +155,8 @@ struct alignas(16) BlockShared {
     uint64_t bar_nc[2];         // bulk warps -> chain warps: panel p+1's columns took panel p-1
     unsigned ph_ls[2], ph_nc[2];  // phases those four barriers completed before this block
     int work_next[4];           // next bulk work item, by (2 p + stage) mod 4
+    uint64_t bar_g0[2];         // bulk -> critical rows: panel p's first row group is up to date (by parity)
+    unsigned ph_g0[2];          // phases bar_g0 completed before this block
     unsigned status;
     int task;
 };
@@ -174,6 +176,10 @@ __device__ __forceinline__ void init_block_sync(BlockShared &sh)
             sh.ph_ls[i] = sh.ph_nc[i] = 0;
         }
         for (int i = 0; i < 4; ++i) sh.work_next[i] = 0;
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&sh.bar_g0[i], 1);
+            sh.ph_g0[i] = 0;
+        }
         fence_mbar_init();
     }
     __syncthreads();
@@ -560,18 +566,9 @@ __device__ __forceinline__ void update_diag_block(double *A, int Mp, int k0, int
 // broadcasts behind a compiler fence so the factor values are not all
 // hoisted into registers.  The two values on the dependent chain of step
 // q + 1 (1 / L_{q+1,q+1} and L_{q+2,q+1}) are read one step ahead.
-__device__ __forceinline__ void solve_rows(double *A, int Mp, int k0, int kb, int base, int nl,
-                                           const BlockShared &sh)
+// The substitution itself on one row held in w (solve_rows).
+__device__ __forceinline__ void solve_row_regs(double (&w)[kNB], int kb, const BlockShared &sh)
 {
-    const int lane = threadIdx.x & 31;
-    const int r = base + lane;
-    if (lane >= nl || r >= Mp) return;
-    int cof[kNB];
-#pragma unroll
-    for (int c = 0; c < kNB; ++c) cof[c] = poff(k0 + (c < kb ? c : 0), Mp);
-    double w[kNB];
-#pragma unroll
-    for (int c = 0; c < kNB; ++c) w[c] = (c < kb) ? A[cof[c] + r] : 0.0;
     double inv_q = sh.inv[0];
     double l_next = sh.Lt[0][1];
 #pragma unroll
@@ -595,6 +592,21 @@ __device__ __forceinline__ void solve_rows(double *A, int Mp, int k0, int kb, in
             }
         }
     }
+}
+
+__device__ __forceinline__ void solve_rows(double *A, int Mp, int k0, int kb, int base, int nl,
+                                           const BlockShared &sh)
+{
+    const int lane = threadIdx.x & 31;
+    const int r = base + lane;
+    if (lane >= nl || r >= Mp) return;
+    int cof[kNB];
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) cof[c] = poff(k0 + (c < kb ? c : 0), Mp);
+    double w[kNB];
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) w[c] = (c < kb) ? A[cof[c] + r] : 0.0;
+    solve_row_regs(w, kb, sh);
 #pragma unroll
     for (int c = 0; c < kNB; ++c)
         if (c < kb) A[cof[c] + r] = w[c];
@@ -683,6 +695,7 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
     const int P = (M + kNB - 1) / kNB;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const unsigned base = sh.phase_base;
+    const unsigned g0b[2] = {sh.ph_g0[0], sh.ph_g0[1]};
     bool timed_out = false;
     if (warp == 0) {
         for (int p = 0; p < P; ++p) {
@@ -722,10 +735,38 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
             const int kb1 = max(0, min(kNB, M - n0));
             const int n1 = n0 + kb1;
             const int n2 = min(Mp, n1 + kNB);
-            if (!mbar_wait_bounded(&sh.bar_lready, (base + p) & 1u)) timed_out = true;
             // The 16 rows below panel p+1: solved in panel p, then brought up
-            // to date in panel p+1's columns (panels p and p-1).
-            solve_rows(A, Mp, k0, kb, n1, n2 - n1, sh);
+            // to date in panel p+1's columns (panels p and p-1).  Their panel-p
+            // values are read while warp 0 still factors: final once the
+            // previous panel's first bulk row group (these rows, when the
+            // previous panel had bulk groups) has taken its update.
+            {
+                const int r = n1 + lane;
+                const bool act = lane < n2 - n1;
+                if (p > 0 && Mp > min(Mp, min(kNB * (p + 1), M) + kNB)) {
+                    const int k = (p - 1) & 1;
+                    if (!mbar_wait_bounded(&sh.bar_g0[k], (g0b[k] + ((p - 1) >> 1)) & 1u)) timed_out = true;
+                }
+                int cof[kNB];
+                {
+                    int o = poff(k0, Mp);
+#pragma unroll
+                    for (int c = 0; c < kNB; ++c) {
+                        cof[c] = o;
+                        o += Mp - (k0 + c) - 1;
+                    }
+                }
+                double w[kNB];
+#pragma unroll
+                for (int c = 0; c < kNB; ++c) w[c] = (act && c < kb) ? A[cof[c] + r] : 0.0;
+                if (!mbar_wait_bounded(&sh.bar_lready, (base + p) & 1u)) timed_out = true;
+                if (act) {
+                    solve_row_regs(w, kb, sh);
+#pragma unroll
+                    for (int c = 0; c < kNB; ++c)
+                        if (c < kb) A[cof[c] + r] = w[c];
+                }
+            }
             __syncwarp();
             if (kb1 > 0 && n2 > n1) update_next_rows16(A, Mp, k0, kb, n0, kb1, n1, p > 0, sh);
             __syncwarp();
@@ -768,6 +809,11 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
                     __syncwarp();
                     if (kb1 > 0) {
                         update_next_rows16(A, Mp, k0, kb, n0, kb1, rb, p > 0, sh);
+                        if (item == 0) {
+                            // The next panel's critical rows are up to date.
+                            __syncwarp();
+                            if (lane == 0) mbar_arrive(&sh.bar_g0[p & 1]);
+                        }
                         if (rb + 16 < Mp) update_next_rows16(A, Mp, k0, kb, n0, kb1, rb + 16, p > 0, sh);
                     }
                 } else {
@@ -786,7 +832,15 @@ __device__ __forceinline__ void cholesky_ws(double *A, int M, int mc, BlockShare
     }
     if (timed_out) atomicOr(&sh.status, kStDeviceTimeout);
     __syncthreads();
-    if (tid == 0) sh.phase_base = base + (unsigned)P;
+    if (tid == 0) {
+        sh.phase_base = base + (unsigned)P;
+        // bar_g0[k] took one arrival per panel p = k, k+2, ... with bulk row
+        // groups (those panels are a prefix 0..pg-1).
+        int pg = 0;
+        while (pg < P && Mp > min(Mp, min(kNB * (pg + 2), M) + kNB)) ++pg;
+        sh.ph_g0[0] = g0b[0] + (unsigned)((pg + 1) >> 1);
+        sh.ph_g0[1] = g0b[1] + (unsigned)(pg >> 1);
+    }
 }
 
 // ---------------------------------------------------------------------------
