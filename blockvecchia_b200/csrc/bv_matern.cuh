@@ -78,8 +78,10 @@ inline void matern_prepare(MaternParams &p)
 }
 
 // K_mu(x), K_{mu+1}(x) for |mu| <= 1/2 and 0 < x < 2 (Temme's series), with
-// lx = log(2/x) and ix = 1/x from the caller.  One reciprocal per term:
-// 1/(k - mu) = (k + mu) / (k^2 - mu^2) and likewise 1/(k + mu).
+// lx = log(2/x) and ix = 1/x from the caller.  1/(k - mu) = (k + mu) /
+// (k^2 - mu^2) and likewise 1/(k + mu); the reciprocals of each term depend
+// on k and mu only, so they are multiplied in rather than divided by and stay
+// off the chain of loop-carried values.
 __device__ __forceinline__ void temme_series(double x, double lx, double ix, const MaternParams &mp,
                                              double &kmu, double &kmu1)
 {
@@ -115,7 +117,7 @@ __device__ __forceinline__ void temme_series(double x, double lx, double ix, con
         const double kk = (double)k;
         const double r = 1.0 / fma(kk, kk, -m2);
         f = (kk * f + p + q) * r;
-        c *= d / kk;
+        c *= d * (1.0 / kk);
         p *= (kk + mu) * r;
         q *= (kk - mu) * r;
         const double t0 = c * f;
@@ -132,7 +134,9 @@ __device__ __forceinline__ void temme_series(double x, double lx, double ix, con
 // Temme's continued fraction (N. M. Temme, J. Comput. Phys. 19 (1975)
 // 324-337), the method GSL's K_nu uses for x >= 2.  The fraction for
 // K_{mu+1}/K_mu and the series normalising K_mu are summed together; a few
-// dozen iterations of plain arithmetic, one exp and one sqrt.
+// dozen iterations of plain arithmetic, one exp and one sqrt.  Term i uses
+// a_i = -(1/4 - mu^2) - i(i-1) and the reciprocals of i and a_i, which do not
+// depend on x; only 1/(b + a d) is a division on the recurrence.
 __device__ __forceinline__ void steed_cf2(double mu, double x, double &kmu, double &kmu1)
 {
     const double a1 = 0.25 - mu * mu;
@@ -140,12 +144,12 @@ __device__ __forceinline__ void steed_cf2(double mu, double x, double &kmu, doub
     double d = 1.0 / b;
     double h = d, delh = d;
     double q1 = 0.0, q2 = 1.0;
-    double q = a1, c = a1, a = -a1;
+    double q = a1, c = a1;
     double s = 1.0 + q * delh;
     for (int i = 2; i < 20000; ++i) {
-        a -= 2.0 * (double)(i - 1);
-        c = -a * c / (double)i;
-        const double qn = (q1 - b * q2) / a;
+        const double a = -a1 - (double)(i * (i - 1));
+        c = -a * c * (1.0 / (double)i);
+        const double qn = (q1 - b * q2) * (1.0 / a);
         q1 = q2;
         q2 = qn;
         q += c * qn;
