@@ -77,6 +77,17 @@ inline void matern_prepare(MaternParams &p)
     p.fact = (std::fabs(pimu) < 1e-300) ? 1.0 : pimu / std::sin(pimu);
 }
 
+// 1/k for k = 1..kRecipN, folded at compile time (correctly rounded, the same
+// bits as the division), read from the constant cache by the K_nu loops.
+constexpr int kRecipN = 48;
+#define BV_R4(k) 1.0 / (k), 1.0 / ((k) + 1.0), 1.0 / ((k) + 2.0), 1.0 / ((k) + 3.0)
+static __constant__ double kRecip[kRecipN] = {
+    BV_R4(1.0),  BV_R4(5.0),  BV_R4(9.0),  BV_R4(13.0), BV_R4(17.0), BV_R4(21.0),
+    BV_R4(25.0), BV_R4(29.0), BV_R4(33.0), BV_R4(37.0), BV_R4(41.0), BV_R4(45.0)};
+#undef BV_R4
+
+__device__ __forceinline__ double recip_int(int k) { return (k <= kRecipN) ? kRecip[k - 1] : 1.0 / (double)k; }
+
 // K_mu(x), K_{mu+1}(x) for |mu| <= 1/2 and 0 < x < 2 (Temme's series), with
 // lx = log(2/x) and ix = 1/x from the caller.  1/(k - mu) = (k + mu) /
 // (k^2 - mu^2) and likewise 1/(k + mu); the reciprocals of each term depend
@@ -117,7 +128,7 @@ __device__ __forceinline__ void temme_series(double x, double lx, double ix, con
         const double kk = (double)k;
         const double r = 1.0 / fma(kk, kk, -m2);
         f = (kk * f + p + q) * r;
-        c *= d * (1.0 / kk);
+        c *= d * recip_int(k);
         p *= (kk + mu) * r;
         q *= (kk - mu) * r;
         const double t0 = c * f;
@@ -148,7 +159,7 @@ __device__ __forceinline__ void steed_cf2(double mu, double x, double &kmu, doub
     double s = 1.0 + q * delh;
     for (int i = 2; i < 20000; ++i) {
         const double a = -a1 - (double)(i * (i - 1));
-        c = -a * c * (1.0 / (double)i);
+        c = -a * c * recip_int(i);
         const double qn = (q1 - b * q2) * (1.0 / a);
         q1 = q2;
         q2 = qn;
