@@ -6,12 +6,13 @@
 // --num_loc --knn --perf --seed --xy_path --obs_path --tol --maxiter
 // --omp_threads --permutation --dist_scale --lower_bound --upper_bound.
 // --perf evaluates once at --ikernel with zero observations on GenerateXYLoc
-// locations; otherwise the locations/observations CSVs are fitted from
-// --kernel_init.  The objective is bv_llh (the NLopt signature of
-// llh_Xvecchia_batch); NLopt BOBYQA is used when <nlopt.h> exists at build
-// time, else a bounded Nelder-Mead (Nelder & Mead, Comput. J. 7 (1965)
-// 308-313) with the same stopping rule (relative change of the parameters
-// below --tol, at most --maxiter evaluations).  Additional flags:
+// locations and writes the blocks' points and conditioning points to
+// ./log/points_Random.csv and ./log/neighbors_Random.csv; otherwise the
+// locations/observations CSVs are fitted from --kernel_init.  The objective
+// is bv_llh (the NLopt signature of llh_Xvecchia_batch); NLopt BOBYQA is used
+// when <nlopt.h> exists at build time, else a bounded Nelder-Mead (Nelder &
+// Mead, Comput. J. 7 (1965) 308-313) with the same stopping rule (relative
+// change of the parameters below --tol, at most --maxiter evaluations).  Additional flags:
 // --precision fp64|mixed, --device N, --print-opts (print the parsed options
 // as JSON and exit; needs no GPU).
 #include <sys/stat.h>
@@ -348,6 +349,23 @@ int main(int argc, char **argv)
             for (int t = 0; t < cs; ++t) knn[t] = t;
             for (int i = 1; i < bc; ++i)
                 for (int t = 0; t < cs; ++t) knn[(size_t)i * cs + t] = acc[i] - cs + t;
+        }
+    }
+    if (o.perf) {
+        // src/test_Xvecchia_batch.cpp:405-451 with random ordering (the only
+        // ordering here): every block's points with the block's index, then
+        // every block's cs conditioning points with the block's index (block
+        // 0's are the first cs points, as the reference fills them at :359-361).
+        mkdir("./log", 0755);
+        std::ofstream pts("./log/points_Random.csv");
+        pts << "x,y,cluster\n";
+        for (int i = 0; i < bc; ++i)
+            for (int j = 0; j < bn[i]; ++j) pts << xn[acc[i] + j] << "," << yn[acc[i] + j] << "," << i << "\n";
+        std::ofstream nbr("./log/neighbors_Random.csv");
+        nbr << "x,y,cluster\n";
+        for (size_t t = 0; t < (size_t)bc * cs; ++t) {
+            const int src = (t < (size_t)cs) ? (int)t : knn[t];
+            nbr << xn[src] << "," << yn[src] << "," << t / cs << "\n";
         }
     }
     fprintf(stderr, "--------------Nearest Neighbor Done-----------------\n");

@@ -43,6 +43,19 @@ def test_perf_mode_matches_oracle(exe, bvlib, oracle, tmp_path):
     P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, knn, cs)
     ref = oracle.llh(P, (1.5, 0.1, 0.5))
     assert abs(llk - ref) <= 1e-10 * abs(ref)
+    # The perf-mode dumps (src/test_Xvecchia_batch.cpp:405-451), in the
+    # stream's default 6-significant-digit format: each block's points, then
+    # each block's conditioning points (block 0: the first cs points).
+    g = lambda v: f"{v:g}"
+    pts = (tmp_path / "log" / "points_Random.csv").read_text().splitlines()
+    assert pts[0] == "x,y,cluster" and len(pts) == n + 1
+    cl = np.repeat(np.arange(len(L.batchNum)), L.batchNum)
+    assert pts[1:] == [f"{g(a)},{g(b)},{c}" for a, b, c in zip(L.x, L.y, cl)]
+    nbr = (tmp_path / "log" / "neighbors_Random.csv").read_text().splitlines()
+    bc_eff = len(L.batchNum)
+    assert nbr[0] == "x,y,cluster" and len(nbr) == bc_eff * cs + 1
+    src = np.concatenate([np.arange(cs), np.asarray(knn).reshape(-1)[cs:]])
+    assert nbr[1:] == [f"{g(L.x[s])},{g(L.y[s])},{t // cs}" for t, s in enumerate(src)]
 
 
 def test_fit_matches_oracle_fit(exe, bvlib, oracle, tmp_path):
