@@ -88,105 +88,151 @@ static __constant__ double kRecip[kRecipN] = {
 
 __device__ __forceinline__ double recip_int(int k) { return (k <= kRecipN) ? kRecip[k - 1] : 1.0 / (double)k; }
 
-// K_mu(x), K_{mu+1}(x) for |mu| <= 1/2 and 0 < x < 2 (Temme's series), with
-// lx = log(2/x) and ix = 1/x from the caller.  1/(k - mu) = (k + mu) /
-// (k^2 - mu^2) and likewise 1/(k + mu); the reciprocals of each term depend
-// on k and mu only, so they are multiplied in rather than divided by and stay
-// off the chain of loop-carried values.
-__device__ __forceinline__ void temme_series(double x, double lx, double ix, const MaternParams &mp,
-                                             double &kmu, double &kmu1)
+// K_mu(x), K_{mu+1}(x) for |mu| <= 1/2 and 0 < x < 2 (Temme's series),
+// written for N arguments at once (their chains interleave and share each
+// term's factors; matern_general uses N = 1, which runs faster than the same
+// loop with a plain break, and a two-argument form measured slower), with
+// lx = log(2/x) and ix = 1/x from the caller.  1/(k - mu) =
+// (k + mu) / (k^2 - mu^2) and likewise 1/(k + mu); the reciprocals of each
+// term depend on k and mu only, so they are multiplied in rather than divided
+// by and stay off the chain of loop-carried values.  An argument whose sum
+// has converged keeps it while the others run on, so every argument gets the
+// bits it gets alone.
+template <int N>
+__device__ __forceinline__ void temme_series(const double (&x)[N], const double (&lx)[N],
+                                             const double (&ix)[N], const MaternParams &mp,
+                                             double (&kmu)[N], double (&kmu1)[N])
 {
     const double mu = mp.mu;
     const double m2 = mu * mu;
-    const double sigma = mu * lx;
-    const double e = exp(sigma);  // (x/2)^(-mu)
-    const double ie = 1.0 / e;
-    const double ch = 0.5 * (e + ie);
-    double shs;                   // sinh(sigma) / sigma
-    if (fabs(sigma) < 0.5) {
-        // sum_k sigma^(2k) / (2k+1)!, truncated below 1e-19 relative
-        const double s2 = sigma * sigma;
-        double t = 1.0 / 355687428096000.0;  // 1/17!
-        t = fma(t, s2, 1.0 / 1307674368000.0);
-        t = fma(t, s2, 1.0 / 6227020800.0);
-        t = fma(t, s2, 1.0 / 39916800.0);
-        t = fma(t, s2, 1.0 / 362880.0);
-        t = fma(t, s2, 1.0 / 5040.0);
-        t = fma(t, s2, 1.0 / 120.0);
-        t = fma(t, s2, 1.0 / 6.0);
-        shs = fma(t, s2, 1.0);
-    } else {
-        shs = 0.5 * (e - ie) / sigma;
+    double f[N], p[N], q[N], c[N], d[N], s0[N], s1[N];
+    bool done[N];
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+        const double sigma = mu * lx[n];
+        const double e = exp(sigma);  // (x/2)^(-mu)
+        const double ie = 1.0 / e;
+        const double ch = 0.5 * (e + ie);
+        double shs;                   // sinh(sigma) / sigma
+        if (fabs(sigma) < 0.5) {
+            // sum_k sigma^(2k) / (2k+1)!, truncated below 1e-19 relative
+            const double s2 = sigma * sigma;
+            double t = 1.0 / 355687428096000.0;  // 1/17!
+            t = fma(t, s2, 1.0 / 1307674368000.0);
+            t = fma(t, s2, 1.0 / 6227020800.0);
+            t = fma(t, s2, 1.0 / 39916800.0);
+            t = fma(t, s2, 1.0 / 362880.0);
+            t = fma(t, s2, 1.0 / 5040.0);
+            t = fma(t, s2, 1.0 / 120.0);
+            t = fma(t, s2, 1.0 / 6.0);
+            shs = fma(t, s2, 1.0);
+        } else {
+            shs = 0.5 * (e - ie) / sigma;
+        }
+        f[n] = mp.fact * (mp.g1 * ch + mp.g2 * lx[n] * shs);
+        p[n] = 0.5 * e * mp.gam_p;
+        q[n] = 0.5 * ie * mp.gam_m;
+        c[n] = 1.0;
+        d[n] = 0.25 * x[n] * x[n];
+        s0[n] = f[n];
+        s1[n] = p[n];
+        done[n] = false;
     }
-    double f = mp.fact * (mp.g1 * ch + mp.g2 * lx * shs);
-    double p = 0.5 * e * mp.gam_p;
-    double q = 0.5 * ie * mp.gam_m;
-    double c = 1.0;
-    const double d = 0.25 * x * x;
-    double s0 = f, s1 = p;
     for (int k = 1; k < 200; ++k) {
         const double kk = (double)k;
         const double r = 1.0 / fma(kk, kk, -m2);
-        f = (kk * f + p + q) * r;
-        c *= d * recip_int(k);
-        p *= (kk + mu) * r;
-        q *= (kk - mu) * r;
-        const double t0 = c * f;
-        const double t1 = c * (p - kk * f);
-        s0 += t0;
-        s1 += t1;
-        if (fabs(t0) < 1e-17 * fabs(s0) && fabs(t1) < 1e-17 * fabs(s1)) break;
+        const double ik = recip_int(k);
+        bool all = true;
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            f[n] = (kk * f[n] + p[n] + q[n]) * r;
+            c[n] *= d[n] * ik;
+            p[n] *= (kk + mu) * r;
+            q[n] *= (kk - mu) * r;
+            const double t0 = c[n] * f[n];
+            const double t1 = c[n] * (p[n] - kk * f[n]);
+            const double n0 = s0[n] + t0, n1 = s1[n] + t1;
+            const bool conv = fabs(t0) < 1e-17 * fabs(n0) && fabs(t1) < 1e-17 * fabs(n1);
+            s0[n] = done[n] ? s0[n] : n0;
+            s1[n] = done[n] ? s1[n] : n1;
+            done[n] = done[n] || conv;
+            all = all && done[n];
+        }
+        if (all) break;
     }
-    kmu = s0;
-    kmu1 = s1 * 2.0 * ix;
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+        kmu[n] = s0[n];
+        kmu1[n] = s1[n] * 2.0 * ix[n];
+    }
 }
 
 // K_mu(x) and K_{mu+1}(x) for x >= 2, |mu| <= 1/2: Steed's algorithm for
 // Temme's continued fraction (N. M. Temme, J. Comput. Phys. 19 (1975)
-// 324-337), the method GSL's K_nu uses for x >= 2.  The fraction for
-// K_{mu+1}/K_mu and the series normalising K_mu are summed together; a few
-// dozen iterations of plain arithmetic, one exp and one sqrt.  Term i uses
-// a_i = -(1/4 - mu^2) - i(i-1) and the reciprocals of i and a_i, which do not
-// depend on x; only 1/(b + a d) is a division on the recurrence.
-__device__ __forceinline__ void steed_cf2(double mu, double x, double &kmu, double &kmu1)
+// 324-337), the method GSL's K_nu uses for x >= 2, written for N arguments
+// as above.  The fraction for K_{mu+1}/K_mu and the series normalising K_mu
+// are summed together; a few dozen iterations of plain arithmetic, one exp
+// and one sqrt.  Term i uses a_i = -(1/4 - mu^2) - i(i-1) and the
+// reciprocals of i and a_i, which do not depend on x; only 1/(b + a d) is a
+// division on the recurrence.
+template <int N>
+__device__ __forceinline__ void steed_cf2(double mu, const double (&x)[N], double (&kmu)[N],
+                                          double (&kmu1)[N])
 {
     const double a1 = 0.25 - mu * mu;
-    double b = 2.0 * (1.0 + x);
-    double d = 1.0 / b;
-    double h = d, delh = d;
-    double q1 = 0.0, q2 = 1.0;
-    double q = a1, c = a1;
-    double s = 1.0 + q * delh;
+    double b[N], d[N], h[N], delh[N], q1[N], q2[N], q[N], c[N], s[N];
+    bool done[N];
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+        b[n] = 2.0 * (1.0 + x[n]);
+        d[n] = 1.0 / b[n];
+        h[n] = d[n];
+        delh[n] = d[n];
+        q1[n] = 0.0;
+        q2[n] = 1.0;
+        q[n] = a1;
+        c[n] = a1;
+        s[n] = 1.0 + q[n] * delh[n];
+        done[n] = false;
+    }
     for (int i = 2; i < 20000; ++i) {
         const double a = -a1 - (double)(i * (i - 1));
-        c = -a * c * recip_int(i);
-        const double qn = (q1 - b * q2) * (1.0 / a);
-        q1 = q2;
-        q2 = qn;
-        q += c * qn;
-        b += 2.0;
-        d = 1.0 / (b + a * d);
-        delh = (b * d - 1.0) * delh;
-        h += delh;
-        const double dels = q * delh;
-        s += dels;
-        if (fabs(dels) < 1e-17 * fabs(s)) break;
+        const double ii = recip_int(i);
+        const double ia = 1.0 / a;
+        bool all = true;
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            c[n] = -a * c[n] * ii;
+            const double qn = (q1[n] - b[n] * q2[n]) * ia;
+            q1[n] = q2[n];
+            q2[n] = qn;
+            q[n] += c[n] * qn;
+            b[n] += 2.0;
+            d[n] = 1.0 / (b[n] + a * d[n]);
+            delh[n] = (b[n] * d[n] - 1.0) * delh[n];
+            const double dels = q[n] * delh[n];
+            const double sn = s[n] + dels;
+            const bool conv = fabs(dels) < 1e-17 * fabs(sn);
+            h[n] = done[n] ? h[n] : h[n] + delh[n];
+            s[n] = done[n] ? s[n] : sn;
+            done[n] = done[n] || conv;
+            all = all && done[n];
+        }
+        if (all) break;
     }
-    h = a1 * h;
-    kmu = sqrt(3.14159265358979323846 / (2.0 * x)) * exp(-x) / s;
-    kmu1 = kmu * (mu + x + 0.5 - h) / x;
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+        const double hh = a1 * h[n];
+        kmu[n] = sqrt(3.14159265358979323846 / (2.0 * x[n])) * exp(-x[n]) / s[n];
+        kmu1[n] = kmu[n] * (mu + x[n] + 0.5 - hh) / x[n];
+    }
 }
 
-// con * r^nu * K_nu(r) for general nu (out of line: long and rare).
-static __device__ __noinline__ double matern_general(double r, const MaternParams &mp)
+// Upward recurrence K_{m+1} = 2m/x K_m + K_{m-1} to order nu, then
+// con * x^nu * K_nu(x).
+__device__ __forceinline__ double matern_knu_finish(double lr, double ix, double k0, double k1,
+                                                    const MaternParams &mp)
 {
-    const double lr = log(r);
-    const double ix = 1.0 / r;
-    double k0, k1;
-    if (r < 2.0)
-        temme_series(r, 0.6931471805599453094 - lr, ix, mp, k0, k1);
-    else
-        steed_cf2(mp.mu, r, k0, k1);
     for (int j = 1; j <= mp.nn; ++j) {
         const double m = mp.mu + (double)j;
         const double k2 = 2.0 * m * ix * k1 + k0;
@@ -195,6 +241,22 @@ static __device__ __noinline__ double matern_general(double r, const MaternParam
     }
     const double nu = mp.nu < 0 ? -mp.nu : mp.nu;
     return mp.con * exp(nu * lr) * k0;
+}
+
+// con * r^nu * K_nu(r) for general nu and r > 0 (out of line: long).
+static __device__ __noinline__ double matern_general(double r, const MaternParams &mp)
+{
+    const double lr[1] = {log(r)};
+    const double ix[1] = {1.0 / r};
+    const double x[1] = {r};
+    double k0[1], k1[1];
+    if (r < 2.0) {
+        const double lx[1] = {0.6931471805599453094 - lr[0]};
+        temme_series<1>(x, lx, ix, mp, k0, k1);
+    } else {
+        steed_cf2<1>(mp.mu, x, k0, k1);
+    }
+    return matern_knu_finish(lr[0], ix[0], k0[0], k1[0], mp);
 }
 
 // a / b from the correctly rounded reciprocal y = RN(1/b) with one
