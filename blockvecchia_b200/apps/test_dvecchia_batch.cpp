@@ -365,6 +365,7 @@ int main(int argc, char **argv)
         nbr << "x,y,cluster\n";
         for (size_t t = 0; t < (size_t)bc * cs; ++t) {
             const int src = (t < (size_t)cs) ? (int)t : knn[t];
+            if (src < 0 || src >= n) continue;  // "previous cs points" before an early block
             nbr << xn[src] << "," << yn[src] << "," << t / cs << "\n";
         }
     }
