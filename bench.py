@@ -384,7 +384,7 @@ def run_ours(args):
                 sm_ = Mx.status()
                 sweep.append({"range": rg_, "rel_err": abs(vm_ - v64_) / abs(v64_) if v64_ else None,
                               "fp32_fallback_blocks": sm_["fp32_fallback"],
-                              "fp64_failed_blocks": s64_["cond_fail"] + s64_["schur_fail"]})
+                              "fp64_failed_blocks": s64_["failed"]})
             D(theta)
         mixed = {"value": args.steps / (ms_mx / 1e3), "unit": "evals/s",
                  "vs_fp64": (args.steps / (ms_mx / 1e3)) / (args.steps / (ms / 1e3)),
@@ -419,7 +419,7 @@ def run_ours(args):
                    "cs": w["cs"], "nu": w["nu"], "sigma2": w["sigma2"], "range": w["range"],
                    "precision": args.precision, "kmeans_epochs": w["kmeans_epochs"],
                    "l2": "flushed between evaluations (256 MB device write, inside the timed region)",
-                   "blocks_failed_fp64": int(st["cond_fail"] + st["schur_fail"]),
+                   "blocks_failed_fp64": int(st["failed"]),
                    "setup_layout_knn_s": round(setup_layout_s, 2)},
         "e2e": {"value": args.steps / (ms_e2e / 1e3), "unit": "evals/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": 48},

@@ -41,6 +41,7 @@ EXPORTS = {
     "bv_llh": (C.c_double, [C.c_uint, _D, _D, C.c_void_p]),
     "bv_llh_eval": (C.c_int, [C.c_void_p, _D, _D]),
     "bv_block_llk": (C.c_int, [C.c_void_p, _D, C.c_int]),
+    "bv_block_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint), C.c_int]),
     "bv_get_status": (C.c_int, [C.c_void_p, C.c_void_p]),
     "bv_iterations": (C.c_int, [C.c_void_p]),
     "bv_last_error": (C.c_char_p, []),
@@ -88,7 +89,8 @@ class BvOpts(C.Structure):
 class BvStatus(C.Structure):
     _fields_ = [("blocks", C.c_int), ("cond_fail", C.c_int), ("schur_fail", C.c_int),
                 ("fp32_fallback", C.c_int), ("nonfinite", C.c_int), ("flags_or", C.c_uint),
-                ("llk", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double)]
+                ("llk", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double),
+                ("failed", C.c_int)]
 
 
 class BvServerOpts(C.Structure):

@@ -640,6 +640,7 @@ static int eval_locked(bv_handle *h, const double *theta, double *llk)
     s.fp32_fallback = r.fallback;
     s.nonfinite = r.nonfinite;
     s.flags_or = r.flags_or;
+    s.failed = r.failed;
     s.llk = r.llk;
     s.device_ms = ms;
     s.kernel_ms = kms;
@@ -724,6 +725,18 @@ extern "C" int bv_block_llk(bv_handle *h, double *out, int count)
     return BV_OK;
 }
 
+extern "C" int bv_block_status(bv_handle *h, unsigned *out, int count)
+{
+    if (!h || !out || count < h->bc) {
+        set_error("bv_block_status: need room for %d values", h ? h->bc : 0);
+        return BV_E_INVALID;
+    }
+    std::lock_guard<std::mutex> lk(h->mu);
+    BV_CUDA_TRY(cudaSetDevice(h->device));
+    BV_CUDA_TRY(cudaMemcpy(out, h->d_block_status, sizeof(unsigned) * h->bc, cudaMemcpyDeviceToHost));
+    return BV_OK;
+}
+
 extern "C" int bv_get_status(bv_handle *h, bv_status *st)
 {
     if (!h || !st) return BV_E_INVALID;
@@ -780,8 +793,10 @@ static int g_noalloc_smem_max_m[64] = {0};
 
 // Validation of a caller's layout on the device: offsets non-decreasing and
 // ending at n, every block fits in shared memory, every conditioning index of
-// block b >= 1 lies in [0, batchNumAccum[b]).  check[0] = first bad block + 1
-// (offsets/indices), check[1] = largest M.
+// block b >= 1 lies in [0, batchNumAccum[b]), and block 0 holds at least cs
+// points when other blocks condition on it (the rule bv_create applies).
+// check[0] = first bad block + 1 (offsets/indices), check[1] = largest M,
+// check[2] = 1 when block 0 is smaller than cs.
 __global__ void noalloc_check_kernel(const int *acc, const int *knn, int n, int bc, int cs,
                                      int *check, int *order)
 {
@@ -792,6 +807,7 @@ __global__ void noalloc_check_kernel(const int *acc, const int *knn, int n, int 
         bool ok = a0 >= 0 && a1 >= a0 && a1 <= n && (b + 1 < bc || a1 == n) && (b > 0 || a0 == 0);
         const int M = (a1 - a0) + (b == 0 ? 0 : cs);
         atomicMax(&check[1], M);
+        if (b == 0 && cs > 0 && bc > 1 && a1 - a0 < cs) check[2] = 1;
         if (ok && b > 0 && cs > 0) {
             const int *k = knn + (size_t)b * cs;
             for (int t = 0; t < cs; ++t)
@@ -802,6 +818,16 @@ __global__ void noalloc_check_kernel(const int *acc, const int *knn, int n, int 
         }
         if (!ok) atomicCAS(&check[0], 0, b + 1);
     }
+}
+
+// Final value of an allocation-free call: the reduced log-likelihood, or
+// -HUGE_VAL when a block failed or the sum is not finite (the handle's
+// default failure policy, BV_FAIL_NEGINF).
+__global__ void noalloc_result_kernel(const EvalResult *r, double *llk_out)
+{
+    const double v = r->llk;
+    const bool failed = (r->cond_fail + r->schur_fail + r->nonfinite) > 0 || !isfinite(v);
+    *llk_out = failed ? -HUGE_VAL : v;
 }
 
 }  // namespace bv
@@ -854,16 +880,21 @@ extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *ob
     int *order = reinterpret_cast<int *>(base + kNaOrder);
     unsigned *counter = reinterpret_cast<unsigned *>(base + kNaCounter);
     // Validate the layout on the device; read back 8 bytes.
-    BV_CUDA_TRY(cudaMemsetAsync(check, 0, 2 * sizeof(int), s));
+    BV_CUDA_TRY(cudaMemsetAsync(check, 0, 3 * sizeof(int), s));
     noalloc_check_kernel<<<(bc + 255) / 256, 256, 0, s>>>(batchNumAccum, knn_idx, n, bc, cs, check,
                                                           order);
     BV_CUDA_TRY(cudaGetLastError());
-    int hc[2] = {0, 0};
+    int hc[3] = {0, 0, 0};
     BV_CUDA_TRY(cudaMemcpyAsync(hc, check, sizeof(hc), cudaMemcpyDeviceToHost, s));
     BV_CUDA_TRY(cudaStreamSynchronize(s));
     if (hc[0]) {
         set_error("bv_llh_noalloc: block %d has inconsistent offsets or a conditioning index "
                   "outside the earlier blocks", hc[0] - 1);
+        return BV_E_INVALID;
+    }
+    if (hc[2]) {
+        set_error("bv_llh_noalloc: block 0 has fewer than cs=%d points (firstbatch merges "
+                  "clusters until >= cs)", cs);
         return BV_E_INVALID;
     }
     if (hc[1] > smem_max_m) {
@@ -879,7 +910,7 @@ extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *ob
                   nu, dist_scale);
         return BV_E_INVALID;
     }
-    MaternParams mp;
+    MaternParams mp{};
     double con = std::pow(2.0, nu - 1.0) * std::tgamma(nu);
     con = 1.0 / con;
     mp.sigma2 = sigma2;
@@ -933,7 +964,8 @@ extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *ob
     EvalResult *d_res = reinterpret_cast<EvalResult *>(base + kNaResult);
     reduce_kernel<<<1, kReduceThreads, 0, s>>>(a.block_llk, a.block_status, bc, d_res);
     BV_CUDA_TRY(cudaGetLastError());
-    BV_CUDA_TRY(cudaMemcpyAsync(llk_out, &d_res->llk, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    noalloc_result_kernel<<<1, 1, 0, s>>>(d_res, llk_out);
+    BV_CUDA_TRY(cudaGetLastError());
     unsigned flags = 0;
     BV_CUDA_TRY(cudaMemcpyAsync(&flags, &d_res->flags_or, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     BV_CUDA_TRY(cudaStreamSynchronize(s));

@@ -12,12 +12,12 @@ struct EvalResult {
     double llk;
     int blocks, cond_fail, schur_fail, fallback, nonfinite;
     unsigned flags_or;
-    int pad;
+    int failed;  // blocks with a failed pivot in either factor (counted once)
 };
 
 constexpr int kReduceThreads = 1024;  // virtual lanes of the reduction tree
 constexpr int kReduceScratchBytes =
-    2 * kReduceThreads * (int)sizeof(double) + 6 * 32 * (int)sizeof(int);
+    2 * kReduceThreads * (int)sizeof(double) + 7 * 32 * (int)sizeof(int);
 
 // Deterministic reduction of the per-block contributions by one CTA: the
 // blocks are split into kReduceThreads contiguous chunks (virtual lanes), each
@@ -33,12 +33,12 @@ __device__ __forceinline__ void reduce_blocks(const double *v, const unsigned *s
 {
     double *s_s = reinterpret_cast<double *>(scratch);
     double *s_c = s_s + kReduceThreads;
-    int *s_cnt = reinterpret_cast<int *>(s_c + kReduceThreads);  // [5][32]
-    unsigned *s_or = reinterpret_cast<unsigned *>(s_cnt + 5 * 32);
+    int *s_cnt = reinterpret_cast<int *>(s_c + kReduceThreads);  // [6][32]
+    unsigned *s_or = reinterpret_cast<unsigned *>(s_cnt + 6 * 32);
     const int T = blockDim.x;
     const int t = threadIdx.x;
     const int chunk = (n + kReduceThreads - 1) / kReduceThreads;
-    int cf = 0, sf = 0, fb = 0, nf = 0, nb = 0;
+    int cf = 0, sf = 0, fb = 0, nf = 0, nb = 0, fl = 0;
     unsigned fo = 0;
     for (int lane = t; lane < kReduceThreads; lane += T) {
         const int b0 = lane * chunk, b1 = min(n, b0 + chunk);
@@ -57,6 +57,7 @@ __device__ __forceinline__ void reduce_blocks(const double *v, const unsigned *s
             sf += (f & BV_ST_SCHUR_FAIL) ? 1 : 0;
             fb += (f & BV_ST_FP32_FALLBACK) ? 1 : 0;
             nf += (f & BV_ST_NONFINITE) ? 1 : 0;
+            fl += (f & (BV_ST_COND_FAIL | BV_ST_SCHUR_FAIL)) ? 1 : 0;
             ++nb;
         }
         s_s[lane] = s;
@@ -70,6 +71,7 @@ __device__ __forceinline__ void reduce_blocks(const double *v, const unsigned *s
         fb += __shfl_xor_sync(0xffffffffu, fb, o);
         nf += __shfl_xor_sync(0xffffffffu, nf, o);
         nb += __shfl_xor_sync(0xffffffffu, nb, o);
+        fl += __shfl_xor_sync(0xffffffffu, fl, o);
         fo |= __shfl_xor_sync(0xffffffffu, fo, o);
     }
     if ((t & 31) == 0) {
@@ -78,6 +80,7 @@ __device__ __forceinline__ void reduce_blocks(const double *v, const unsigned *s
         s_cnt[2 * 32 + (t >> 5)] = fb;
         s_cnt[3 * 32 + (t >> 5)] = nf;
         s_cnt[4 * 32 + (t >> 5)] = nb;
+        s_cnt[5 * 32 + (t >> 5)] = fl;
         s_or[t >> 5] = fo;
     }
     __syncthreads();
@@ -98,10 +101,10 @@ __device__ __forceinline__ void reduce_blocks(const double *v, const unsigned *s
     if (t == 0) {
         EvalResult r;
         r.llk = s_s[0] + s_c[0];
-        int c5[5] = {0, 0, 0, 0, 0};
+        int c5[6] = {0, 0, 0, 0, 0, 0};
         unsigned o = 0;
         for (int w = 0; w < T / 32; ++w) {
-            for (int q = 0; q < 5; ++q) c5[q] += s_cnt[q * 32 + w];
+            for (int q = 0; q < 6; ++q) c5[q] += s_cnt[q * 32 + w];
             o |= s_or[w];
         }
         r.cond_fail = c5[0];
@@ -110,7 +113,7 @@ __device__ __forceinline__ void reduce_blocks(const double *v, const unsigned *s
         r.nonfinite = c5[3];
         r.blocks = c5[4];
         r.flags_or = o;
-        r.pad = 0;
+        r.failed = c5[5];
         *out = r;
     }
     __syncthreads();

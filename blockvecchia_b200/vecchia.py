@@ -215,6 +215,12 @@ class LlhData:
         check(lib().bv_block_llk(self._h, dp(out), len(out)))
         return out
 
+    def block_status(self) -> np.ndarray:
+        """Per-block BV_ST_* bits of the last evaluation."""
+        out = np.zeros(self.layout.bc, dtype=np.uint32)
+        check(lib().bv_block_status(self._h, out.ctypes.data_as(C.POINTER(C.c_uint)), len(out)))
+        return out
+
     def status(self) -> dict:
         s = _lib.BvStatus()
         check(lib().bv_get_status(self._h, C.byref(s)))

@@ -102,6 +102,9 @@ typedef struct {
     double llk;          /* last log-likelihood (before the failure policy)  */
     double device_ms;    /* device time of the last evaluation               */
     double kernel_ms;    /* of which the fused per-block kernel(s)            */
+    int failed;          /* blocks with a failed pivot in either factor
+                            (cond_fail and schur_fail may count one block
+                            twice; this counts it once)                      */
 } bv_status;
 
 typedef struct bv_handle bv_handle;
@@ -132,6 +135,11 @@ int bv_llh_eval(bv_handle *h, const double *theta, double *llk);
 /* Per-block contributions of the last evaluation, copied to host [bc]. */
 int bv_block_llk(bv_handle *h, double *out, int count);
 
+/* Per-block BV_ST_* bits of the last evaluation, copied to host [bc] (the
+ * reference keeps MAGMA's per-block info arrays but never reads them,
+ * include/llh_Xvecchia_batch.h:295-299,449-453). */
+int bv_block_status(bv_handle *h, unsigned *out, int count);
+
 int bv_get_status(bv_handle *h, bv_status *st);
 
 /* The CUDA stream (cudaStream_t) the handle launches on, for callers that
@@ -160,18 +168,23 @@ int bv_llh_host(bv_handle *h, const double *x, const double *y,
  * obs [n]), the block offsets (batchNumAccum [bc+1]) and the conditioning
  * indices (knn_idx [bc*cs]; block 0 unconditioned), the host parameters
  * theta = {sigma2, range, nu}, and a device pointer llk_out that receives the
- * log-likelihood.  The library's working memory for this call is a fixed
- * 2 MB device array inside the library (every device that loads the library
- * holds it until exit): at most BV_NOALLOC_MAX_BLOCKS blocks, and every
- * block must fit in one SM's shared memory (cs + bs <= about 236), else
- * BV_E_TOOLARGE.  Invalid offsets or indices give BV_E_INVALID.  The first
- * call on a device looks up that array's device address, so make that first
- * call before any stream capture.  Every call shares the array: calls that
- * overlap on the GPU race, so serialise them (one stream, or synchronise).
- * Runs on `stream` (a cudaStream_t of the current device; NULL = the default
- * stream) and returns after the evaluation has finished.  Allocates nothing:
- * no cudaMalloc, cudaFree or allocating library call.  *status_flags (may be
- * NULL) receives the OR of the blocks' BV_ST_* bits. */
+ * log-likelihood, or -HUGE_VAL when a block meets a non-positive pivot or the
+ * sum is not finite (the BV_FAIL_NEGINF policy; *status_flags then says
+ * why).  The library's working memory for this call is a fixed 2 MB device
+ * array inside the library (every device that loads the library holds it
+ * until exit): at most BV_NOALLOC_MAX_BLOCKS blocks, and every block must
+ * fit in one SM's shared memory (cs + bs <= about 236), else BV_E_TOOLARGE.
+ * Invalid offsets or indices, or a block 0 with fewer than cs points while
+ * other blocks condition on it, give BV_E_INVALID.  The first call on a
+ * device looks up that array's device address (cached per device ordinal;
+ * a cudaDeviceReset invalidates it, so do not call this entry point after
+ * one), so make that first call before any stream capture.  Every call
+ * shares the array: calls that overlap on the GPU race, so serialise them
+ * (one stream, or synchronise).  Runs on `stream` (a cudaStream_t of the
+ * current device; NULL = the default stream) and waits for its own work
+ * before it returns: it reads back the layout check and the status flags.
+ * Allocates nothing: no cudaMalloc, cudaFree or allocating library call.
+ * *status_flags (may be NULL) receives the OR of the blocks' BV_ST_* bits. */
 #define BV_NOALLOC_MAX_BLOCKS 131072
 int bv_llh_noalloc(const double *x, const double *y, const double *obs,
                    const int *batchNumAccum, const int *knn_idx, int n, int bc,
