@@ -306,6 +306,21 @@ void bvo_knn_all(const double *x, const double *y, int bc, int cs,
                       knn_idx + (size_t)i * cs);
 }
 
+void bvo_knn_all_fast(const double *x, const double *y, int bc, int cs,
+                      const int *batchNumAccum, const double *cx,
+                      const double *cy, int *knn_idx, int threads)
+{
+    for (int t = 0; t < cs; ++t) knn_idx[t] = t;
+#ifdef _OPENMP
+    int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+#endif
+    for (int i = 1; i < bc; ++i)
+        bvo_knn_block_fast(x, y, batchNumAccum[i], cx[i], cy[i], cs,
+                           knn_idx + (size_t)i * cs);
+    (void)threads;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Dense FP64 kernels (plain loops), column-major                           */
 /* ------------------------------------------------------------------------ */
@@ -410,6 +425,9 @@ static void bvo_block(const bvo_problem *p, const double *theta, int i,
 
     /* :117-150  Sigma11 */
     bvo_matern(S11, bs, bs, xb, yb, xb, yb, theta, p->dist_scale);
+    /* The nugget extension (not in the reference): tau^2 on the diagonal. */
+    if (p->nugget != 0.0)
+        for (int j = 0; j < bs; ++j) S11[j + (size_t)j * bs] += p->nugget;
     for (int j = 0; j < bs; ++j) z[j] = p->obs[off + j];
     if (cs > 0) {
         /* locations_con / h_obs_conditioning gathered at the kNN indices
@@ -422,6 +440,8 @@ static void bvo_block(const bvo_problem *p, const double *theta, int i,
         }
         /* :196-207  Sigma22 (cs x cs, full), Sigma21 (cs x bs) */
         bvo_matern(S22, cs, cs, xc, yc, xc, yc, theta, p->dist_scale);
+        if (p->nugget != 0.0)
+            for (int j = 0; j < cs; ++j) S22[j + (size_t)j * cs] += p->nugget;
         bvo_matern(S21, cs, bs, xc, yc, xb, yb, theta, p->dist_scale);
         /* :295-299 potrf, :320-337 trsm x2, :352-378 gemm x2 */
         if (la) {

@@ -65,6 +65,12 @@ void bvo_knn_all(const double *x, const double *y, int bc, int cs,
                  const int *batchNumAccum, const double *cx, const double *cy,
                  int *knn_idx);
 
+/* bvo_knn_all with bvo_knn_block_fast per block (same result), OpenMP over
+ * blocks with `threads` workers (<= 0: the OpenMP default). */
+void bvo_knn_all_fast(const double *x, const double *y, int bc, int cs,
+                      const int *batchNumAccum, const double *cx,
+                      const double *cy, int *knn_idx, int threads);
+
 /* The problem one log-likelihood evaluation reads (the llh_data fields of
  * include/vecchia_helper_data.h:69-146 that the FP64 Matern path uses). */
 typedef struct {
@@ -77,6 +83,8 @@ typedef struct {
     const double *obs;        /* [n] block-ordered observations (h_obs_new) */
     const int *knn_idx;       /* [bc*cs] conditioning indices into x/y/obs  */
     double dist_scale;        /* --dist_scale, 1.0 by default               */
+    double nugget;            /* tau^2 on the diagonal of Sigma11 and Sigma22;
+                                 0 = the reference's likelihood (no nugget)  */
 } bvo_problem;
 
 /* Per-block result of the restated likelihood. */

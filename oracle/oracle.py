@@ -26,10 +26,16 @@ def _ip(a):
     return a.ctypes.data_as(_I)
 
 
+def ref_root() -> str:
+    """The reference tree: $REF_ROOT, else a checkout named `reference` beside
+    this repository."""
+    return os.environ.get("REF_ROOT") or os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
+
+
 def build(ref: bool = False) -> None:
     """Compile the oracle (and oracle/_ref when the reference tree exists)."""
-    target = "ref" if (ref and os.path.isdir(os.environ.get("REF_ROOT", "/root/reference"))) else "all"
-    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+    target = "ref" if (ref and os.path.isdir(ref_root())) else "all"
+    subprocess.run(["make", "-s", "-C", HERE, target, f"REF_ROOT={ref_root()}"], check=True)
 
 
 class BlockResult(C.Structure):
@@ -41,7 +47,7 @@ class Problem(C.Structure):
     _fields_ = [("n", C.c_int), ("bc", C.c_int), ("cs", C.c_int),
                 ("batchNum", _I), ("batchNumAccum", _I),
                 ("x", _D), ("y", _D), ("obs", _D), ("knn_idx", _I),
-                ("dist_scale", C.c_double)]
+                ("dist_scale", C.c_double), ("nugget", C.c_double)]
 
 
 _lib = None
@@ -61,6 +67,7 @@ def lib():
         L.bvo_knn_block.restype = C.c_int
         L.bvo_knn_block.argtypes = [_D, _D, C.c_int, C.c_double, C.c_double, C.c_int, _I]
         L.bvo_knn_all.argtypes = [_D, _D, C.c_int, C.c_int, _I, _D, _D, _I]
+        L.bvo_knn_all_fast.argtypes = [_D, _D, C.c_int, C.c_int, _I, _D, _D, _I, C.c_int]
         L.bvo_knn_block_fast.restype = C.c_int
         L.bvo_knn_block_fast.argtypes = [_D, _D, C.c_int, C.c_double, C.c_double, C.c_int, _I]
         L.bvo_llh.restype = C.c_double
@@ -140,10 +147,24 @@ def knn_all(x, y, cs, batchNumAccum, cx, cy):
     return out
 
 
+def knn_all_fast(x, y, cs, batchNumAccum, cx, cy, threads=0):
+    """Every block's conditioning set by the fast restatement (quickselect +
+    selection-sort replay; the same indices as knn_all), OpenMP over blocks."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    acc = np.ascontiguousarray(batchNumAccum, dtype=np.int32)
+    cx = np.ascontiguousarray(cx, dtype=np.float64)
+    cy = np.ascontiguousarray(cy, dtype=np.float64)
+    bc = len(acc) - 1
+    out = np.zeros(bc * cs, dtype=np.int32)
+    lib().bvo_knn_all_fast(_dp(x), _dp(y), bc, cs, _ip(acc), _dp(cx), _dp(cy), _ip(out), int(threads))
+    return out
+
+
 class OracleProblem:
     """Holds numpy arrays alive behind a bvo_problem."""
 
-    def __init__(self, batchNum, batchNumAccum, x, y, obs, knn_idx, cs, dist_scale=1.0):
+    def __init__(self, batchNum, batchNumAccum, x, y, obs, knn_idx, cs, dist_scale=1.0, nugget=0.0):
         self.batchNum = np.ascontiguousarray(batchNum, dtype=np.int32)
         self.batchNumAccum = np.ascontiguousarray(batchNumAccum, dtype=np.int32)
         self.x = np.ascontiguousarray(x, dtype=np.float64)
@@ -153,7 +174,8 @@ class OracleProblem:
         self.cs = int(cs)
         self.bc = len(self.batchNum)
         self.p = Problem(len(self.x), self.bc, self.cs, _ip(self.batchNum), _ip(self.batchNumAccum),
-                         _dp(self.x), _dp(self.y), _dp(self.obs), _ip(self.knn_idx), float(dist_scale))
+                         _dp(self.x), _dp(self.y), _dp(self.obs), _ip(self.knn_idx), float(dist_scale),
+                         float(nugget))
 
 
 def llh(prob: OracleProblem, theta, threads: int = 0, per_block: bool = False):
@@ -161,9 +183,15 @@ def llh(prob: OracleProblem, theta, threads: int = 0, per_block: bool = False):
     res = (BlockResult * prob.bc)()
     v = lib().bvo_llh(C.byref(prob.p), _dp(th), res, int(threads))
     if per_block:
-        arr = np.array([(r.logdet, r.norm2, r.info22, r.info11) for r in res])
-        return v, arr
+        return v, _per_block_array(res)
     return v
+
+
+def _per_block_array(res):
+    arr = np.frombuffer(res, dtype=np.dtype([("logdet", "<f8"), ("norm2", "<f8"),
+                                             ("info22", "<i4"), ("info11", "<i4")]))
+    return np.stack([arr["logdet"], arr["norm2"], arr["info22"].astype(np.float64),
+                     arr["info11"].astype(np.float64)], 1)
 
 
 _blas = None
@@ -199,15 +227,29 @@ def _openblas():
     return _blas
 
 
-def llh_blas(prob: OracleProblem, theta, threads: int = 0, block_begin: int = 0, block_end: int = -1):
-    """Same evaluation with OpenBLAS dense LA (one BLAS thread per OpenMP worker)."""
+def llh_blas(prob: OracleProblem, theta, threads: int = 0, block_begin: int = 0, block_end: int = -1,
+             per_block: bool = False):
+    """Same evaluation with OpenBLAS dense LA (one BLAS thread per OpenMP
+    worker).  per_block=True also returns a (bc, 4) array of (logdet, norm2,
+    info22, info11); rows outside [block_begin, block_end) are zero."""
     B, names, setth = _openblas()
     if setth is not None:
         setth(1)
     th = np.ascontiguousarray(theta, dtype=np.float64)
-    return lib().bvo_llh_blas(C.byref(prob.p), _dp(th), None, int(threads),
-                              names["potrf"], names["trsm"], names["gemm"],
-                              int(block_begin), int(block_end))
+    res = (BlockResult * prob.bc)() if per_block else None
+    v = lib().bvo_llh_blas(C.byref(prob.p), _dp(th), res, int(threads),
+                           names["potrf"], names["trsm"], names["gemm"],
+                           int(block_begin), int(block_end))
+    if per_block:
+        return v, _per_block_array(res)
+    return v
+
+
+def block_llk(batchNum, per_block):
+    """Per-block contributions -(norm2^2 + logdet + bs log 2 PI) / 2 from the
+    per-block arrays of llh / llh_blas (include/llh_Xvecchia_batch.h:482)."""
+    bn = np.asarray(batchNum, dtype=np.float64)
+    return -(per_block[:, 1] ** 2 + per_block[:, 0] + bn * np.log(2 * 3.141592653589793)) * 0.5
 
 
 # ------------------------------------------------------------- reference API

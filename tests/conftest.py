@@ -46,7 +46,7 @@ def oracle():
 def ref(oracle):
     """The reference's own host code (oracle/_ref), when it can be built."""
     if not oracle.ref_available():
-        if os.path.isdir(os.environ.get("REF_ROOT", "/root/reference")):
+        if os.path.isdir(oracle.ref_root()):
             oracle.build(ref=True)
     if not oracle.ref_available():
         pytest.skip("reference sources not present and oracle/_ref not built")

@@ -4,7 +4,7 @@ oracle/Makefile) and the CPU oracle.
 
     python tests/golden/make_golden.py
 
-Needs the reference tree (REF_ROOT, default /root/reference) to build
+Needs the reference tree (REF_ROOT, else a checkout named `reference` beside this repository) to build
 oracle/_ref; the fixtures it writes are small .npz files that the tests read
 on any machine.
 """

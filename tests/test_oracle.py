@@ -93,6 +93,47 @@ def test_llh_exact_two_blocks(oracle):
         assert abs(v - exact) <= 1e-10 * abs(exact), (th, v, exact)
 
 
+def test_llh_exact_with_nugget(oracle):
+    """The nugget extension: with tau^2 on the diagonal of Sigma11 and
+    Sigma22, block 1 conditioning on all of block 0 gives the exact density
+    of N(0, Sigma + tau^2 I) -- including two points at the same location,
+    which share covariance sigma2 but get the nugget once each."""
+    scipy_stats = pytest.importorskip("scipy.stats")
+    rng = np.random.default_rng(4)
+    cs, bs1 = 30, 11
+    n = cs + bs1
+    x, y = rng.random(n), rng.random(n)
+    x[cs + 2], y[cs + 2] = x[5], y[5]  # a repeated location across the blocks
+    z = rng.standard_normal(n)
+    bn = np.array([cs, bs1], dtype=np.int32)
+    acc = np.array([0, cs, n], dtype=np.int32)
+    knn = np.concatenate([np.arange(cs), rng.permutation(cs)]).astype(np.int32)
+    for tau2 in (0.01, 0.3):
+        P = oracle.OracleProblem(bn, acc, x, y, z, knn, cs, nugget=tau2)
+        for th in [(1.5, 0.3, 0.5), (1.0, 0.25, 0.8), (1.2, 0.15, 2.5)]:
+            Sigma = oracle.matern(x, y, x, y, th) + tau2 * np.eye(n)
+            exact = scipy_stats.multivariate_normal(mean=np.zeros(n), cov=Sigma).logpdf(z)
+            v = oracle.llh(P, th)
+            assert abs(v - exact) <= 1e-10 * abs(exact), (tau2, th, v, exact)
+            assert abs(oracle.llh_blas(P, th) - exact) <= 1e-10 * abs(exact)
+
+
+def test_knn_all_fast_matches_restatement(oracle):
+    """The fast all-blocks conditioning sets equal the selection-sort
+    restatement's (the one pinned against the reference's own code)."""
+    rng = np.random.default_rng(9)
+    n, bc, cs = 4000, 120, 50
+    x, y = rng.random(n), rng.random(n)
+    x[100:140] = x[10]  # exact ties at the selection threshold
+    y[100:140] = y[10]
+    acc = np.linspace(0, n, bc + 1).astype(np.int32)
+    acc[1] = max(acc[1], cs)
+    cx, cy = rng.random(bc), rng.random(bc)
+    a = oracle.knn_all_fast(x, y, cs, acc, cx, cy, threads=4)
+    b = oracle.knn_all(x, y, cs, acc, cx, cy)
+    assert np.array_equal(a, b)
+
+
 def test_llh_matches_blas_variant(oracle, golden_layout):
     """The OpenBLAS-backed CPU baseline computes the same quantity."""
     g = golden_layout
