@@ -63,6 +63,7 @@ EXPORTS = {
     "bv_server_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "bv_server_destroy": (None, [C.c_void_p]),
     "bv_server_open_job": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, _I]),
+    "bv_server_open_job_ex": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _I]),
     "bv_server_job_admitted": (C.c_int, [C.c_void_p, C.c_int, _I]),
     "bv_server_close_job": (C.c_int, [C.c_void_p, C.c_int]),
     "bv_server_submit": (C.c_int, [C.c_void_p, C.c_int, _D, C.POINTER(C.c_longlong)]),
@@ -83,7 +84,8 @@ class BvOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("kernel", C.c_int), ("dist_scale", C.c_double),
                 ("device", C.c_int), ("on_failure", C.c_int), ("print_iter", C.c_int),
                 ("use_graph", C.c_int), ("schedule", C.c_int), ("mixed_tol", C.c_double),
-                ("shard_count", C.c_int), ("shard_index", C.c_int), ("large_blocks", C.c_int)]
+                ("shard_count", C.c_int), ("shard_index", C.c_int), ("large_blocks", C.c_int),
+                ("nugget", C.c_int)]
 
 
 class BvStatus(C.Structure):
@@ -91,6 +93,10 @@ class BvStatus(C.Structure):
                 ("fp32_fallback", C.c_int), ("nonfinite", C.c_int), ("flags_or", C.c_uint),
                 ("llk", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double),
                 ("failed", C.c_int)]
+
+
+class BvJobOpts(C.Structure):
+    _fields_ = [("dist_scale", C.c_double), ("nugget", C.c_int)]
 
 
 class BvServerOpts(C.Structure):

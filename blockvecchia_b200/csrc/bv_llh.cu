@@ -170,6 +170,7 @@ extern "C" void bv_default_opts(bv_opts *o)
     o->shard_count = 1;
     o->shard_index = 0;
     o->large_blocks = BV_LARGE_AUTO;
+    o->nugget = 0;
 }
 
 // Cost rank (largest first, ties by index) shared by the schedule and the
@@ -596,7 +597,13 @@ static int fill_params(bv_handle *h, const double *theta)
         set_error("bv_llh: invalid theta (%g, %g, %g)", sigma2, range, nu);
         return BV_E_INVALID;
     }
+    const double tau2 = h->opts.nugget ? theta[3] : 0.0;
+    if (!(tau2 >= 0) || !std::isfinite(tau2)) {
+        set_error("bv_llh: invalid nugget %g", tau2);
+        return BV_E_INVALID;
+    }
     MaternParams &p = *h->h_mp;
+    p.nugget = tau2;
     p.sigma2 = sigma2;
     p.range = range;
     p.nu = nu;
@@ -654,7 +661,7 @@ static int eval_locked(bv_handle *h, const double *theta, double *llk)
 static void print_iteration(bv_handle *h, const double *theta, double llk)
 {
     // include/llh_Xvecchia_batch.h:500-511
-    if (h->opts.kernel == 3)
+    if (h->opts.kernel == 3 || h->opts.nugget)
         printf("%dth Model Parameters (Variance, range, smoothness, nugget): (%1.8lf, %1.8lf, "
                "%1.8lf, %1.8lf) -> Loglik: %.18lf \n",
                h->iterations, theta[0], theta[1], theta[2], theta[3], llk);
@@ -683,8 +690,8 @@ extern "C" double bv_llh(unsigned n, const double *theta, double *grad, void *f_
 {
     (void)grad;
     bv_handle *h = static_cast<bv_handle *>(f_data);
-    if (!h || !theta || n < 3) {
-        set_error("bv_llh: need a handle and at least 3 parameters");
+    if (!h || !theta || n < (h && h->opts.nugget ? 4u : 3u)) {
+        set_error("bv_llh: need a handle and at least 3 parameters (4 with the nugget)");
         return -HUGE_VAL;
     }
     double v = -HUGE_VAL;

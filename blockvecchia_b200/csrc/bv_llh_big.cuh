@@ -121,13 +121,16 @@ __device__ __forceinline__ void update_warps_sync()
     asm volatile("bar.sync 1, %0;" ::"n"(kThreads - 32) : "memory");
 }
 
-// Entry (i, j) of the augmented system: covariance for i < M, the
-// observation of point j on row M.  Same argument order as the
-// shared-memory path's generation, so the entries are identical.
+// Entry (i, j) of the augmented system: covariance for i < M (plus the
+// nugget on the diagonal), the observation of point j on row M.  Same
+// argument order and the same nugget addition as the shared-memory path's
+// generation, so the entries are identical.
 __device__ __forceinline__ double big_entry(const double *X, const double *Y, const double *Z, int M,
                                             int i, int j, const MaternParams &mp)
 {
-    return (i < M) ? matern(X[i], Y[i], X[j], Y[j], mp) : Z[j];
+    if (i >= M) return Z[j];
+    const double c = matern(X[i], Y[i], X[j], Y[j], mp);
+    return (i == j && mp.nugget != 0.0) ? c + mp.nugget : c;
 }
 
 // Rank-16 update of a panel held in shared memory, dst rows [d0, d1) (panel

@@ -1036,6 +1036,12 @@ __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternPara
     __syncthreads();
     generate(A, X, Y, M, mp);
     __syncthreads();
+    if (mp.nugget != 0.0) {
+        // Nugget: tau^2 on the diagonal of Sigma22 and Sigma11 (a point with
+        // itself), not on other pairs at distance 0.
+        for (int t = tid; t < M; t += kThreads) A[poff(t, Mp) + t] += mp.nugget;
+        __syncthreads();
+    }
 
     // Cholesky of the first M columns; row M rides along as the
     // forward-substitution right-hand side.

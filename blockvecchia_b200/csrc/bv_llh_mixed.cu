@@ -302,8 +302,8 @@ __device__ void residual(const double *X, const double *Y, const double *S21, co
         for (int j0 = 0; j0 < cs; j0 += 64) {
             const int ja = j0 + lane, jb = j0 + 32 + lane;
             double va = 0.0, vb = 0.0;
-            if (ja < cs) va = matern(xi, yi, X[ja], Y[ja], mp);
-            if (jb < cs) vb = matern(xi, yi, X[jb], Y[jb], mp);
+            if (ja < cs) va = matern(xi, yi, X[ja], Y[ja], mp) + (ja == i ? mp.nugget : 0.0);
+            if (jb < cs) vb = matern(xi, yi, X[jb], Y[jb], mp) + (jb == i ? mp.nugget : 0.0);
             if (ja < cs) K[ja] = va;
             if (jb < cs) K[jb] = vb;
         }
@@ -340,6 +340,7 @@ __device__ bool mixed_block(const MixedArgs &a, const MaternParams &mp, int b, c
     float *P = reinterpret_cast<float *>(sm + l.o_P);
     const double inv_s2 = 1.0 / mp.sigma2;
     const float inv_range_f = (float)mp.inv_range, inv_ds_f = (float)mp.inv_ds;
+    const float nug_unit = (float)(mp.nugget * inv_s2);
 
     const int off = a.acc[b];
     const int *kidx = a.knn + (size_t)b * cs;
@@ -362,7 +363,9 @@ __device__ bool mixed_block(const MixedArgs &a, const MaternParams &mp, int b, c
         for (int r = lane; r < n1 + n2; r += 32) {
             const int j = (r < n1) ? j1 : j2;
             const int i = j + ((r < n1) ? r : r - n1);
-            T[tro(j, Mt) + i - j] = cov_unit_f32(X[i], Y[i], X[j], Y[j], mp, inv_range_f, inv_ds_f, inv_s2);
+            float t = cov_unit_f32(X[i], Y[i], X[j], Y[j], mp, inv_range_f, inv_ds_f, inv_s2);
+            if (i == j) t += nug_unit;  // the nugget on Sigma22's diagonal
+            T[tro(j, Mt) + i - j] = t;
         }
     }
     // FP64 Sigma21 (row j: conditioning point j, column c: block point c).
@@ -423,7 +426,7 @@ __device__ bool mixed_block(const MixedArgs &a, const MaternParams &mp, int b, c
         if (r < bs && c > r) continue;
         double s;
         if (r < bs) {
-            s = matern(X[cs + r], Y[cs + r], X[cs + c], Y[cs + c], mp);
+            s = matern(X[cs + r], Y[cs + r], X[cs + c], Y[cs + c], mp) + (r == c ? mp.nugget : 0.0);
             for (int j = 0; j < cs; ++j) s = fma(-S21[j * bs + r], X1[j * bs + c], s);
         } else {
             s = zb[c];

@@ -35,6 +35,8 @@ struct MaternParams {
     double inv_ds;      // RN(1 / dist_scale), host-computed
     int nu_kind;        // NuKind
     int scale_is_one;   // dist_scale == 1.0: the second division is exact and skipped
+    double nugget;      // tau^2 added to the diagonal of Sigma11 and Sigma22 (0: none,
+                        // the reference's likelihood, which never reads theta[3])
     // General nu (matern_prepare): nu = mu + nn, |mu| <= 1/2.
     int nn;
     double mu;

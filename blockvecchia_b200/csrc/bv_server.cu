@@ -98,6 +98,7 @@ struct Job {
     int id = 0;
     int n = 0, bc = 0, cs = 0, max_m = 1;
     double dist_scale = 1.0;
+    bool nugget = false;  // theta[3] = tau^2 on the covariance diagonals
     std::vector<int> acc, knn;
     std::vector<double> x, y, obs;
     std::vector<int> sorted;   // blocks by M descending (ties by index)
@@ -114,7 +115,7 @@ struct Job {
 struct Req {
     long long id = 0;
     int job = 0;
-    double theta[3] = {0, 0, 0};
+    double theta[4] = {0, 0, 0, 0};  // theta[3]: the nugget, 0 unless the job has one
     Clock::time_point submitted;
     bool done = false;
     int rc = BV_OK;
@@ -272,6 +273,7 @@ void fill_params(MaternParams &p, const double *theta, double dist_scale)
     p.inv_ds = 1.0 / dist_scale;
     p.nu_kind = (nu == 0.5) ? kNuHalf : (nu == 1.5) ? kNuThreeHalves : (nu == 2.5) ? kNuFiveHalves
                                                                                   : kNuGeneral;
+    p.nugget = theta[3];
     matern_prepare(p);
 }
 
@@ -681,7 +683,16 @@ extern "C" void bv_server_destroy(bv_server *S)
 
 extern "C" int bv_server_open_job(bv_server *S, const bv_layout *L, double dist_scale, int *job_id)
 {
-    if (!S || !job_id) {
+    bv_job_opts o;
+    o.dist_scale = dist_scale;
+    o.nugget = 0;
+    return bv_server_open_job_ex(S, L, &o, job_id);
+}
+
+extern "C" int bv_server_open_job_ex(bv_server *S, const bv_layout *L, const bv_job_opts *jo,
+                                     int *job_id)
+{
+    if (!S || !job_id || !jo) {
         set_error("bv_server_open_job: null argument");
         return BV_E_INVALID;
     }
@@ -695,7 +706,8 @@ extern "C" int bv_server_open_job(bv_server *S, const bv_layout *L, double dist_
     j->n = L->n;
     j->bc = L->bc;
     j->cs = L->cs;
-    j->dist_scale = dist_scale > 0 ? dist_scale : 1.0;
+    j->dist_scale = jo->dist_scale > 0 ? jo->dist_scale : 1.0;
+    j->nugget = jo->nugget != 0;
     j->acc.assign(L->batchNumAccum, L->batchNumAccum + L->bc + 1);
     std::vector<int> m(L->bc);
     for (int b = 0; b < L->bc; ++b) {
@@ -775,10 +787,15 @@ extern "C" int bv_server_submit(bv_server *S, int job_id, const double *theta, l
         set_error("bv_server_submit: no open job %d", job_id);
         return BV_E_INVALID;
     }
+    const bool nug = it->second->nugget;
+    if (nug && (!(theta[3] >= 0) || !std::isfinite(theta[3]))) {
+        set_error("bv_server_submit: invalid nugget %g", theta[3]);
+        return BV_E_INVALID;
+    }
     Req r;
     r.id = S->next_req++;
     r.job = job_id;
-    std::memcpy(r.theta, theta, sizeof(r.theta));
+    std::memcpy(r.theta, theta, (nug ? 4 : 3) * sizeof(double));
     r.submitted = Clock::now();
     it->second->inflight++;
     S->reqs[r.id] = r;

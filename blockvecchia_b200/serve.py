@@ -54,8 +54,9 @@ class Server:
     def __exit__(self, *exc):
         self.close()
 
-    def open_job(self, layout: Layout, dist_scale: float = 1.0) -> int:
-        """Queue a job for admission; its conditioning indices must be set."""
+    def open_job(self, layout: Layout, dist_scale: float = 1.0, nugget: bool = False) -> int:
+        """Queue a job for admission; its conditioning indices must be set.
+        nugget=True: the job's thetas carry tau^2 as a fourth value."""
         L = layout.normalized()
         if L.cs > 0 and L.knn_idx is None:
             raise ValueError("open_job: the layout needs knn_idx (blockvecchia_b200.knn computes it)")
@@ -64,7 +65,8 @@ class Server:
                            dp(L.y), dp(L.obs), ip(L.knn_idx) if L.knn_idx is not None
                            else C.POINTER(C.c_int)(), null_d, null_d)
         jid = C.c_int()
-        check(lib().bv_server_open_job(self._s, C.byref(bl), float(dist_scale), C.byref(jid)))
+        jo = _lib.BvJobOpts(float(dist_scale), int(bool(nugget)))
+        check(lib().bv_server_open_job_ex(self._s, C.byref(bl), C.byref(jo), C.byref(jid)))
         return jid.value
 
     def admitted(self, job: int) -> bool:
@@ -76,7 +78,9 @@ class Server:
         check(lib().bv_server_close_job(self._s, int(job)))
 
     def submit(self, job: int, theta) -> int:
-        t = np.ascontiguousarray(np.asarray(theta, dtype=np.float64)[:3])
+        t = np.zeros(4)
+        th = np.asarray(theta, dtype=np.float64)[:4]
+        t[:len(th)] = th
         rid = C.c_longlong()
         check(lib().bv_server_submit(self._s, int(job), dp(t), C.byref(rid)))
         return rid.value

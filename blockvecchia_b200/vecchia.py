@@ -142,7 +142,7 @@ class LlhData:
                  dist_scale: float = 1.0, device: int = 0, on_failure: str = "neginf",
                  print_iter: bool = False, use_graph: bool = True, schedule: str = "persistent",
                  mixed_tol: float = 1e-8, shard_count: int = 1, shard_index: int = 0,
-                 large_blocks: str = "auto"):
+                 large_blocks: str = "auto", nugget: bool = False):
         L = layout.normalized()
         self.layout = L
         o = _lib.BvOpts()
@@ -159,6 +159,7 @@ class LlhData:
         o.shard_count = int(shard_count)
         o.shard_index = int(shard_index)
         o.large_blocks = _LARGE[large_blocks]
+        o.nugget = int(bool(nugget))
         null_i = C.POINTER(C.c_int)()
         null_d = C.POINTER(C.c_double)()
         self._l = _lib.BvLayout(L.n, L.bc, L.cs, ip(L.batchNum), ip(L.batchNumAccum), dp(L.x),
@@ -169,7 +170,7 @@ class LlhData:
         self._h = C.c_void_p()
         check(lib().bv_create(C.byref(self._l), C.byref(o), C.byref(self._h)))
         self.kernel = kernel
-        self.num_params = 3
+        self.num_params = 4 if nugget else 3
 
     def close(self):
         if self._h:
@@ -193,14 +194,17 @@ class LlhData:
         return self._h
 
     def __call__(self, theta) -> float:
-        th = np.ascontiguousarray(theta, dtype=np.float64)
+        """theta = (sigma2, range, nu), plus tau^2 when the handle has a nugget."""
+        th = np.zeros(max(4, len(theta)))
+        th[:len(theta)] = np.asarray(theta, dtype=np.float64)
         out = C.c_double(0.0)
         check(lib().bv_llh_eval(self._h, dp(th), C.byref(out)))
         return out.value
 
     def eval_host(self, obs, theta, x=None, y=None, knn_idx=None) -> float:
         """End-to-end evaluation from host buffers (copies in, evaluates)."""
-        th = np.ascontiguousarray(theta, dtype=np.float64)
+        th = np.zeros(max(4, len(theta)))
+        th[:len(theta)] = np.asarray(theta, dtype=np.float64)
         obs = np.ascontiguousarray(obs, dtype=np.float64)
         nd = C.POINTER(C.c_double)()
         ni = C.POINTER(C.c_int)()

@@ -90,6 +90,13 @@ typedef struct {
                           BV_LARGE_AUTO (default: the streamed path when more
                           than one wave of blocks needs it, else the slab),
                           BV_LARGE_STREAMED, BV_LARGE_SLAB                   */
+    int nugget;        /* 0 (default): theta = {sigma2, range, nu}; theta[3],
+                          if given, is not read -- the reference's likelihood
+                          never reads it (include/llh_Xvecchia_batch.h:126-144),
+                          even for its 4-parameter kernel 3.  1: theta[3] =
+                          tau^2 >= 0 is added to the diagonal of Sigma11 and
+                          Sigma22 (a point with itself), and bv_llh needs
+                          n >= 4 parameters.                                  */
 } bv_opts;
 
 typedef struct {
@@ -122,8 +129,9 @@ int bv_create(const bv_layout *layout, const bv_opts *opts, bv_handle **out);
 void bv_destroy(bv_handle *h);
 
 /* NLopt objective (replaces llh_Xvecchia_batch<double>,
- * include/llh_Xvecchia_batch.h:24): n = number of parameters (3 for Matern),
- * theta = {sigma2, range, nu}, grad ignored (derivative-free optimizer),
+ * include/llh_Xvecchia_batch.h:24): n = number of parameters (3 for Matern,
+ * 4 with bv_opts.nugget), theta = {sigma2, range, nu[, tau^2]}, grad ignored
+ * (derivative-free optimizer),
  * f_data = bv_handle*.  Returns the block-Vecchia log-likelihood; on a block
  * failure under BV_FAIL_NEGINF, or on an error, returns -HUGE_VAL and records
  * the reason in bv_get_status / bv_last_error. */
@@ -223,10 +231,19 @@ void bv_server_destroy(bv_server *s);
 /* Copies the layout (conditioning indices required); *job_id identifies it. */
 int bv_server_open_job(bv_server *s, const bv_layout *layout, double dist_scale,
                        int *job_id);
+/* The same with per-job options: nugget = 1 makes the job's requests carry
+ * theta = {sigma2, range, nu, tau^2} (bv_opts.nugget semantics). */
+typedef struct {
+    double dist_scale;
+    int nugget;
+} bv_job_opts;
+int bv_server_open_job_ex(bv_server *s, const bv_layout *layout,
+                          const bv_job_opts *opts, int *job_id);
 int bv_server_job_admitted(bv_server *s, int job_id, int *admitted);
 /* The job's memory is released once its in-flight requests complete. */
 int bv_server_close_job(bv_server *s, int job_id);
-/* Queue one evaluation at theta = {sigma2, range, nu}; returns at once. */
+/* Queue one evaluation at theta = {sigma2, range, nu} (plus tau^2 for a job
+ * opened with a nugget); returns at once. */
 int bv_server_submit(bv_server *s, int job_id, const double *theta,
                      long long *req_id);
 /* Wait for a request (timeout_ms < 0: no limit; BV_E_TIMEOUT otherwise). */

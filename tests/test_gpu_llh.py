@@ -281,3 +281,36 @@ def test_failure_policy_large_blocks(bvlib):
         a, b = D(th), D(th)
         st2 = D.status()
     assert np.isfinite(a) and a == b and st2["cond_fail"] + st2["schur_fail"] == nfail
+
+
+@pytest.mark.parametrize("n,bc,cs", [(3000, 200, 100), (3000, 200, 205), (1500, 100, 300)])
+def test_nugget(bvlib, oracle, n, bc, cs):
+    """tau^2 on the diagonal of Sigma11 and Sigma22 (the nugget option; the
+    reference's likelihood has none) against the oracle with the same
+    addition: panel-parallel, warp-specialised and streamed large-block
+    paths, closed-form and general nu; tau^2 = 0 gives the plain bits."""
+    L = _gen(bvlib, n, bc, cs)
+    with bvlib.LlhData(L) as D0, bvlib.LlhData(L, nugget=True) as D:
+        for th in THETAS[:4]:
+            assert D(tuple(th) + (0.0,)) == D0(th)
+            for tau2 in (0.01, 0.2):
+                P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, L.knn_idx,
+                                         L.cs, nugget=tau2)
+                ref = oracle.llh(P, th)
+                v = D(tuple(th) + (tau2,))
+                assert abs(v - ref) <= REL * abs(ref), (th, tau2, v, ref)
+
+
+def test_nugget_served_and_mixed(bvlib):
+    """A server job opened with a nugget gives the handle's bits; the mixed
+    path with a nugget stays within its 1e-8 accuracy bound."""
+    L = _gen(bvlib, 3000, 200, 100)
+    th = (1.0, 0.1, 0.5, 0.05)
+    with bvlib.LlhData(L, nugget=True) as D:
+        v = D(th)
+    with bvlib.Server() as srv:
+        j = srv.open_job(L, nugget=True)
+        assert srv.evaluate(j, th) == v
+    with bvlib.LlhData(L, nugget=True, precision="mixed") as M:
+        vm = M(th)
+    assert abs(vm - v) <= 1e-8 * abs(v)
