@@ -56,6 +56,50 @@ __global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel_t(LlhArgs a)
 static void (*const llh_fp64_kernel)(LlhArgs) = llh_fp64_kernel_t<false>;
 static void (*const llh_fp64_big_kernel)(LlhArgs) = llh_fp64_kernel_t<true>;
 
+// The streamed (left-looking, panels through L2) path run by small CTAs,
+// several per SM, so that the pivot chains of several blocks overlap on one
+// SM: NT threads per CTA, RC rows per streamed chunk, MINB CTAs per SM.
+template <int NT, int RC, int MINB>
+__global__ void __launch_bounds__(NT, MINB) llh_lean_kernel_t(LlhArgs a)
+{
+    extern __shared__ __align__(128) double smem[];
+    __shared__ LeanShared sh;
+    const MaternParams mp = *a.mp;
+    const int tid = threadIdx.x;
+    const int task_end = a.task_count ? min(a.task_end, *a.task_count) : a.task_end;
+    double *slab = a.gslab + (size_t)blockIdx.x * a.gslab_stride;
+    for (;;) {
+        if (tid == 0) {
+            sh.task = (int)atomicAdd(a.work_counter, 1u) + a.task_begin;
+            sh.status = 0u;
+        }
+        __syncthreads();
+        const int task = sh.task;
+        if (task >= task_end) break;
+        const int b = a.order[task];
+        if (a.acc[b + 1] == a.acc[b]) {  // empty block: contributes -(0 + 0 + 0) / 2
+            if (tid == 0) {
+                a.block_llk[b] = -0.0;
+                a.block_status[b] = a.status_or;
+            }
+        } else {
+            process_block_big<NT, RC>(a, mp, b, reinterpret_cast<unsigned char *>(smem), slab, sh);
+        }
+        __syncthreads();
+    }
+}
+
+struct LeanVariant {
+    void (*kernel)(LlhArgs);
+    int threads, rc;
+};
+static const LeanVariant kLeanVariants[] = {
+    {llh_lean_kernel_t<256, 64, 2>, 256, 64},
+    {llh_lean_kernel_t<128, 32, 3>, 128, 32},
+    {llh_lean_kernel_t<256, 32, 2>, 256, 32},
+    {llh_lean_kernel_t<128, 64, 2>, 128, 64},
+};
+
 static thread_local char g_err[1024] = "";
 
 void set_error(const char *fmt, ...)
@@ -108,6 +152,7 @@ struct bv_handle {
     void (*kernel)(LlhArgs) = nullptr;
     size_t smem_bytes = 0;
     int grid = 0;
+    int block_threads = kThreads;
     struct Launch {
         int begin, end, grid;
     };
@@ -298,10 +343,52 @@ bool bv::use_big_path(const int *batchNum, int bc, int cs, int small_m, int big_
     return n_big > sm_count;
 }
 
+// Multi-CTA streamed schedule: every block on the lean kernel.
+static int plan_lean(bv_handle *h, const cudaDeviceProp &prop, int variant)
+{
+    const LeanVariant &v = kLeanVariants[variant];
+    cudaFuncAttributes fa;
+    BV_CUDA_TRY(cudaFuncGetAttributes(&fa, v.kernel));
+    int optin = 0;
+    BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    const size_t avail = (size_t)optin - fa.sharedSizeBytes;
+    if ((size_t)big_layout(h->max_m, v.rc).total > avail) {
+        set_error("plan: blocks of M = %d exceed the streamed schedule's shared memory", h->max_m);
+        return BV_E_TOOLARGE;
+    }
+    h->kernel = v.kernel;
+    h->block_threads = v.threads;
+    h->smem_bytes = big_layout(h->max_m, v.rc).total;
+    h->use_big = true;
+    BV_CUDA_TRY(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)h->smem_bytes));
+    int occ = 0;
+    BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.kernel, v.threads, h->smem_bytes));
+    if (occ < 1) {
+        set_error("plan: streamed kernel cannot be resident (smem %zu B)", h->smem_bytes);
+        return BV_E_TOOLARGE;
+    }
+    h->grid = prop.multiProcessorCount * occ;
+    h->smem_max_m = 0;
+    h->big_max_m = h->max_m;
+    h->slab_stride = (big_slab_doubles(h->max_m) + 31) & ~(size_t)31;
+    const size_t bytes = h->slab_stride * sizeof(double) * (size_t)h->grid;
+    if (cudaMalloc(&h->d_slab, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("plan: cannot allocate %zu B of block slabs", bytes);
+        return BV_E_NOMEM;
+    }
+    h->launches.clear();
+    if (h->owned > 0) h->launches.push_back({0, h->owned, h->grid});
+    BV_CUDA_TRY(cudaMalloc(&h->d_counters, sizeof(unsigned)));
+    return BV_OK;
+}
+
 static int plan_launches(bv_handle *h)
 {
     cudaDeviceProp prop;
     BV_CUDA_TRY(cudaGetDeviceProperties(&prop, h->device));
+    if (h->opts.schedule >= 2) return plan_lean(h, prop, h->opts.schedule - 2);
     size_t avail = 0;
     int cap_m = 0;
     {
@@ -431,13 +518,13 @@ static int enqueue_eval(bv_handle *h, cudaStream_t s)
             LlhArgs a = fp64_args(h->d_counters, h->mixed.fallback_list, 0, h->owned);
             a.task_count = h->mixed.fallback_count;
             a.status_or = BV_ST_FP32_FALLBACK;
-            h->kernel<<<h->grid, kThreads, h->smem_bytes, s>>>(a);
+            h->kernel<<<h->grid, h->block_threads, h->smem_bytes, s>>>(a);
             BV_CUDA_TRY(cudaGetLastError());
         }
     } else {
         for (size_t l = 0; l < h->launches.size(); ++l) {
             LlhArgs a = fp64_args(h->d_counters + l, h->d_order, h->launches[l].begin, h->launches[l].end);
-            h->kernel<<<h->launches[l].grid, kThreads, h->smem_bytes, s>>>(a);
+            h->kernel<<<h->launches[l].grid, h->block_threads, h->smem_bytes, s>>>(a);
             BV_CUDA_TRY(cudaGetLastError());
         }
     }
@@ -508,6 +595,11 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
         h->max_m = std::max(h->max_m, h->batchNum[b] + (b == 0 ? 0 : h->cs));
     // Largest blocks first (longest-processing-time order), ties by index;
     // with sharding, every shard_count-th block of that order.
+    if (h->opts.schedule < 0 || h->opts.schedule >= 2 + (int)(sizeof(kLeanVariants) / sizeof(kLeanVariants[0]))) {
+        set_error("bv_create: unknown schedule %d", h->opts.schedule);
+        handle_free(h);
+        return BV_E_INVALID;
+    }
     if (h->opts.shard_count < 1 || h->opts.shard_index < 0 ||
         h->opts.shard_index >= h->opts.shard_count) {
         set_error("bv_create: shard_index %d outside [0, %d)", h->opts.shard_index,

@@ -62,7 +62,7 @@ struct BigLayout {
 
 __host__ __device__ inline unsigned big_align(unsigned v) { return (v + 127u) & ~127u; }
 
-__host__ __device__ inline BigLayout big_layout(int M)
+__host__ __device__ inline BigLayout big_layout(int M, int rc = kBigRC)
 {
     BigLayout l;
     const unsigned Mp = (unsigned)M + 1;
@@ -72,20 +72,20 @@ __host__ __device__ inline BigLayout big_layout(int M)
     l.o_Z = o;      o = big_align(o + 8u * M);
     l.o_cur = o;    o = big_align(o + 128u * Mp);
     l.o_next = o;   o = big_align(o + 128u * Mp);
-    l.o_stage0 = o; o = big_align(o + 128u * (kBigRC + 16));
-    l.o_stage1 = o; o = big_align(o + 128u * (kBigRC + 16));
+    l.o_stage0 = o; o = big_align(o + 128u * (rc + 16));
+    l.o_stage1 = o; o = big_align(o + 128u * (rc + 16));
     l.o_bar = o;    o = o + 16;
     l.total = o;
     return l;
 }
 
 // Largest M whose streamed-path layout fits in `bytes` of dynamic shared memory.
-inline int big_max_m_for_bytes(size_t bytes)
+inline int big_max_m_for_bytes(size_t bytes, int rc = kBigRC)
 {
     int lo = 1, hi = 8192;
     while (lo < hi) {
         const int mid = (lo + hi + 1) / 2;
-        if (big_layout(mid).total <= bytes)
+        if (big_layout(mid, rc).total <= bytes)
             lo = mid;
         else
             hi = mid - 1;
@@ -115,10 +115,21 @@ inline size_t big_slab_stride(int max_m, int small_m, int big_m)
 
 __device__ __forceinline__ int swz(int r, int c) { return c ^ ((r & 3) << 2); }
 
-// Named barrier over warps 1..15 (the update warps).
+// The static shared scratch the streamed path needs (a subset of
+// BlockShared), for kernels that run only this path.
+struct alignas(16) LeanShared {
+    double Lt[kNB][kNB];  // factored diagonal block, transposed
+    double inv[kNB];      // 1 / L_jj (0: failed pivot)
+    double red[2][kWarps];
+    unsigned status;
+    int task;
+};
+
+// Named barrier over warps 1..NT/32-1 (the update warps).
+template <int NT>
 __device__ __forceinline__ void update_warps_sync()
 {
-    asm volatile("bar.sync 1, %0;" ::"n"(kThreads - 32) : "memory");
+    asm volatile("bar.sync 1, %0;" ::"n"(NT - 32) : "memory");
 }
 
 // Entry (i, j) of the augmented system: covariance for i < M (plus the
@@ -180,18 +191,23 @@ __device__ __forceinline__ void panel_update_tiles(double *dst, int dst_r0, cons
     }
 }
 
-// One block with M > the shared-memory capacity.  smem: the dynamic area;
-// slab: this CTA's global slab (big_slab_doubles(M) doubles).
+// One block by the streamed path, run by a CTA of NT threads (warp 0
+// factors, the other NT/32 - 1 warps generate and update), with RC rows per
+// streamed chunk.  smem: the dynamic area (big_layout(M, RC).total bytes);
+// slab: this CTA's global slab (big_slab_doubles(M) doubles).  Every
+// element's operations and their order are the same for every NT and RC.
+template <int NT, int RC, typename SH>
 static __device__ __noinline__ void process_block_big(const LlhArgs &a, const MaternParams &mp, int b,
-                                               unsigned char *smem, double *slab, BlockShared &sh)
+                                                      unsigned char *smem, double *slab, SH &sh)
 {
+    constexpr int kT = NT, kW = NT / 32;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int off = a.acc[b];
     const int bs = a.acc[b + 1] - off;
     const int mc = (b == 0) ? 0 : a.cs;
     const int M = mc + bs, Mp = M + 1;
     const int P = big_panels(M);
-    const BigLayout l = big_layout(M);
+    const BigLayout l = big_layout(M, RC);
     double *X = reinterpret_cast<double *>(smem + l.o_X);
     double *Y = reinterpret_cast<double *>(smem + l.o_Y);
     double *Z = reinterpret_cast<double *>(smem + l.o_Z);
@@ -202,7 +218,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + l.o_bar);
 
     const int *kidx = a.knn + (size_t)b * a.cs;
-    for (int t = tid; t < M; t += kThreads) {
+    for (int t = tid; t < M; t += kT) {
         const int src = (t < mc) ? __ldg(kidx + t) : off + (t - mc);
         X[t] = __ldg(a.x + src);
         Y[t] = __ldg(a.y + src);
@@ -215,7 +231,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
     }
     __syncthreads();
     // Panel 0 into Pcur.
-    for (int e = tid; e < Mp * 16; e += kThreads) {
+    for (int e = tid; e < Mp * 16; e += kT) {
         const int r = e >> 4, c = e & 15;
         const double v = (c < M && r >= c) ? big_entry(X, Y, Z, M, r, c, mp) : 0.0;
         cur[r * 16 + swz(r, c)] = v;
@@ -254,27 +270,27 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         } else if (kb1 > 0) {
             // Panel p+1: generate, then apply panels 0..p-1 from the slab.
             const int nrows = Mp - n0;
-            for (int e = tid - 32; e < nrows * 16; e += kThreads - 32) {
+            for (int e = tid - 32; e < nrows * 16; e += kT - 32) {
                 const int r = n0 + (e >> 4), c = e & 15;
                 const int j = n0 + c;
                 const double v = (c < kb1 && r >= j) ? big_entry(X, Y, Z, M, r, j, mp) : 0.0;
                 nxt[(r - n0) * 16 + swz(r, c)] = v;
             }
-            update_warps_sync();
-            const int nchunk = (nrows + kBigRC - 1) / kBigRC;
+            update_warps_sync<NT>();
+            const int nchunk = (nrows + RC - 1) / RC;
             const int items = nchunk * p;       // (chunk, q), q fastest
             const bool producer = (tid == 32);
             auto issue = [&](int it) {
                 const int ch = it / p, q = it - ch * p;
                 const int s = it & 1;
-                const int r0 = n0 + ch * kBigRC, r1 = min(Mp, r0 + kBigRC);
+                const int r0 = n0 + ch * RC, r1 = min(Mp, r0 + RC);
                 const int nb = min(kNB, Mp - n0);
                 const double *pq = slab + big_panel_base(q, Mp);
                 const int q0 = q * kNB;
                 const unsigned abytes = 128u * (unsigned)(r1 - r0), bbytes = 128u * (unsigned)nb;
                 mbar_arrive_expect_tx(&bar[s], abytes + bbytes);
                 bulk_g2s(stage[s], pq + (size_t)(r0 - q0) * 16, abytes, &bar[s]);
-                bulk_g2s(stage[s] + kBigRC * 16, pq + (size_t)(n0 - q0) * 16, bbytes, &bar[s]);
+                bulk_g2s(stage[s] + RC * 16, pq + (size_t)(n0 - q0) * 16, bbytes, &bar[s]);
             };
             // The producer (thread 32) counts the copies it issued per stage
             // and the phases it saw complete, to drain after a timeout.
@@ -288,7 +304,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
             for (int it = 0; it < items; ++it) {
                 const int ch = it / p;
                 const int s = it & 1;
-                const int r0 = n0 + ch * kBigRC, r1 = min(Mp, r0 + kBigRC);
+                const int r0 = n0 + ch * RC, r1 = min(Mp, r0 + RC);
                 const unsigned par = (phase_bits >> s) & 1u;
                 if (!timed_out) {
                     if (mbar_wait_bounded(&bar[s], par))
@@ -297,9 +313,9 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
                         timed_out = true;
                 }
                 phase_bits ^= 1u << s;
-                panel_update_tiles(nxt, n0, stage[s], r0, stage[s] + kBigRC * 16, n0, r0, r1, 1,
-                                   kWarps - 1);
-                update_warps_sync();
+                panel_update_tiles(nxt, n0, stage[s], r0, stage[s] + RC * 16, n0, r0, r1, 1,
+                                   kW - 1);
+                update_warps_sync<NT>();
                 if (producer && !timed_out && it + 2 < items) {
                     fence_proxy_async_shared();
                     issue(it + 2);
@@ -317,7 +333,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         // Rows below the diagonal block: forward substitution against L_kk,
         // the two operands on step q+1's dependent chain (1 / L_{q+1,q+1} and
         // L_{q+2,q+1}) read one step ahead.
-        for (int r = k0 + kb + tid; r < Mp; r += kThreads) {
+        for (int r = k0 + kb + tid; r < Mp; r += kT) {
             double *row = cur + (r - k0) * 16;
             double w[kNB];
 #pragma unroll
@@ -355,10 +371,10 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
             double *pg = slab + big_panel_base(p, Mp);
             const double2 *s2 = reinterpret_cast<const double2 *>(cur);
             double2 *g2 = reinterpret_cast<double2 *>(pg);
-            for (int e = tid; e < (Mp - k0) * 8; e += kThreads) g2[e] = s2[e];
+            for (int e = tid; e < (Mp - k0) * 8; e += kT) g2[e] = s2[e];
         }
         if (kb1 > 0)
-            panel_update_tiles(nxt, n0, cur, k0, cur + (n0 - k0) * 16, n0, n0, Mp, 0, kWarps);
+            panel_update_tiles(nxt, n0, cur, k0, cur + (n0 - k0) * 16, n0, n0, Mp, 0, kW);
         fence_proxy_async_global();
         __syncthreads();
         double *t = cur;
@@ -368,7 +384,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
 
     // log det of the conditional factor (positive pivots) and |u|^2 (row M).
     double ld = 0.0, qf = 0.0;
-    for (int j = mc + tid; j < M; j += kThreads) {
+    for (int j = mc + tid; j < M; j += kT) {
         const int q = j / kNB, c = j - q * kNB;
         const double *pq = slab + big_panel_base(q, Mp);
         const double d = pq[(j - q * kNB) * 16 + swz(j, c)];
@@ -390,7 +406,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
     __syncthreads();
     if (tid == 0) {
         double Ls = 0.0, Qs = 0.0;
-        for (int w = 0; w < kWarps; ++w) {
+        for (int w = 0; w < kW; ++w) {
             Ls += sh.red[0][w];
             Qs += sh.red[1][w];
         }
@@ -428,7 +444,8 @@ __device__ __forceinline__ void run_block(const LlhArgs &a, const MaternParams &
     } else {
         double *slab = a.gslab + (size_t)blockIdx.x * a.gslab_stride;
         if (kBig && M <= a.big_max_m)
-            process_block_big(a, mp, b, reinterpret_cast<unsigned char *>(smem), slab, sh);
+            process_block_big<kThreads, kBigRC>(a, mp, b, reinterpret_cast<unsigned char *>(smem), slab,
+                                                sh);
         else
             process_block(a, mp, b, slab, slab + M, slab + 2 * M, sh);
     }

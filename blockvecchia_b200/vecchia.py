@@ -130,7 +130,7 @@ def knn(layout: Layout, device: int = 0) -> np.ndarray:
 
 _PREC = {"fp64": _lib.BV_PREC_FP64, "mixed": _lib.BV_PREC_MIXED}
 _FAIL = {"neginf": _lib.BV_FAIL_NEGINF, "continue": _lib.BV_FAIL_CONTINUE}
-_SCHED = {"persistent": 0, "bucketed": 1}
+_SCHED = {"persistent": 0, "bucketed": 1, "lean0": 2, "lean1": 3, "lean2": 4, "lean3": 5}
 _LARGE = {"auto": _lib.BV_LARGE_AUTO, "streamed": _lib.BV_LARGE_STREAMED, "slab": _lib.BV_LARGE_SLAB}
 
 
