@@ -273,21 +273,36 @@ def oracle_parity(L, theta, dev_blocks, dev_status, dev_total, threads):
     rel = np.abs(dev_blocks - ref_blocks) / np.maximum(1.0, np.abs(ref_blocks))
     ref_ok = float(np.sum(ref_blocks[ok]))
     dev_ok = float(np.sum(dev_blocks[ok]))
-    worst = np.argsort(-np.where(ok, rel, -1.0))[:5]
+    # The blocks furthest apart, and two others, against a 40-digit
+    # evaluation of the same inputs, with the condition number of each
+    # block's joint covariance.
+    from oracle import hp
+    eps = np.finfo(np.float64).eps
+    okb = np.nonzero(ok)[0]
+    worst = okb[np.argsort(-rel[okb])[:3]]
+    others = np.random.default_rng(1).choice(np.setdiff1d(okb, worst), min(2, len(okb) - len(worst)),
+                                             replace=False) if len(okb) > 3 else np.zeros(0, int)
     worst_rows = []
-    for b in worst:
-        if not ok[b]:
-            continue
+    for b in np.concatenate([worst, others]).astype(int):
         cs = L.cs
         ci = L.knn_idx[b * cs:(b + 1) * cs] if b > 0 else np.zeros(0, dtype=np.int32)
-        S22 = O.matern(L.x[ci], L.y[ci], L.x[ci], L.y[ci], theta) if len(ci) else np.ones((1, 1))
-        ev = np.linalg.eigvalsh(S22)
+        p = np.concatenate([ci, np.arange(L.batchNumAccum[b], L.batchNumAccum[b + 1])])
+        ev = np.linalg.eigvalsh(O.matern(L.x[p], L.y[p], L.x[p], L.y[p], theta))
+        kap = float(ev[-1] / ev[0]) if ev[0] > 0 else None
+        try:
+            truth = hp.block_llk(L.x, L.y, L.obs, L.batchNumAccum, L.knn_idx, L.cs, int(b), theta)
+        except ArithmeticError:
+            truth = None
         worst_rows.append({"block": int(b), "bs": int(L.batchNum[b]), "rel_diff": float(rel[b]),
-                           "kappa_sigma22": float(ev[-1] / ev[0]) if ev[0] > 0 else None,
-                           "min_eig_sigma22": float(ev[0])})
+                           "kappa_joint_cov": kap,
+                           "rel_diff_over_kappa_eps": float(rel[b] / (kap * eps)) if kap else None,
+                           "hp40_value": truth,
+                           "device_abs_err_vs_hp40": abs(float(dev_blocks[b]) - truth) if truth is not None else None,
+                           "oracle_abs_err_vs_hp40": abs(float(ref_blocks[b]) - truth) if truth is not None else None})
+    fin = lambda v: float(v) if np.isfinite(v) else None  # noqa: E731
     parity = {
-        "oracle_llk": ref_total,
-        "rel_err_total": abs(dev_total - ref_total) / abs(ref_total),
+        "oracle_llk": fin(ref_total),
+        "rel_err_total": fin(abs(dev_total - ref_total) / abs(ref_total)),
         "blocks": int(len(ref_blocks)),
         "failed_blocks_oracle": int(((pb[:, 2] != 0) | (pb[:, 3] != 0)).sum()),
         "failed_blocks_device": int(((dev_status & 3) != 0).sum()),
@@ -297,8 +312,10 @@ def oracle_parity(L, theta, dev_blocks, dev_status, dev_total, threads):
         "comparable_blocks_over_1e-8": int((rel[ok] > 1e-8).sum()),
         "max_block_rel_diff": float(rel[ok].max()) if ok.any() else None,
         "failed_blocks_over_1e-10": int((rel[failed] > 1e-10).sum()),
-        "worst_comparable_blocks": worst_rows,
-        "tolerance": "1e-10 relative (FP64 parity bound); per block |diff| / max(1, |block|)",
+        "blocks_checked_at_40_digits": worst_rows,
+        "tolerance": "1e-10 relative (FP64 parity bound); per block |diff| / max(1, |block|); "
+                     "a block with joint-covariance condition number kappa carries ~kappa*eps "
+                     "in any FP64 evaluation",
     }
     cpu = {"value": 1.0 / dt, "unit": "evals/s", "cores": threads, "kind": "port",
            "sample": f"one whole evaluation ({len(ref_blocks)} blocks) in {dt:.1f} s: the oracle "

@@ -986,14 +986,14 @@ extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *ob
     int hc[3] = {0, 0, 0};
     BV_CUDA_TRY(cudaMemcpyAsync(hc, check, sizeof(hc), cudaMemcpyDeviceToHost, s));
     BV_CUDA_TRY(cudaStreamSynchronize(s));
-    if (hc[0]) {
-        set_error("bv_llh_noalloc: block %d has inconsistent offsets or a conditioning index "
-                  "outside the earlier blocks", hc[0] - 1);
-        return BV_E_INVALID;
-    }
     if (hc[2]) {
         set_error("bv_llh_noalloc: block 0 has fewer than cs=%d points (firstbatch merges "
                   "clusters until >= cs)", cs);
+        return BV_E_INVALID;
+    }
+    if (hc[0]) {
+        set_error("bv_llh_noalloc: block %d has inconsistent offsets or a conditioning index "
+                  "outside the earlier blocks", hc[0] - 1);
         return BV_E_INVALID;
     }
     if (hc[1] > smem_max_m) {

@@ -199,6 +199,66 @@ void bvo_matern(double *A, int m, int n,
     }
 }
 
+/* core_dcmg with z_flag = 1 (the --3D / time_flag distance,
+ * src/ckernel.cpp:165-186 with the third coordinate):
+ * sqrt(pow(dx,2)+pow(dy,2)+pow(dz,2)), which the reference build contracts to
+ * sqrt(fma(dz, dz, fma(dx, dx, dy*dy))). */
+static double bvo_dist3(double x1, double y1, double z1, double x2, double y2,
+                        double z2)
+{
+    double dx = x2 - x1, dy = y2 - y1, dz = z2 - z1;
+    return sqrt(fma(dz, dz, fma(dx, dx, dy * dy)));
+}
+
+void bvo_matern3(double *A, int m, int n, const double *x1, const double *y1,
+                 const double *z1, const double *x2, const double *y2,
+                 const double *z2, const double *theta, double dist_scale)
+{
+    double sigma_square = theta[0];
+    double con = pow(2.0, theta[2] - 1.0) * tgamma(theta[2]);
+    con = 1.0 / con;
+    con = sigma_square * con;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < n; ++j) {
+            double expr = bvo_dist3(x1[i], y1[i], z1[i], x2[j], y2[j], z2[j]) / theta[1];
+            expr /= dist_scale;
+            A[i + (size_t)j * m] = (expr == 0)
+                                       ? sigma_square
+                                       : con * pow(expr, theta[2]) * bvo_besselk(theta[2], expr);
+        }
+}
+
+/* core_dcmg_spacetime_matern (src/ckernel.cpp:1421-1458), theta = {sigma2,
+ * range_spatial, nu_spatial, range_time, smooth_time, separability, aux}:
+ *   expr  = dist3(l1_i, l2_j) / theta[1]   (the distance includes z: the
+ *           reference calls calculateDistance with z_flag = 1)
+ *   g     = |z_i - z_j|^(2 theta[4]) / theta[3] + 1
+ *   expr3 = expr / g^(theta[5] / 2),  expr4 = g^(theta[5] + theta[6])
+ *   A     = expr == 0 ? sigma2 / expr4
+ *                     : con expr3^nu K_nu(expr3) / expr4. */
+void bvo_matern_st(double *A, int m, int n, const double *x1, const double *y1,
+                   const double *z1, const double *x2, const double *y2,
+                   const double *z2, const double *theta)
+{
+    double sigma_square = theta[0];
+    double con = pow(2.0, theta[2] - 1.0) * tgamma(theta[2]);
+    con = 1.0 / con;
+    con = sigma_square * con;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < n; ++j) {
+            double expr = bvo_dist3(x1[i], y1[i], z1[i], x2[j], y2[j], z2[j]) / theta[1];
+            double dz = z1[i] - z2[j];
+            double at = sqrt(dz * dz);
+            double g = pow(at, 2 * theta[4]) / theta[3] + 1.0;
+            double expr2 = pow(g, theta[5] / 2.0);
+            double expr3 = expr / expr2;
+            double expr4 = pow(g, theta[5] + theta[6]);
+            A[i + (size_t)j * m] =
+                (expr == 0) ? sigma_square / expr4
+                            : con * pow(expr3, theta[2]) * bvo_besselk(theta[2], expr3) / expr4;
+        }
+}
+
 /* ------------------------------------------------------------------------ */
 /* kNN conditioning sets (findNearestPoints)                                */
 /* ------------------------------------------------------------------------ */
@@ -304,6 +364,56 @@ void bvo_knn_all(const double *x, const double *y, int bc, int cs,
     for (int i = 1; i < bc; ++i)
         bvo_knn_block(x, y, batchNumAccum[i], cx[i], cy[i], cs,
                       knn_idx + (size_t)i * cs);
+}
+
+/* bvo_knn_block_fast with the time_flag key of findNearestPoints
+ * (include/nearest_neighbor.h:101-104): d = calEucDistance (contracted
+ * sqrt(fma(dx,dx,dy*dy))), then sqrt(d*d + dz*dz) contracted to
+ * sqrt(fma(d, d, dz*dz)), dz = cz - z_p. */
+int bvo_knn_block3_fast(const double *x, const double *y, const double *z,
+                        int prefix, double cx, double cy, double cz, int k,
+                        int *out_idx)
+{
+    if (prefix <= 0 || k <= 0) return 0;
+    if (k > prefix) k = prefix;
+    double *dist = (double *)malloc(sizeof(double) * (size_t)prefix);
+    double *tmp = (double *)malloc(sizeof(double) * (size_t)prefix);
+    for (int p = 0; p < prefix; ++p) {
+        double dx = x[p] - cx;
+        double dy = y[p] - cy;
+        double d = sqrt(fma(dx, dx, dy * dy));
+        double dz = cz - z[p];
+        dist[p] = sqrt(fma(d, d, dz * dz));
+        tmp[p] = dist[p];
+    }
+    double dk = bvo_select_kth(tmp, prefix, k - 1);
+    int m = 0;
+    for (int p = 0; p < prefix; ++p)
+        if (dist[p] <= dk) tmp[m++] = (double)p;
+    int *sidx = (int *)malloc(sizeof(int) * (size_t)m);
+    int *pos = (int *)malloc(sizeof(int) * (size_t)m);
+    for (int e = 0; e < m; ++e) {
+        sidx[e] = (int)tmp[e];
+        pos[e] = sidx[e];
+    }
+    for (int t = 0; t < k; ++t) {
+        int best = -1, occ = -1;
+        for (int e = 0; e < m; ++e) {
+            if (pos[e] < 0) continue;
+            if (best < 0 || dist[sidx[e]] < dist[sidx[best]] ||
+                (dist[sidx[e]] == dist[sidx[best]] && pos[e] < pos[best]))
+                best = e;
+            if (pos[e] == t) occ = e;
+        }
+        out_idx[t] = sidx[best];
+        if (occ >= 0 && occ != best) pos[occ] = pos[best];
+        pos[best] = -1;
+    }
+    free(dist);
+    free(tmp);
+    free(sidx);
+    free(pos);
+    return k;
 }
 
 void bvo_knn_all_fast(const double *x, const double *y, int bc, int cs,

@@ -65,6 +65,22 @@ void bvo_knn_all(const double *x, const double *y, int bc, int cs,
                  const int *batchNumAccum, const double *cx, const double *cy,
                  int *knn_idx);
 
+/* 3-D (--3D / time_flag) covariance: core_dcmg with z_flag = 1. */
+void bvo_matern3(double *A, int m, int n, const double *x1, const double *y1,
+                 const double *z1, const double *x2, const double *y2,
+                 const double *z2, const double *theta, double dist_scale);
+
+/* Space-time Matern, restating core_dcmg_spacetime_matern
+ * (src/ckernel.cpp:1421-1458); theta[7]. */
+void bvo_matern_st(double *A, int m, int n, const double *x1, const double *y1,
+                   const double *z1, const double *x2, const double *y2,
+                   const double *z2, const double *theta);
+
+/* bvo_knn_block_fast with the time_flag key of findNearestPoints. */
+int bvo_knn_block3_fast(const double *x, const double *y, const double *z,
+                        int prefix, double cx, double cy, double cz, int k,
+                        int *out_idx);
+
 /* bvo_knn_all with bvo_knn_block_fast per block (same result), OpenMP over
  * blocks with `threads` workers (<= 0: the OpenMP default). */
 void bvo_knn_all_fast(const double *x, const double *y, int bc, int cs,

@@ -68,6 +68,11 @@ def lib():
         L.bvo_knn_block.argtypes = [_D, _D, C.c_int, C.c_double, C.c_double, C.c_int, _I]
         L.bvo_knn_all.argtypes = [_D, _D, C.c_int, C.c_int, _I, _D, _D, _I]
         L.bvo_knn_all_fast.argtypes = [_D, _D, C.c_int, C.c_int, _I, _D, _D, _I, C.c_int]
+        L.bvo_matern3.argtypes = [_D, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, _D, C.c_double]
+        L.bvo_matern_st.argtypes = [_D, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, _D]
+        L.bvo_knn_block3_fast.restype = C.c_int
+        L.bvo_knn_block3_fast.argtypes = [_D, _D, _D, C.c_int, C.c_double, C.c_double, C.c_double,
+                                          C.c_int, _I]
         L.bvo_knn_block_fast.restype = C.c_int
         L.bvo_knn_block_fast.argtypes = [_D, _D, C.c_int, C.c_double, C.c_double, C.c_int, _I]
         L.bvo_llh.restype = C.c_double
@@ -94,6 +99,17 @@ def ref():
         L.ref_generate_xy.argtypes = [C.c_int, C.c_int, _D, _D]
         L.ref_core_dcmg.argtypes = [_D, C.c_int, C.c_int, _D, _D, _D, _D, _D, C.c_double]
         L.ref_find_nearest.argtypes = [_D, _D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _I]
+        L.ref_generate_xyt.argtypes = [C.c_int, C.c_int, C.c_int, _D, _D, _D]
+        L.ref_core_dcmg3.argtypes = [_D, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, _D, C.c_double]
+        L.ref_core_dcmg_st.argtypes = [_D, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, _D]
+        L.ref_find_nearest3.argtypes = [_D, _D, _D, C.c_int, C.c_int, C.c_double, C.c_double,
+                                        C.c_double, C.c_int, _I]
+        L.ref_kmeans3.restype = C.c_int
+        L.ref_kmeans3.argtypes = [_D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _I, _D,
+                                  _D, _D]
+        L.ref_layout_from_clusters3.restype = C.c_int
+        L.ref_layout_from_clusters3.argtypes = [_D, _D, _D, _D, C.c_int, C.c_int, _I, _D, _D, _D,
+                                                C.c_int, _I, _I, _D, _D, _D, _D, _D, _D, _D, _I, _I]
         L.ref_kmeans.restype = C.c_int
         L.ref_kmeans.argtypes = [_D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _I, _D, _D]
         L.ref_layout_from_clusters.restype = C.c_int
@@ -117,6 +133,69 @@ def matern(x1, y1, x2, y2, theta, dist_scale=1.0):
     th = np.ascontiguousarray(theta, dtype=np.float64)
     lib().bvo_matern(_dp(A), m, n, _dp(x1), _dp(y1), _dp(x2), _dp(y2), _dp(th), float(dist_scale))
     return A.reshape(n, m).T.copy()
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def matern3(x1, y1, z1, x2, y2, z2, theta, dist_scale=1.0):
+    """core_dcmg with z_flag = 1: (len(x1) x len(x2)) -> numpy (m, n)."""
+    x1, y1, z1, x2, y2, z2 = (_c(a) for a in (x1, y1, z1, x2, y2, z2))
+    m, n = len(x1), len(x2)
+    A = np.zeros(m * n)
+    lib().bvo_matern3(_dp(A), m, n, _dp(x1), _dp(y1), _dp(z1), _dp(x2), _dp(y2), _dp(z2),
+                      _dp(_c(theta)), float(dist_scale))
+    return A.reshape(n, m).T.copy()
+
+
+def matern_st(x1, y1, z1, x2, y2, z2, theta):
+    """core_dcmg_spacetime_matern restatement, theta[7]."""
+    x1, y1, z1, x2, y2, z2 = (_c(a) for a in (x1, y1, z1, x2, y2, z2))
+    m, n = len(x1), len(x2)
+    A = np.zeros(m * n)
+    lib().bvo_matern_st(_dp(A), m, n, _dp(x1), _dp(y1), _dp(z1), _dp(x2), _dp(y2), _dp(z2),
+                        _dp(_c(theta)))
+    return A.reshape(n, m).T.copy()
+
+
+def knn_block3_fast(x, y, z, prefix, cx, cy, cz, k):
+    out = np.zeros(max(k, 1), dtype=np.int32)
+    got = lib().bvo_knn_block3_fast(_dp(_c(x)), _dp(_c(y)), _dp(_c(z)), int(prefix), float(cx),
+                                    float(cy), float(cz), int(k), _ip(out))
+    return out[:got]
+
+
+def ref_generate_xyt(n, t_slots, seed):
+    N = n * t_slots
+    x, y, z = np.zeros(N), np.zeros(N), np.zeros(N)
+    ref().ref_generate_xyt(int(n), int(t_slots), int(seed), _dp(x), _dp(y), _dp(z))
+    return x, y, z
+
+
+def ref_core_dcmg3(x1, y1, z1, x2, y2, z2, theta, dist_scale=1.0):
+    x1, y1, z1, x2, y2, z2 = (_c(a).copy() for a in (x1, y1, z1, x2, y2, z2))
+    m, n = len(x1), len(x2)
+    A = np.zeros(m * n)
+    ref().ref_core_dcmg3(_dp(A), m, n, _dp(x1), _dp(y1), _dp(z1), _dp(x2), _dp(y2), _dp(z2),
+                         _dp(_c(theta)), float(dist_scale))
+    return A.reshape(n, m).T.copy()
+
+
+def ref_core_dcmg_st(x1, y1, z1, x2, y2, z2, theta):
+    x1, y1, z1, x2, y2, z2 = (_c(a).copy() for a in (x1, y1, z1, x2, y2, z2))
+    m, n = len(x1), len(x2)
+    A = np.zeros(m * n)
+    ref().ref_core_dcmg_st(_dp(A), m, n, _dp(x1), _dp(y1), _dp(z1), _dp(x2), _dp(y2), _dp(z2),
+                           _dp(_c(theta)))
+    return A.reshape(n, m).T.copy()
+
+
+def ref_find_nearest3(x, y, z, prefix, cx, cy, cz, k):
+    out = np.zeros(k, dtype=np.int32)
+    ref().ref_find_nearest3(_dp(_c(x)), _dp(_c(y)), _dp(_c(z)), len(x), int(prefix), float(cx),
+                            float(cy), float(cz), int(k), _ip(out))
+    return out[:min(k, prefix)]
 
 
 def knn_block(x, y, prefix, cx, cy, k):

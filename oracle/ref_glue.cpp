@@ -82,27 +82,96 @@ void ref_find_nearest(const double *x, const double *y, int n, int prefix,
     for (int t = 0; t < kk; ++t) out_idx[t] = (int)cond_obs[(size_t)kk + t];
 }
 
+/* GenerateXYLoc_ST (src/ckernel.cpp:78-118): n jittered grid points
+ * repeated over t_slots time slots, z = (slot + 1) / t_slots. */
+void ref_generate_xyt(int n, int t_slots, int seed, double *x, double *y, double *z)
+{
+    location *l = GenerateXYLoc_ST(n, t_slots, seed);
+    const size_t N = (size_t)n * t_slots;
+    memcpy(x, l->x, sizeof(double) * N);
+    memcpy(y, l->y, sizeof(double) * N);
+    memcpy(z, l->z, sizeof(double) * N);
+    free(l->x);
+    free(l->y);
+    free(l->z);
+    free(l);
+}
+
+/* core_dcmg with z_flag = 1 (the --3D / time_flag distance, src/ckernel.cpp
+ * :165-186 with the third coordinate). */
+void ref_core_dcmg3(double *A, int m, int n, double *x1, double *y1, double *z1,
+                    double *x2, double *y2, double *z2, const double *theta,
+                    double dist_scale)
+{
+    location l1 = {x1, y1, z1};
+    location l2 = {x2, y2, z2};
+    core_dcmg(A, m, n, &l1, &l2, theta, 0, 1, dist_scale);
+}
+
+/* core_dcmg_spacetime_matern (src/ckernel.cpp:1421-1458), theta[7]. */
+void ref_core_dcmg_st(double *A, int m, int n, double *x1, double *y1,
+                      double *z1, double *x2, double *y2, double *z2,
+                      const double *theta)
+{
+    location l1 = {x1, y1, z1};
+    location l2 = {x2, y2, z2};
+    core_dcmg_spacetime_matern(A, m, n, &l1, &l2, theta, 0);
+}
+
+/* findNearestPoints with time_flag (the 3-D key, include/nearest_neighbor.h
+ * :101-104). */
+void ref_find_nearest3(const double *x, const double *y, const double *z, int n,
+                       int prefix, double cx, double cy, double cz, int k,
+                       int *out_idx)
+{
+    std::vector<double> obs(n), xs(x, x + n), ys(y, y + n), zs(z, z + n);
+    for (int p = 0; p < n; ++p) obs[p] = (double)p;
+    std::vector<double> cond_obs((size_t)2 * k), cond_x((size_t)2 * k),
+        cond_y((size_t)2 * k), cond_z((size_t)2 * k);
+    location con = {cond_x.data(), cond_y.data(), cond_z.data()};
+    double cxv[2] = {cx, cx}, cyv[2] = {cy, cy}, czv[2] = {cz, cz};
+    location cent = {cxv, cyv, czv};
+    int fcc = 1;
+    location lnew = {xs.data(), ys.data(), zs.data()};
+    findNearestPoints(cond_obs.data(), &con, &cent, &fcc, obs.data(), &lnew, 0,
+                      prefix, k, 1, 0, true);
+    int kk = k < prefix ? k : prefix;
+    for (int t = 0; t < kk; ++t) out_idx[t] = (int)cond_obs[(size_t)kk + t];
+}
+
 /* random_initializer (include/initializer.h:35-56) + kmean_par
  * (src/kmeans.cpp:59-145).  Point coordinates[2] is set to 0 here; the
  * reference leaves it uninitialised (include/Point.h:20,30-39), and its
  * accumulators start from default-constructed Points whose coordinates are
  * never initialised either, so results can depend on memory contents. */
-int ref_kmeans(const double *x, const double *y, int n, int k, int seed,
-               int epochs, int threads, int *labels, double *cx, double *cy)
+int ref_kmeans3(const double *x, const double *y, const double *z, int n, int k,
+                int seed, int epochs, int threads, int *labels, double *cx,
+                double *cy, double *cz)
 {
-    location l = {(double *)x, (double *)y, nullptr};
+    location l = {(double *)x, (double *)y, (double *)z};
     location *lp = &l;
-    std::vector<Point> points = convertToPoints(lp, n, false);
-    for (auto &p : points) p.coordinates[2] = 0.0;
+    const bool tf = z != nullptr;
+    std::vector<Point> points = convertToPoints(lp, n, tf);
+    if (!tf)
+        for (auto &p : points) p.coordinates[2] = 0.0;
     std::vector<Point> centroids = random_initializer(points, k, seed);
-    for (auto &c : centroids) c.coordinates[2] = 0.0;
+    if (!tf)
+        for (auto &c : centroids) c.coordinates[2] = 0.0;
     kmean_par(points, centroids, epochs, k, threads);
     for (int i = 0; i < n; ++i) labels[i] = points[i].cluster;
     for (int c = 0; c < k; ++c) {
         cx[c] = centroids[c].coordinates[0];
         cy[c] = centroids[c].coordinates[1];
+        if (tf) cz[c] = centroids[c].coordinates[2];
     }
     return 0;
+}
+
+int ref_kmeans(const double *x, const double *y, int n, int k, int seed,
+               int epochs, int threads, int *labels, double *cx, double *cy)
+{
+    return ref_kmeans3(x, y, nullptr, n, k, seed, epochs, threads, labels, cx,
+                       cy, nullptr);
 }
 
 /* The driver's layout steps after clustering
@@ -112,23 +181,25 @@ int ref_kmeans(const double *x, const double *y, int n, int k, int seed,
  * Outputs (caller-allocated): batchNum[nclusters], batchNumAccum[nclusters+1],
  * x/y/obs_new[n], block centroids bcx/bcy[nclusters] (block i uses centroid
  * locsCentroid[i + firstClusterCount - 1]).  Returns batchCount. */
-int ref_layout_from_clusters(const double *x, const double *y,
-                             const double *obs, int n, int nclusters,
-                             const int *labels, const double *cx,
-                             const double *cy, int cs, int *batchNum,
-                             int *batchNumAccum, double *x_new, double *y_new,
-                             double *obs_new, double *bcx, double *bcy,
-                             int *first_cluster_count, int *first_cluster_size)
+int ref_layout_from_clusters3(const double *x, const double *y, const double *z,
+                              const double *obs, int n, int nclusters,
+                              const int *labels, const double *cx,
+                              const double *cy, const double *cz, int cs,
+                              int *batchNum, int *batchNumAccum, double *x_new,
+                              double *y_new, double *z_new, double *obs_new,
+                              double *bcx, double *bcy, double *bcz,
+                              int *first_cluster_count, int *first_cluster_size)
 {
-    location l = {(double *)x, (double *)y, nullptr};
+    const bool tf = z != nullptr;
+    location l = {(double *)x, (double *)y, (double *)z};
     location *lp = &l;
-    std::vector<Point> points = convertToPoints(lp, n, false);
+    std::vector<Point> points = convertToPoints(lp, n, tf);
     for (int i = 0; i < n; ++i) points[i].cluster = labels[i];
     std::vector<Point> centroids(nclusters);
     for (int c = 0; c < nclusters; ++c) {
         centroids[c].coordinates[0] = cx[c];
         centroids[c].coordinates[1] = cy[c];
-        centroids[c].coordinates[2] = 0.0;
+        centroids[c].coordinates[2] = tf ? cz[c] : 0.0;
         centroids[c].cluster = c;
     }
     int *clusterNum = countPointsInClusters(points);                    /* :266 */
@@ -136,14 +207,18 @@ int ref_layout_from_clusters(const double *x, const double *y,
     location cent;
     cent.x = (double *)malloc(sizeof(double) * (size_t)nclusters);
     cent.y = (double *)malloc(sizeof(double) * (size_t)nclusters);
-    cent.z = nullptr;
+    cent.z = tf ? (double *)malloc(sizeof(double) * (size_t)nclusters) : nullptr;
     for (int i = 0; i < nclusters; ++i) {                               /* :273-282 */
         cent.x[i] = centroids[i].coordinates[0];
         cent.y[i] = centroids[i].coordinates[1];
+        if (tf) cent.z[i] = centroids[i].coordinates[2];
         permIndex[i] = centroids[i].cluster;
     }
-    random_reordering(nclusters, &cent);                                /* :288 */
-    reorderIndex(&cent, centroids, permIndex, nclusters, false);        /* :319 */
+    if (tf)                                                             /* :288 */
+        random_reordering_3d(nclusters, &cent);
+    else
+        random_reordering(nclusters, &cent);
+    reorderIndex(&cent, centroids, permIndex, nclusters, tf);           /* :319 */
     int fcs = 0, fcc = 0;
     firstbatch(nclusters, clusterNum, permIndex, &fcs, &fcc, cs);       /* :323 */
     int batchCount = nclusters - fcc + 1;                               /* :325 */
@@ -154,13 +229,14 @@ int ref_layout_from_clusters(const double *x, const double *y,
         batchNum[i] = clusterNum[permIndex[i + fcc - 1]];
     for (int i = 1; i < batchCount + 1; ++i)                            /* :345-349 */
         batchNumAccum[i] += batchNumAccum[i - 1] + batchNum[i - 1];
-    location lnew = {x_new, y_new, nullptr};
+    location lnew = {x_new, y_new, tf ? z_new : nullptr};
     std::vector<double> obs_copy(obs, obs + n);
     cluster_to_batch(n, batchCount, batchNum, batchNumAccum, batchIndex, &l,  /* :352 */
-                     obs_copy.data(), &lnew, obs_new, points, &cent, false);
+                     obs_copy.data(), &lnew, obs_new, points, &cent, tf);
     for (int i = 0; i < batchCount; ++i) {
         bcx[i] = cent.x[i + fcc - 1];
         bcy[i] = cent.y[i + fcc - 1];
+        if (tf) bcz[i] = cent.z[i + fcc - 1];
     }
     *first_cluster_count = fcc;
     *first_cluster_size = fcs;
@@ -168,7 +244,23 @@ int ref_layout_from_clusters(const double *x, const double *y,
     free(permIndex);
     free(cent.x);
     free(cent.y);
+    free(cent.z);
     return batchCount;
+}
+
+int ref_layout_from_clusters(const double *x, const double *y,
+                             const double *obs, int n, int nclusters,
+                             const int *labels, const double *cx,
+                             const double *cy, int cs, int *batchNum,
+                             int *batchNumAccum, double *x_new, double *y_new,
+                             double *obs_new, double *bcx, double *bcy,
+                             int *first_cluster_count, int *first_cluster_size)
+{
+    return ref_layout_from_clusters3(x, y, nullptr, obs, n, nclusters, labels, cx,
+                                     cy, nullptr, cs, batchNum, batchNumAccum,
+                                     x_new, y_new, nullptr, obs_new, bcx, bcy,
+                                     nullptr, first_cluster_count,
+                                     first_cluster_size);
 }
 
 } /* extern "C" */

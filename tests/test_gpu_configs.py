@@ -14,13 +14,22 @@ headline metric and its companions are quoted on, at full size:
 Observations are one random-Fourier-feature draw of the same process (the
 value depends on them only through the quadratic form).
 
-Tolerances: the total log-likelihood within 1e-10 relative of the oracle
-(the FP64 parity bound); per block, |device - oracle| / max(1, |block|),
-counted above 1e-10 and 1e-8 and reported (-s shows the counts).  Blocks
-where either side met a non-positive pivot are not comparable (the oracle's
-LAPACK potrf stops at the failing column, the device zeroes it and goes on)
-and are left out of the per-block counts and the sample sum.
+Tolerances.  The total log-likelihood: within 1e-10 relative of the oracle
+(the FP64 parity bound) where the blocks are well conditioned (the first two
+configurations).  Per block, rel = |device - oracle| / max(1, |block|): a
+block whose joint covariance (conditioning and block points together) has
+condition number kappa carries about kappa * eps of rounding in any FP64
+evaluation, so every block must satisfy rel <= 1e-10 or rel <= 10 * kappa *
+eps.  At the headline configuration (nu = 2.5, range 0.05, 1M points)
+kappa reaches 1e16: there the sample's sum is reported, not bounded, and for
+four blocks (the two furthest apart and two others) a 40-digit evaluation of
+the same inputs (oracle/hp.py) decides: the device must be as close to it as
+the oracle is, within a factor of 10.  Blocks where either side met a
+non-positive pivot are not comparable (the oracle's LAPACK potrf stops at
+the failing column, the device zeroes it and goes on) and are left out.
 """
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 import pytest
 
@@ -29,6 +38,8 @@ from bench import make_locations, rff_draw
 pytestmark = pytest.mark.gpu
 
 REL = 1e-10
+EPS = np.finfo(np.float64).eps
+KAPPA_FACTOR = 10.0
 
 
 def _layout(bv, x, y, theta, bc, cs, epochs=50):
@@ -36,6 +47,22 @@ def _layout(bv, x, y, theta, bc, cs, epochs=50):
     L = bv.build_layout(x, y, obs, bc, cs, seed=0, epochs=epochs)
     L.knn_idx = bv.knn(L)
     return L
+
+
+def _block_points(L, b):
+    cs = L.cs
+    idx = L.knn_idx[b * cs:(b + 1) * cs] if b > 0 else np.zeros(0, dtype=np.int32)
+    return np.concatenate([idx, np.arange(L.batchNumAccum[b], L.batchNumAccum[b + 1])])
+
+
+def _kappas(oracle, L, blocks, theta):
+    """Condition number of each block's joint covariance (oracle Matern)."""
+    def one(b):
+        p = _block_points(L, b)
+        ev = np.linalg.eigvalsh(oracle.matern(L.x[p], L.y[p], L.x[p], L.y[p], theta))
+        return ev[-1] / ev[0] if ev[0] > 0 else np.inf
+    with ThreadPoolExecutor(16) as ex:
+        return np.array(list(ex.map(one, blocks)))
 
 
 def _compare(bv, oracle, L, theta, b0=0, b1=None):
@@ -50,41 +77,64 @@ def _compare(bv, oracle, L, theta, b0=0, b1=None):
     failed = (pb[b0:b1, 2] != 0) | (pb[b0:b1, 3] != 0) | ((dev_status & 3) != 0)
     ok = ~failed
     rel = np.abs(dev_blocks - ref_blocks) / np.maximum(1.0, np.abs(ref_blocks))
+    over = np.nonzero(ok & (rel > REL))[0]
+    kap = _kappas(oracle, L, over + b0, theta)
+    ratio = rel[over] / (kap * EPS) if len(over) else np.zeros(0)
     ref_sum = float(np.sum(ref_blocks[ok]))
     dev_sum = float(np.sum(dev_blocks[ok]))
     stats = dict(blocks=int(b1 - b0), failed=int(failed.sum()),
                  sum_rel_err=abs(dev_sum - ref_sum) / abs(ref_sum),
-                 blocks_over_1e10=int((rel[ok] > 1e-10).sum()),
-                 blocks_over_1e8=int((rel[ok] > 1e-8).sum()),
-                 max_block_rel=float(rel[ok].max()) if ok.any() else 0.0)
+                 blocks_over_1e10=int(len(over)), blocks_over_1e8=int((rel[ok] > 1e-8).sum()),
+                 max_block_rel=float(rel[ok].max()) if ok.any() else 0.0,
+                 max_rel_over_kappa_eps=float(ratio.max()) if len(ratio) else 0.0,
+                 min_kappa_of_those=float(kap.min()) if len(kap) else None)
     print(stats)
-    return total, ref_total, stats
+    return dict(total=total, ref_total=ref_total, stats=stats, rel=rel, ok=ok,
+                dev=dev_blocks, ref=ref_blocks, b0=b0)
 
 
 def test_c1_20k_cs300(bvlib, oracle):
     x, y = bvlib.generate_xy(20_000, 0)
     th = (1.5, 0.1, 0.5)
     L = _layout(bvlib, x, y, th, 1500, 300)
-    total, ref, s = _compare(bvlib, oracle, L, th)
+    r = _compare(bvlib, oracle, L, th)
+    s = r["stats"]
     assert s["failed"] == 0
-    assert abs(total - ref) <= REL * abs(ref), (total, ref)
-    assert s["blocks_over_1e8"] == 0, s
+    assert abs(r["total"] - r["ref_total"]) <= REL * abs(r["ref_total"])
+    assert s["blocks_over_1e10"] == 0, s
 
 
 def test_c2_200k_cs120(bvlib, oracle):
     x, y = make_locations(200_000, 0)
     th = (1.0, 0.08, 1.5)
     L = _layout(bvlib, x, y, th, 20_000, 120)
-    total, ref, s = _compare(bvlib, oracle, L, th)
+    r = _compare(bvlib, oracle, L, th)
+    s = r["stats"]
     assert s["failed"] == 0
-    assert abs(total - ref) <= REL * abs(ref), (total, ref)
-    assert s["blocks_over_1e8"] <= s["blocks"] // 1000, s
+    assert abs(r["total"] - r["ref_total"]) <= REL * abs(r["ref_total"])
+    assert s["max_rel_over_kappa_eps"] <= KAPPA_FACTOR, s
 
 
 def test_c3_1m_cs200_sample(bvlib, oracle):
+    from oracle import hp
     x, y = make_locations(1_000_000, 0)
     th = (1.0, 0.05, 2.5)
     L = _layout(bvlib, x, y, th, 100_000, 200)
     mid = L.bc // 2
-    _, _, s = _compare(bvlib, oracle, L, th, b0=mid, b1=mid + 3000)
-    assert s["sum_rel_err"] <= REL, s
+    r = _compare(bvlib, oracle, L, th, b0=mid, b1=mid + 3000)
+    s = r["stats"]
+    assert s["max_rel_over_kappa_eps"] <= KAPPA_FACTOR, s
+    # A 40-digit evaluation of four comparable blocks: the device is as close
+    # to it as the oracle is.
+    ok = np.nonzero(r["ok"])[0]
+    worst = ok[np.argsort(-r["rel"][ok])[:2]]
+    rng = np.random.default_rng(1)
+    pick = np.concatenate([worst, rng.choice(np.setdiff1d(ok, worst), 2, replace=False)])
+    dev_err = ref_err = 0.0
+    for i in pick:
+        b = int(i) + r["b0"]
+        truth = hp.block_llk(L.x, L.y, L.obs, L.batchNumAccum, L.knn_idx, L.cs, b, th)
+        dev_err += abs(r["dev"][i] - truth)
+        ref_err += abs(r["ref"][i] - truth)
+        print({"block": b, "truth": truth, "device": float(r["dev"][i]), "oracle": float(r["ref"][i])})
+    assert dev_err <= 10 * ref_err + 1e-12, (dev_err, ref_err)

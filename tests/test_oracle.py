@@ -178,3 +178,30 @@ def test_knn_fast_matches_selection_sort(oracle):
         cx, cy = np.round(rng.random(2), 3)
         assert np.array_equal(oracle.knn_block_fast(x, y, prefix, cx, cy, k),
                               oracle.knn_block(x, y, prefix, cx, cy, k))
+
+
+def test_spacetime_and_3d_pins_against_reference(ref):
+    """Space-time Matern (core_dcmg_spacetime_matern), the 3-D core_dcmg
+    (z_flag = 1) and the time_flag conditioning-set key: the oracle's
+    restatements are bit-identical to the reference's own code."""
+    rng = np.random.default_rng(21)
+    n = 400
+    x, y = rng.random(n), rng.random(n)
+    z = rng.random(n)
+    zt = np.floor(rng.random(n) * 8 + 1) / 8  # time slots (slot + 1) / t_slots
+    for th in [(1.5, 0.1, 0.5), (1.0, 0.07, 1.3), (0.5, 0.2, 2.7)]:
+        assert np.array_equal(ref.matern3(x[:50], y[:50], z[:50], x, y, z, th),
+                              ref.ref_core_dcmg3(x[:50], y[:50], z[:50], x, y, z, th))
+    for th in [(1.0, 0.1, 0.5, 0.5, 0.9, 0.7, 0.0), (1.3, 0.2, 1.1, 0.3, 0.5, 0.4, 0.2),
+               (0.8, 0.05, 2.5, 1.0, 0.7, 1.0, 0.1)]:
+        assert np.array_equal(ref.matern_st(x[:50], y[:50], zt[:50], x, y, zt, th),
+                              ref.ref_core_dcmg_st(x[:50], y[:50], zt[:50], x, y, zt, th))
+    # Conditioning sets with the 3-D key, including exact ties (repeated
+    # locations in other time slots).
+    xs, ys = np.tile(x[:100], 4), np.tile(y[:100], 4)
+    zs = np.repeat(np.arange(1, 5) / 4.0, 100)
+    for t in range(60):
+        p = int(rng.integers(40, 400))
+        c = rng.random(3)
+        assert np.array_equal(ref.knn_block3_fast(xs, ys, zs, p, c[0], c[1], c[2], 30),
+                              ref.ref_find_nearest3(xs, ys, zs, p, c[0], c[1], c[2], 30))
