@@ -47,12 +47,16 @@ EXPORTS = {
     "bv_last_error": (C.c_char_p, []),
     "bv_llh_host": (C.c_int, [C.c_void_p, _D, _D, _D, _I, _D, _D]),
     "bv_knn": (C.c_int, [_D, _D, C.c_int, C.c_int, C.c_int, _I, _D, _D, _I, C.c_int]),
+    "bv_knn3": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, C.c_int, _I, _D, _D, _D, _I, C.c_int]),
     "bv_layout_build": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                   _I, _I, _D, _D, _D, _D, _D, _I, _I]),
     "bv_layout_from_clusters": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, _I, _D, _D, C.c_int,
                                           _I, _I, _D, _D, _D, _D, _D, _I, _I]),
     "bv_kmeans": (C.c_int, [_D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _I, _D, _D]),
     "bv_generate_xy": (C.c_int, [C.c_int, C.c_int, _D, _D]),
+    "bv_generate_xyt": (C.c_int, [C.c_int, C.c_int, C.c_int, _D, _D, _D]),
+    "bv_layout_build3": (C.c_int, [_D, _D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.c_int, _I, _I, _D, _D, _D, _D, _D, _D, _D, _I, _I]),
     "bv_shard_blocks": (C.c_int, [_I, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_ubyte)]),
     "bv_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "bv_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -77,7 +81,7 @@ class BvLayout(C.Structure):
     _fields_ = [("n", C.c_int), ("bc", C.c_int), ("cs", C.c_int),
                 ("batchNum", _I), ("batchNumAccum", _I),
                 ("x", _D), ("y", _D), ("obs", _D), ("knn_idx", _I),
-                ("cx", _D), ("cy", _D)]
+                ("cx", _D), ("cy", _D), ("z", _D), ("cz", _D)]
 
 
 class BvOpts(C.Structure):

@@ -25,7 +25,8 @@ int validate_layout(const bv_layout *L);
 // large-block path holds.  Every caller (handles, the server, the
 // allocation-free entry point) uses the same limits, so a block always takes
 // the same path.
-int fp64_limits(int device, size_t *avail, int *small_m, int *big_m);
+// nz = 1 for layouts with a third coordinate (one more array per block).
+int fp64_limits(int device, size_t *avail, int *small_m, int *big_m, int nz = 0);
 
 // Whether a layout's evaluation compiles the streamed large-block path in:
 // only when more than one wave (sm_count) of blocks has small_m < M <= big_m;

@@ -6,7 +6,11 @@
 //   key(p) = sqrt(fma(dx, dx, dy*dy)), dx = x[p] - cx, dy = y[p] - cy
 //   (calEucDistance :30-35 as the reference's -O3 -march=native build
 //   contracts it), then k = cs rounds of a selection sort with swaps and a
-//   strict '<' (:115-133), output in selection order.
+//   strict '<' (:115-133), output in selection order.  With a third
+//   coordinate (the reference's time_flag, :101-104) the key is
+//   sqrt(fma(d, d, dz*dz)), d the 2-D key and dz = cz - z[p], as contracted.
+// Both keys are the square root of a "pre-key" computed exactly as the
+// reference computes the root's argument; the selection works on pre-keys.
 //
 // The warp streams the candidates once, keeping those whose squared distance
 // is within a few ulps of the running k-th smallest (a threshold that only
@@ -47,8 +51,10 @@ struct KnnWarpSmem {
 
 struct KnnArgs {
     const double *x, *y;
+    const double *z;        // third coordinate, or nullptr (2-D)
     const int *acc;
     const double *cx, *cy;  // device copies
+    const double *cz;       // device copy, when z is set
     int bc, cs;
     int *out;
     unsigned *counter;
@@ -56,6 +62,18 @@ struct KnnArgs {
     int *heavy;  // blocks whose ties overflow the buffer, for knn_heavy_kernel
     unsigned *heavy_count;
 };
+
+// The argument of the key's final square root for candidate p.
+__device__ __forceinline__ double knn_prekey(const KnnArgs &a, int p, double cx, double cy, double cz)
+{
+    const double dx = __ldg(a.x + p) - cx;
+    const double dy = __ldg(a.y + p) - cy;
+    const double s = __fma_rn(dx, dx, __dmul_rn(dy, dy));
+    if (!a.z) return s;
+    const double d = __dsqrt_rn(s);
+    const double dz = cz - __ldg(a.z + p);
+    return __fma_rn(d, d, __dmul_rn(dz, dz));
+}
 
 __device__ __forceinline__ unsigned lanemask_lt()
 {
@@ -173,7 +191,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
         const int i = a.bc - 1 - (int)task;
         if (i < 1) break;
         const int P = a.acc[i];
-        const double cx = a.cx[i], cy = a.cy[i];
+        const double cx = a.cx[i], cy = a.cy[i], cz = a.z ? a.cz[i] : 0.0;
         int *out = a.out + (size_t)i * k;
         if (P < k) {
             if (lane == 0) atomicCAS(a.error, 0, i + 1);
@@ -193,9 +211,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
                 keep[u] = false;
                 key[u] = 0ull;
                 if (p < P) {
-                    const double dx = __ldg(a.x + p) - cx;
-                    const double dy = __ldg(a.y + p) - cy;
-                    const double s = __fma_rn(dx, dx, __dmul_rn(dy, dy));
+                    const double s = knn_prekey(a, p, cx, cy, cz);
                     key[u] = (unsigned long long)__double_as_longlong(s);
                     keep[u] = key[u] <= lim;
                 }
@@ -308,12 +324,10 @@ struct KnnHeavyScratch {
     int *pos;
 };
 
-__device__ __forceinline__ unsigned long long knn_skey(const double *x, const double *y, int p, double cx,
-                                                       double cy)
+__device__ __forceinline__ unsigned long long knn_skey(const KnnArgs &a, int p, double cx, double cy,
+                                                       double cz)
 {
-    const double dx = __ldg(x + p) - cx;
-    const double dy = __ldg(y + p) - cy;
-    return (unsigned long long)__double_as_longlong(__fma_rn(dx, dx, __dmul_rn(dy, dy)));
+    return (unsigned long long)__double_as_longlong(knn_prekey(a, p, cx, cy, cz));
 }
 
 __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int nheavy, KnnHeavyScratch scr,
@@ -331,7 +345,7 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
     for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
         const int i = a.heavy[h];
         const int P = a.acc[i];
-        const double cx = a.cx[i], cy = a.cy[i];
+        const double cx = a.cx[i], cy = a.cy[i], cz = a.z ? a.cz[i] : 0.0;
         int *out = a.out + (size_t)i * k;
         // 1. Exact k-th smallest squared distance, MSB-first radix select.
         if (tid == 0) {
@@ -344,7 +358,7 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
             __syncthreads();
             const unsigned long long prefix = s_prefix;
             for (int p = tid; p < P; p += kHeavyThreads) {
-                const unsigned long long key = knn_skey(a.x, a.y, p, cx, cy);
+                const unsigned long long key = knn_skey(a, p, cx, cy, cz);
                 if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255ull], 1u);
             }
             __syncthreads();
@@ -371,7 +385,7 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
         if (tid == 0) s_count = 0;
         __syncthreads();
         for (int p = tid; p < P; p += kHeavyThreads) {
-            const unsigned long long key = knn_skey(a.x, a.y, p, cx, cy);
+            const unsigned long long key = knn_skey(a, p, cx, cy, cz);
             if (key <= hi) {
                 const double d = __dsqrt_rn(__longlong_as_double((long long)key));
                 if (d <= dk) {
@@ -437,9 +451,14 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
     }
 }
 
-int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, const int *d_acc,
-               const double *cx, const double *cy, int *d_knn, cudaStream_t s)
+int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, int bc, int cs,
+               const int *d_acc, const double *cx, const double *cy, const double *cz, int *d_knn,
+               cudaStream_t s)
 {
+    if (d_z && !cz) {
+        set_error("bv_knn: 3-D locations need the centroids' third coordinate");
+        return BV_E_INVALID;
+    }
     if (cs <= 0) return BV_OK;
     if (cs > kKnnMaxCs) {
         set_error("bv_knn: cs=%d exceeds the supported maximum %d", cs, kKnnMaxCs);
@@ -456,7 +475,7 @@ int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, cons
         rc = BV_E_CUDA;
     };
     cudaError_t e;
-    if ((e = cudaMalloc(&d_c, sizeof(double) * 2 * (size_t)bc)) != cudaSuccess) {
+    if ((e = cudaMalloc(&d_c, sizeof(double) * 3 * (size_t)bc)) != cudaSuccess) {
         fail(e, "cudaMalloc");
         return rc;
     }
@@ -473,6 +492,8 @@ int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, cons
     do {
         if ((e = cudaMemcpyAsync(d_c, cx, sizeof(double) * bc, cudaMemcpyHostToDevice, s)) ||
             (e = cudaMemcpyAsync(d_c + bc, cy, sizeof(double) * bc, cudaMemcpyHostToDevice, s)) ||
+            (d_z && (e = cudaMemcpyAsync(d_c + 2 * (size_t)bc, cz, sizeof(double) * bc,
+                                         cudaMemcpyHostToDevice, s))) ||
             (e = cudaMemcpyAsync(d_knn, first.data(), sizeof(int) * cs, cudaMemcpyHostToDevice, s)) ||
             (e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned) * 3, s))) {
             fail(e, "copy");
@@ -481,9 +502,11 @@ int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, cons
         KnnArgs ka;
         ka.x = d_x;
         ka.y = d_y;
+        ka.z = d_z;
         ka.acc = d_acc;
         ka.cx = d_c;
         ka.cy = d_c + bc;
+        ka.cz = d_c + 2 * (size_t)bc;
         ka.bc = bc;
         ka.cs = cs;
         ka.out = d_knn;
@@ -552,12 +575,13 @@ int knn_device(const double *d_x, const double *d_y, int n, int bc, int cs, cons
 
 }  // namespace bv
 
-extern "C" int bv_knn(const double *x, const double *y, int n, int bc, int cs,
-                      const int *batchNumAccum, const double *cx, const double *cy, int *knn_idx,
-                      int device)
+static int knn_host(const double *x, const double *y, const double *z, int n, int bc, int cs,
+                    const int *batchNumAccum, const double *cx, const double *cy, const double *cz,
+                    int *knn_idx, int device)
 {
     using namespace bv;
-    if (!x || !y || !batchNumAccum || !cx || !cy || !knn_idx || n <= 0 || bc <= 0 || cs < 0) {
+    if (!x || !y || !batchNumAccum || !cx || !cy || !knn_idx || n <= 0 || bc <= 0 || cs < 0 ||
+        (z && !cz)) {
         set_error("bv_knn: invalid argument");
         return BV_E_INVALID;
     }
@@ -574,12 +598,13 @@ extern "C" int bv_knn(const double *x, const double *y, int n, int bc, int cs,
     BV_CUDA_TRY(cudaSetDevice(device));
     cudaStream_t s;
     BV_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    double *d_x = nullptr, *d_y = nullptr;
+    double *d_x = nullptr, *d_y = nullptr, *d_z = nullptr;
     int *d_acc = nullptr, *d_knn = nullptr;
     int rc = BV_OK;
     cudaError_t e;
     do {
         if ((e = cudaMalloc(&d_x, sizeof(double) * n)) || (e = cudaMalloc(&d_y, sizeof(double) * n)) ||
+            (z && (e = cudaMalloc(&d_z, sizeof(double) * n))) ||
             (e = cudaMalloc(&d_acc, sizeof(int) * (bc + 1))) ||
             (e = cudaMalloc(&d_knn, sizeof(int) * (size_t)bc * cs))) {
             set_error("bv_knn: cudaMalloc: %s", cudaGetErrorString(e));
@@ -588,12 +613,13 @@ extern "C" int bv_knn(const double *x, const double *y, int n, int bc, int cs,
         }
         if ((e = cudaMemcpyAsync(d_x, x, sizeof(double) * n, cudaMemcpyHostToDevice, s)) ||
             (e = cudaMemcpyAsync(d_y, y, sizeof(double) * n, cudaMemcpyHostToDevice, s)) ||
+            (z && (e = cudaMemcpyAsync(d_z, z, sizeof(double) * n, cudaMemcpyHostToDevice, s))) ||
             (e = cudaMemcpyAsync(d_acc, batchNumAccum, sizeof(int) * (bc + 1), cudaMemcpyHostToDevice, s))) {
             set_error("bv_knn: copy: %s", cudaGetErrorString(e));
             rc = BV_E_CUDA;
             break;
         }
-        rc = knn_device(d_x, d_y, n, bc, cs, d_acc, cx, cy, d_knn, s);
+        rc = knn_device(d_x, d_y, d_z, n, bc, cs, d_acc, cx, cy, cz, d_knn, s);
         if (rc) break;
         if ((e = cudaMemcpyAsync(knn_idx, d_knn, sizeof(int) * (size_t)bc * cs, cudaMemcpyDeviceToHost, s)) ||
             (e = cudaStreamSynchronize(s))) {
@@ -603,8 +629,27 @@ extern "C" int bv_knn(const double *x, const double *y, int n, int bc, int cs,
     } while (0);
     cudaFree(d_x);
     cudaFree(d_y);
+    cudaFree(d_z);
     cudaFree(d_acc);
     cudaFree(d_knn);
     cudaStreamDestroy(s);
     return rc;
+}
+
+extern "C" int bv_knn(const double *x, const double *y, int n, int bc, int cs,
+                      const int *batchNumAccum, const double *cx, const double *cy, int *knn_idx,
+                      int device)
+{
+    return knn_host(x, y, nullptr, n, bc, cs, batchNumAccum, cx, cy, nullptr, knn_idx, device);
+}
+
+extern "C" int bv_knn3(const double *x, const double *y, const double *z, int n, int bc, int cs,
+                       const int *batchNumAccum, const double *cx, const double *cy,
+                       const double *cz, int *knn_idx, int device)
+{
+    if (!z || !cz) {
+        bv::set_error("bv_knn3: z and cz are required");
+        return BV_E_INVALID;
+    }
+    return knn_host(x, y, z, n, bc, cs, batchNumAccum, cx, cy, cz, knn_idx, device);
 }

@@ -133,6 +133,8 @@ struct bv_handle {
     int owned = 0;  // blocks this handle evaluates (all, or its shard)
     // device
     double *d_x = nullptr, *d_y = nullptr, *d_obs = nullptr;
+    double *d_z = nullptr;  // third coordinate of 3-D layouts
+    int nz = 0;             // 1 when the layout has a third coordinate
     int *d_acc = nullptr, *d_knn = nullptr, *d_order = nullptr;
     double *d_block_llk = nullptr;
     unsigned *d_block_status = nullptr;
@@ -183,6 +185,7 @@ static void handle_free(bv_handle *h)
     cudaFree(h->d_x);
     cudaFree(h->d_y);
     cudaFree(h->d_obs);
+    cudaFree(h->d_z);
     cudaFree(h->d_acc);
     cudaFree(h->d_knn);
     cudaFree(h->d_order);
@@ -309,12 +312,12 @@ static size_t fused_static_smem()
 }
 
 // Largest M whose block fits in `bytes` of dynamic shared memory.
-static int max_m_for_bytes(size_t bytes, size_t per_double)
+static int max_m_for_bytes(size_t bytes, size_t per_double, int nz = 0)
 {
     int lo = 1, hi = 4096;
     while (lo < hi) {
         int mid = (lo + hi + 1) / 2;
-        if (block_doubles(mid) * per_double <= bytes)
+        if (block_doubles(mid, nz) * per_double <= bytes)
             lo = mid;
         else
             hi = mid - 1;
@@ -322,14 +325,14 @@ static int max_m_for_bytes(size_t bytes, size_t per_double)
     return lo;
 }
 
-int bv::fp64_limits(int device, size_t *avail, int *small_m, int *big_m)
+int bv::fp64_limits(int device, size_t *avail, int *small_m, int *big_m, int nz)
 {
     int optin = 0;
     BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     const size_t av = (size_t)optin - fused_static_smem();
     if (avail) *avail = av;
-    if (small_m) *small_m = max_m_for_bytes(av, sizeof(double));
-    if (big_m) *big_m = big_max_m_for_bytes(av);
+    if (small_m) *small_m = max_m_for_bytes(av, sizeof(double), nz);
+    if (big_m) *big_m = big_max_m_for_bytes(av, kBigRC, nz);
     return BV_OK;
 }
 
@@ -352,13 +355,13 @@ static int plan_lean(bv_handle *h, const cudaDeviceProp &prop, int variant)
     int optin = 0;
     BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
     const size_t avail = (size_t)optin - fa.sharedSizeBytes;
-    if ((size_t)big_layout(h->max_m, v.rc).total > avail) {
+    if ((size_t)big_layout(h->max_m, v.rc, h->nz).total > avail) {
         set_error("plan: blocks of M = %d exceed the streamed schedule's shared memory", h->max_m);
         return BV_E_TOOLARGE;
     }
     h->kernel = v.kernel;
     h->block_threads = v.threads;
-    h->smem_bytes = big_layout(h->max_m, v.rc).total;
+    h->smem_bytes = big_layout(h->max_m, v.rc, h->nz).total;
     h->use_big = true;
     BV_CUDA_TRY(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)h->smem_bytes));
@@ -392,7 +395,7 @@ static int plan_launches(bv_handle *h)
     size_t avail = 0;
     int cap_m = 0;
     {
-        const int rc = fp64_limits(h->device, &avail, &cap_m, &h->big_max_m);
+        const int rc = fp64_limits(h->device, &avail, &cap_m, &h->big_max_m, h->nz);
         if (rc) return rc;
     }
     h->smem_max_m = std::min(cap_m, h->max_m);
@@ -410,11 +413,11 @@ static int plan_launches(bv_handle *h)
                                prop.multiProcessorCount));
     h->kernel = h->use_big ? llh_fp64_big_kernel : llh_fp64_kernel;
     if (h->use_big) {
-        h->smem_bytes = big_launch_smem(h->max_m, cap_m, h->big_max_m);
-        h->slab_stride = big_slab_stride(h->max_m, cap_m, h->big_max_m);
+        h->smem_bytes = big_launch_smem(h->max_m, cap_m, h->big_max_m, h->nz);
+        h->slab_stride = big_slab_stride(h->max_m, cap_m, h->big_max_m, h->nz);
     } else {
-        h->smem_bytes = block_doubles(h->smem_max_m) * sizeof(double);
-        h->slab_stride = (h->max_m > cap_m) ? (block_doubles(h->max_m) + 31) & ~(size_t)31 : 0;
+        h->smem_bytes = block_doubles(h->smem_max_m, h->nz) * sizeof(double);
+        h->slab_stride = (h->max_m > cap_m) ? (block_doubles(h->max_m, h->nz) + 31) & ~(size_t)31 : 0;
     }
     int occ = 0;
     BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, h->kernel, kThreads, h->smem_bytes));
@@ -475,6 +478,7 @@ static int enqueue_eval(bv_handle *h, cudaStream_t s)
         a.x = h->d_x;
         a.y = h->d_y;
         a.obs = h->d_obs;
+        a.z = h->d_z;
         a.acc = h->d_acc;
         a.knn = h->d_knn;
         a.order = order;
@@ -585,6 +589,17 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
         handle_free(h);
         return BV_E_NODEVICE;
     }
+    if (h->opts.kernel == 4 && !L->z) {
+        set_error("bv_create: the space-time kernel (4) needs the layout's third coordinate (z)");
+        handle_free(h);
+        return BV_E_INVALID;
+    }
+    if (L->z && h->opts.precision == BV_PREC_MIXED) {
+        set_error("bv_create: the mixed-precision path evaluates 2-D Matern layouts only");
+        handle_free(h);
+        return BV_E_INVALID;
+    }
+    h->nz = L->z ? 1 : 0;
     h->n = L->n;
     h->bc = L->bc;
     h->cs = L->cs;
@@ -637,6 +652,10 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
     BV_CUDA_H(cudaMemcpy(h->d_x, L->x, n * sizeof(double), cudaMemcpyHostToDevice));
     BV_CUDA_H(cudaMemcpy(h->d_y, L->y, n * sizeof(double), cudaMemcpyHostToDevice));
     BV_CUDA_H(cudaMemcpy(h->d_obs, L->obs, n * sizeof(double), cudaMemcpyHostToDevice));
+    if (L->z) {
+        BV_CUDA_H(cudaMalloc(&h->d_z, n * sizeof(double)));
+        BV_CUDA_H(cudaMemcpy(h->d_z, L->z, n * sizeof(double), cudaMemcpyHostToDevice));
+    }
     BV_CUDA_H(cudaMemcpy(h->d_acc, L->batchNumAccum, (bc + 1) * sizeof(int), cudaMemcpyHostToDevice));
     if (h->owned > 0)
         BV_CUDA_H(cudaMemcpy(h->d_order, h->order.data(), h->owned * sizeof(int),
@@ -648,8 +667,8 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
         if (L->knn_idx) {
             BV_CUDA_H(cudaMemcpy(h->d_knn, L->knn_idx, bc * cs * sizeof(int), cudaMemcpyHostToDevice));
         } else {
-            BV_TRY_H(knn_device(h->d_x, h->d_y, h->n, h->bc, h->cs, h->d_acc, L->cx, L->cy,
-                                h->d_knn, h->stream));
+            BV_TRY_H(knn_device(h->d_x, h->d_y, h->d_z, h->n, h->bc, h->cs, h->d_acc, L->cx, L->cy,
+                                L->cz, h->d_knn, h->stream));
             BV_CUDA_H(cudaStreamSynchronize(h->stream));
         }
     }
@@ -689,13 +708,31 @@ static int fill_params(bv_handle *h, const double *theta)
         set_error("bv_llh: invalid theta (%g, %g, %g)", sigma2, range, nu);
         return BV_E_INVALID;
     }
-    const double tau2 = h->opts.nugget ? theta[3] : 0.0;
+    const bool st = h->opts.kernel == 4;
+    // The nugget follows the kernel's own parameters: theta[3], or theta[7]
+    // after the space-time kernel's seven.
+    const double tau2 = h->opts.nugget ? theta[st ? 7 : 3] : 0.0;
     if (!(tau2 >= 0) || !std::isfinite(tau2)) {
         set_error("bv_llh: invalid nugget %g", tau2);
         return BV_E_INVALID;
     }
     MaternParams &p = *h->h_mp;
     p.nugget = tau2;
+    p.model = st ? kModelSpaceTime : (h->nz ? kModel3D : kModel2D);
+    p.st_range_t = p.st_pow = p.st_half = p.st_outer = 0.0;
+    if (st) {
+        // src/ckernel.cpp:1439-1443 (theta[3..6]).
+        if (!(theta[3] > 0) || !std::isfinite(theta[3]) || !std::isfinite(theta[4]) ||
+            !std::isfinite(theta[5]) || !std::isfinite(theta[6])) {
+            set_error("bv_llh: invalid space-time parameters (%g, %g, %g, %g)", theta[3], theta[4],
+                      theta[5], theta[6]);
+            return BV_E_INVALID;
+        }
+        p.st_range_t = theta[3];
+        p.st_pow = 2 * theta[4];
+        p.st_half = theta[5] / 2.0;
+        p.st_outer = theta[5] + theta[6];
+    }
     p.sigma2 = sigma2;
     p.range = range;
     p.nu = nu;
@@ -752,8 +789,12 @@ static int eval_locked(bv_handle *h, const double *theta, double *llk)
 
 static void print_iteration(bv_handle *h, const double *theta, double llk)
 {
-    // include/llh_Xvecchia_batch.h:500-511
-    if (h->opts.kernel == 3 || h->opts.nugget)
+    // include/llh_Xvecchia_batch.h:500-516
+    if (h->opts.kernel == 4)
+        printf("%dth Model Parameters (Variance, beta, nu, beta_time, nu_time, sep): (%lf, %lf, %lf, "
+               "%lf, %lf, %lf) -> Loglik: %lf \n",
+               h->iterations, theta[0], theta[1], theta[2], theta[3], theta[4], theta[5], llk);
+    else if (h->opts.kernel == 3 || h->opts.nugget)
         printf("%dth Model Parameters (Variance, range, smoothness, nugget): (%1.8lf, %1.8lf, "
                "%1.8lf, %1.8lf) -> Loglik: %.18lf \n",
                h->iterations, theta[0], theta[1], theta[2], theta[3], llk);
@@ -782,8 +823,9 @@ extern "C" double bv_llh(unsigned n, const double *theta, double *grad, void *f_
 {
     (void)grad;
     bv_handle *h = static_cast<bv_handle *>(f_data);
-    if (!h || !theta || n < (h && h->opts.nugget ? 4u : 3u)) {
-        set_error("bv_llh: need a handle and at least 3 parameters (4 with the nugget)");
+    const unsigned need = h ? (h->opts.kernel == 4 ? 7u : 3u) + (h->opts.nugget ? 1u : 0u) : 3u;
+    if (!h || !theta || n < need) {
+        set_error("bv_llh: need a handle and at least %u parameters", need);
         return -HUGE_VAL;
     }
     double v = -HUGE_VAL;
@@ -1010,6 +1052,7 @@ extern "C" int bv_llh_noalloc(const double *x, const double *y, const double *ob
         return BV_E_INVALID;
     }
     MaternParams mp{};
+    mp.model = kModel2D;
     double con = std::pow(2.0, nu - 1.0) * std::tgamma(nu);
     con = 1.0 / con;
     mp.sigma2 = sigma2;

@@ -54,15 +54,16 @@ __host__ __device__ inline size_t big_panel_base(int q, int Mp)
     return 16 * ((size_t)q * Mp - 8 * (size_t)q * (q - 1));
 }
 
-// Shared-memory layout (bytes): X, Y, Z (M doubles each), Pcur, Pnext (Mp x
-// 16 doubles), two stages of (kBigRC + 16) x 16 doubles, two mbarriers.
+// Shared-memory layout (bytes): X, Y, Z (observations), T (third
+// coordinate, 3-D locations only; nz = 1) (M doubles each), Pcur, Pnext (Mp
+// x 16 doubles), two stages of (rc + 16) x 16 doubles, two mbarriers.
 struct BigLayout {
-    unsigned o_X, o_Y, o_Z, o_cur, o_next, o_stage0, o_stage1, o_bar, total;
+    unsigned o_X, o_Y, o_Z, o_T, o_cur, o_next, o_stage0, o_stage1, o_bar, total;
 };
 
 __host__ __device__ inline unsigned big_align(unsigned v) { return (v + 127u) & ~127u; }
 
-__host__ __device__ inline BigLayout big_layout(int M, int rc = kBigRC)
+__host__ __device__ inline BigLayout big_layout(int M, int rc = kBigRC, int nz = 0)
 {
     BigLayout l;
     const unsigned Mp = (unsigned)M + 1;
@@ -70,6 +71,7 @@ __host__ __device__ inline BigLayout big_layout(int M, int rc = kBigRC)
     l.o_X = o;      o = big_align(o + 8u * M);
     l.o_Y = o;      o = big_align(o + 8u * M);
     l.o_Z = o;      o = big_align(o + 8u * M);
+    l.o_T = o;      if (nz) o = big_align(o + 8u * M);
     l.o_cur = o;    o = big_align(o + 128u * Mp);
     l.o_next = o;   o = big_align(o + 128u * Mp);
     l.o_stage0 = o; o = big_align(o + 128u * (rc + 16));
@@ -80,12 +82,12 @@ __host__ __device__ inline BigLayout big_layout(int M, int rc = kBigRC)
 }
 
 // Largest M whose streamed-path layout fits in `bytes` of dynamic shared memory.
-inline int big_max_m_for_bytes(size_t bytes, int rc = kBigRC)
+inline int big_max_m_for_bytes(size_t bytes, int rc = kBigRC, int nz = 0)
 {
     int lo = 1, hi = 8192;
     while (lo < hi) {
         const int mid = (lo + hi + 1) / 2;
-        if (big_layout(mid, rc).total <= bytes)
+        if (big_layout(mid, rc, nz).total <= bytes)
             lo = mid;
         else
             hi = mid - 1;
@@ -95,21 +97,21 @@ inline int big_max_m_for_bytes(size_t bytes, int rc = kBigRC)
 
 // Dynamic shared memory and per-CTA slab (doubles) for blocks up to M = max_m,
 // given the shared-memory path's limit small_m and the streamed path's big_m.
-inline size_t big_launch_smem(int max_m, int small_m, int big_m)
+inline size_t big_launch_smem(int max_m, int small_m, int big_m, int nz = 0)
 {
-    size_t b = block_doubles(std::min(max_m, small_m)) * sizeof(double);
+    size_t b = block_doubles(std::min(max_m, small_m), nz) * sizeof(double);
     if (max_m > small_m) {
-        const size_t t = big_layout(std::min(max_m, big_m)).total;
+        const size_t t = big_layout(std::min(max_m, big_m), kBigRC, nz).total;
         if (t > b) b = t;
     }
     return b;
 }
 
-inline size_t big_slab_stride(int max_m, int small_m, int big_m)
+inline size_t big_slab_stride(int max_m, int small_m, int big_m, int nz = 0)
 {
     if (max_m <= small_m) return 0;
     size_t d = big_slab_doubles(std::min(max_m, big_m));
-    if (max_m > big_m) d = std::max(d, block_doubles(max_m));
+    if (max_m > big_m) d = std::max(d, block_doubles(max_m, nz));
     return (d + 31) & ~(size_t)31;
 }
 
@@ -136,11 +138,11 @@ __device__ __forceinline__ void update_warps_sync()
 // nugget on the diagonal), the observation of point j on row M.  Same
 // argument order and the same nugget addition as the shared-memory path's
 // generation, so the entries are identical.
-__device__ __forceinline__ double big_entry(const double *X, const double *Y, const double *Z, int M,
-                                            int i, int j, const MaternParams &mp)
+__device__ __forceinline__ double big_entry(const double *X, const double *Y, const double *Z,
+                                            const double *T, int M, int i, int j, const MaternParams &mp)
 {
     if (i >= M) return Z[j];
-    const double c = matern(X[i], Y[i], X[j], Y[j], mp);
+    const double c = T ? cov_xyz(X[i], Y[i], T[i], X[j], Y[j], T[j], mp) : matern(X[i], Y[i], X[j], Y[j], mp);
     return (i == j && mp.nugget != 0.0) ? c + mp.nugget : c;
 }
 
@@ -207,10 +209,11 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
     const int mc = (b == 0) ? 0 : a.cs;
     const int M = mc + bs, Mp = M + 1;
     const int P = big_panels(M);
-    const BigLayout l = big_layout(M, RC);
+    const BigLayout l = big_layout(M, RC, a.z ? 1 : 0);
     double *X = reinterpret_cast<double *>(smem + l.o_X);
     double *Y = reinterpret_cast<double *>(smem + l.o_Y);
     double *Z = reinterpret_cast<double *>(smem + l.o_Z);
+    double *T = a.z ? reinterpret_cast<double *>(smem + l.o_T) : nullptr;
     double *cur = reinterpret_cast<double *>(smem + l.o_cur);
     double *nxt = reinterpret_cast<double *>(smem + l.o_next);
     double *stage[2] = {reinterpret_cast<double *>(smem + l.o_stage0),
@@ -223,6 +226,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         X[t] = __ldg(a.x + src);
         Y[t] = __ldg(a.y + src);
         Z[t] = __ldg(a.obs + src);
+        if (T) T[t] = __ldg(a.z + src);
     }
     if (tid == 0) {
         mbar_init(&bar[0], 1);
@@ -233,7 +237,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
     // Panel 0 into Pcur.
     for (int e = tid; e < Mp * 16; e += kT) {
         const int r = e >> 4, c = e & 15;
-        const double v = (c < M && r >= c) ? big_entry(X, Y, Z, M, r, c, mp) : 0.0;
+        const double v = (c < M && r >= c) ? big_entry(X, Y, Z, T, M, r, c, mp) : 0.0;
         cur[r * 16 + swz(r, c)] = v;
     }
     __syncthreads();
@@ -273,7 +277,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
             for (int e = tid - 32; e < nrows * 16; e += kT - 32) {
                 const int r = n0 + (e >> 4), c = e & 15;
                 const int j = n0 + c;
-                const double v = (c < kb1 && r >= j) ? big_entry(X, Y, Z, M, r, j, mp) : 0.0;
+                const double v = (c < kb1 && r >= j) ? big_entry(X, Y, Z, T, M, r, j, mp) : 0.0;
                 nxt[(r - n0) * 16 + swz(r, c)] = v;
             }
             update_warps_sync<NT>();
@@ -440,14 +444,17 @@ __device__ __forceinline__ void run_block(const LlhArgs &a, const MaternParams &
             a.block_status[b] = a.status_or;
         }
     } else if (M <= a.smem_max_m) {
-        process_block(a, mp, b, smem, smem + M, smem + 2 * M, sh);
+        const int nc = a.z ? 3 : 2;  // coordinate arrays before the matrix
+        process_block(a, mp, b, smem, smem + M, a.z ? smem + 2 * M : nullptr, smem + nc * M, sh);
     } else {
         double *slab = a.gslab + (size_t)blockIdx.x * a.gslab_stride;
-        if (kBig && M <= a.big_max_m)
+        if (kBig && M <= a.big_max_m) {
             process_block_big<kThreads, kBigRC>(a, mp, b, reinterpret_cast<unsigned char *>(smem), slab,
                                                 sh);
-        else
-            process_block(a, mp, b, slab, slab + M, slab + 2 * M, sh);
+        } else {
+            const int nc = a.z ? 3 : 2;
+            process_block(a, mp, b, slab, slab + M, a.z ? slab + 2 * M : nullptr, slab + nc * M, sh);
+        }
     }
 }
 

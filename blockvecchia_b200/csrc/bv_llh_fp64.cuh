@@ -45,6 +45,7 @@ constexpr unsigned kStDeviceTimeout = 16u;     // block status: a bounded wait g
 
 struct LlhArgs {
     const double *x, *y, *obs;  // [n] block-ordered
+    const double *z;            // [n] block-ordered third coordinate, or nullptr (2-D)
     const int *acc;             // [bc+1]
     const int *knn;             // [bc*cs]
     const int *order;           // [bc] processing order (largest first)
@@ -134,8 +135,12 @@ __device__ __forceinline__ void fence_mbar_init()
 
 __host__ __device__ inline size_t packed_elems(int Mp) { return (size_t)Mp * (Mp + 1) / 2; }
 
-// Doubles a block of size M needs: x[M], y[M], packed (M+1)-row triangle.
-__host__ __device__ inline size_t block_doubles(int M) { return 2 * (size_t)M + packed_elems(M + 1); }
+// Doubles a block of size M needs: x[M], y[M] (and z[M] for 3-D locations,
+// nz = 1), packed (M+1)-row triangle.
+__host__ __device__ inline size_t block_doubles(int M, int nz = 0)
+{
+    return (2 + (size_t)nz) * (size_t)M + packed_elems(M + 1);
+}
 
 __device__ __forceinline__ int poff(int j, int Mp) { return j * Mp - ((j * (j + 1)) >> 1); }
 
@@ -215,9 +220,12 @@ __device__ __forceinline__ double matern_kind(double x1, double y1, double x2, d
     return (r == 0.0) ? mp.sigma2 : mp.sigma2 * c;
 }
 
+// KIND kXYZ: locations with a third coordinate T (cov_xyz).
+constexpr int kXYZ = 16;
+
 template <int KIND>
-__device__ __forceinline__ void generate_t(double *A, const double *X, const double *Y, int M,
-                                           const MaternParams &mp)
+__device__ __forceinline__ void generate_t(double *A, const double *X, const double *Y, const double *T,
+                                           int M, const MaternParams &mp)
 {
     const int Mp = M + 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -248,7 +256,10 @@ __device__ __forceinline__ void generate_t(double *A, const double *X, const dou
             const int i = first ? qq + rr : jbb + (rr - naa);
             const int j = first ? qq : jbb;
             dst[u] = valid ? poff(j, Mp) + i : -1;
-            v[u] = matern_kind<KIND>(X[i], Y[i], X[j], Y[j], mp);
+            if constexpr (KIND == kXYZ)
+                v[u] = cov_xyz(X[i], Y[i], T[i], X[j], Y[j], T[j], mp);
+            else
+                v[u] = matern_kind<KIND>(X[i], Y[i], X[j], Y[j], mp);
         }
 #pragma unroll
         for (int u = 0; u < kGenU; ++u)
@@ -256,21 +267,32 @@ __device__ __forceinline__ void generate_t(double *A, const double *X, const dou
     }
 }
 
-__device__ __forceinline__ void generate(double *A, const double *X, const double *Y, int M,
-                                         const MaternParams &mp)
+// Out of line, so the 2-D kernels' register allocation does not carry it.
+static __device__ __noinline__ void generate_xyz(double *A, const double *X, const double *Y,
+                                                 const double *T, int M, const MaternParams &mp)
 {
+    generate_t<kXYZ>(A, X, Y, T, M, mp);
+}
+
+__device__ __forceinline__ void generate(double *A, const double *X, const double *Y, const double *T,
+                                         int M, const MaternParams &mp)
+{
+    if (T) {
+        generate_xyz(A, X, Y, T, M, mp);
+        return;
+    }
     switch (mp.nu_kind) {
     case kNuHalf:
-        generate_t<kNuHalf>(A, X, Y, M, mp);
+        generate_t<kNuHalf>(A, X, Y, nullptr, M, mp);
         break;
     case kNuThreeHalves:
-        generate_t<kNuThreeHalves>(A, X, Y, M, mp);
+        generate_t<kNuThreeHalves>(A, X, Y, nullptr, M, mp);
         break;
     case kNuFiveHalves:
-        generate_t<kNuFiveHalves>(A, X, Y, M, mp);
+        generate_t<kNuFiveHalves>(A, X, Y, nullptr, M, mp);
         break;
     default:
-        generate_t<kNuGeneral>(A, X, Y, M, mp);
+        generate_t<kNuGeneral>(A, X, Y, nullptr, M, mp);
         break;
     }
 }
@@ -1014,9 +1036,11 @@ __device__ __forceinline__ void cholesky_pp(double *A, int M, int mc, BlockShare
     }
 }
 
-// One block, with its matrix at A (shared memory or the global slab).
+// One block, with its matrix at A (shared memory or the global slab); T
+// holds the third coordinate of 3-D locations (nullptr for 2-D).
 __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternParams &mp, int b,
-                                              double *X, double *Y, double *A, BlockShared &sh)
+                                              double *X, double *Y, double *T, double *A,
+                                              BlockShared &sh)
 {
     const int tid = threadIdx.x;
     const int off = a.acc[b];
@@ -1031,10 +1055,11 @@ __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternPara
         const int src = (t < mc) ? __ldg(kidx + t) : off + (t - mc);
         X[t] = __ldg(a.x + src);
         Y[t] = __ldg(a.y + src);
+        if (T) T[t] = __ldg(a.z + src);
         A[poff(t, Mp) + M] = __ldg(a.obs + src);
     }
     __syncthreads();
-    generate(A, X, Y, M, mp);
+    generate(A, X, Y, T, M, mp);
     __syncthreads();
     if (mp.nugget != 0.0) {
         // Nugget: tau^2 on the diagonal of Sigma22 and Sigma11 (a point with

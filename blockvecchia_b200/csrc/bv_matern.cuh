@@ -23,6 +23,7 @@
 namespace bv {
 
 enum NuKind : int { kNuGeneral = 0, kNuHalf = 1, kNuThreeHalves = 2, kNuFiveHalves = 3 };
+enum Model : int { kModel2D = 0, kModel3D = 1, kModelSpaceTime = 2 };
 
 // Parameters of one evaluation (host-computed scalars).
 struct MaternParams {
@@ -37,6 +38,12 @@ struct MaternParams {
     int scale_is_one;   // dist_scale == 1.0: the second division is exact and skipped
     double nugget;      // tau^2 added to the diagonal of Sigma11 and Sigma22 (0: none,
                         // the reference's likelihood, which never reads theta[3])
+    // Locations with a third coordinate (the reference's time_flag):
+    int model;          // kModel2D, kModel3D (core_dcmg with z_flag = 1) or kModelSpaceTime
+    double st_range_t;  // space-time: theta[3]
+    double st_pow;      // 2 * theta[4]
+    double st_half;     // theta[5] / 2
+    double st_outer;    // theta[5] + theta[6]
     // General nu (matern_prepare): nu = mu + nn, |mu| <= 1/2.
     int nn;
     double mu;
@@ -304,6 +311,32 @@ __device__ __forceinline__ double matern(double x1, double y1, double x2, double
                                          const MaternParams &p)
 {
     return matern_from_r(matern_r(x1, y1, x2, y2, p), p);
+}
+
+// Covariance of two points with a third coordinate.  The distance is
+// calculateDistance with z_flag = 1 (src/ckernel.cpp:165-186),
+// sqrt(pow(dx,2)+pow(dy,2)+pow(dz,2)) as the reference's build contracts it:
+// sqrt(fma(dz, dz, fma(dx, dx, dy*dy))).
+//   kModel3D: core_dcmg on that distance (src/ckernel.cpp:1057-1093).
+//   kModelSpaceTime: core_dcmg_spacetime_matern (src/ckernel.cpp:1421-1458):
+//     r = dist / range, g = |dz|^(2 theta[4]) / theta[3] + 1,
+//     C = r == 0 ? sigma2 / g^(theta[5] + theta[6])
+//               : Matern(r / g^(theta[5] / 2)) / g^(theta[5] + theta[6]).
+__device__ __forceinline__ double cov_xyz(double x1, double y1, double z1, double x2, double y2,
+                                          double z2, const MaternParams &p)
+{
+    const double dx = x2 - x1, dy = y2 - y1, dz = z2 - z1;
+    const double dist = __dsqrt_rn(__fma_rn(dz, dz, __fma_rn(dx, dx, __dmul_rn(dy, dy))));
+    double r = div_by_recip(dist, p.range, p.inv_range);
+    if (p.model != kModelSpaceTime) {
+        if (!p.scale_is_one) r = div_by_recip(r, p.dist_scale, p.inv_ds);
+        return matern_from_r(r, p);
+    }
+    // sqrt(pow(z0 - z1, 2)) is |dz| exactly.
+    const double g = pow(fabs(dz), p.st_pow) / p.st_range_t + 1.0;
+    const double outer = pow(g, p.st_outer);
+    if (r == 0.0) return p.sigma2 / outer;
+    return matern_from_r(r / pow(g, p.st_half), p) / outer;
 }
 
 }  // namespace bv

@@ -274,6 +274,7 @@ void fill_params(MaternParams &p, const double *theta, double dist_scale)
     p.nu_kind = (nu == 0.5) ? kNuHalf : (nu == 1.5) ? kNuThreeHalves : (nu == 2.5) ? kNuFiveHalves
                                                                                   : kNuGeneral;
     p.nugget = theta[3];
+    p.model = kModel2D;
     matern_prepare(p);
 }
 
@@ -698,6 +699,10 @@ extern "C" int bv_server_open_job_ex(bv_server *S, const bv_layout *L, const bv_
     }
     const int vr = validate_layout(L);
     if (vr != BV_OK) return vr;
+    if (L->z) {
+        set_error("bv_server_open_job: the server evaluates 2-D Matern layouts (no third coordinate)");
+        return BV_E_INVALID;
+    }
     if (L->cs > 0 && !L->knn_idx) {
         set_error("bv_server_open_job: the layout's conditioning indices (knn_idx) are required");
         return BV_E_INVALID;

@@ -35,6 +35,8 @@ class Layout:
     knn_idx: Optional[np.ndarray] = None
     first_cluster_count: int = 1
     extra: dict = field(default_factory=dict)
+    z: Optional[np.ndarray] = None    # third coordinate (time or depth), block-ordered
+    cz: Optional[np.ndarray] = None   # the block centroids' third coordinate
 
     @property
     def n(self) -> int:
@@ -55,6 +57,10 @@ class Layout:
             self.cy = np.ascontiguousarray(self.cy, dtype=np.float64)
         if self.knn_idx is not None:
             self.knn_idx = np.ascontiguousarray(self.knn_idx, dtype=np.int32)
+        if self.z is not None:
+            self.z = np.ascontiguousarray(self.z, dtype=np.float64)
+        if self.cz is not None:
+            self.cz = np.ascontiguousarray(self.cz, dtype=np.float64)
         return self
 
 
@@ -64,6 +70,15 @@ def generate_xy(n: int, seed: int = 0):
     y = np.zeros(n)
     check(lib().bv_generate_xy(int(n), int(seed), dp(x), dp(y)))
     return x, y
+
+
+def generate_xyt(n: int, t_slots: int, seed: int = 0):
+    """GenerateXYLoc_ST (src/ckernel.cpp:78-118): n grid points over t_slots
+    time slots, z = (slot + 1) / t_slots; arrays of n * t_slots."""
+    N = n * t_slots
+    x, y, z = np.zeros(N), np.zeros(N), np.zeros(N)
+    check(lib().bv_generate_xyt(int(n), int(t_slots), int(seed), dp(x), dp(y), dp(z)))
+    return x, y, z
 
 
 def kmeans(x, y, k: int, seed: int = 0, epochs: int = 50, threads: int = 0):
@@ -99,9 +114,13 @@ def layout_from_clusters(x, y, obs, labels, ccx, ccy, cs: int) -> Layout:
 
 
 def build_layout(x, y, obs, bc: int, cs: int, seed: int = 0, epochs: int = 50,
-                 threads: int = 0) -> Layout:
+                 threads: int = 0, z=None) -> Layout:
     """The driver's setup: classic Vecchia if n < 2*bc, else k-means; then the
-    random centroid order, first-block merge and block reordering."""
+    random centroid order, first-block merge and block reordering.  With z
+    (a third coordinate: time or depth) every step is the reference's
+    time_flag variant."""
+    if z is not None:
+        return _build_layout3(x, y, z, obs, bc, cs, seed, epochs, threads)
     x, y, obs = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, obs))
     n = len(x)
     k = n if n < 2 * bc else bc
@@ -119,10 +138,33 @@ def build_layout(x, y, obs, bc: int, cs: int, seed: int = 0, epochs: int = 50,
                   cy[:b].copy(), None, fcc.value)
 
 
+def _build_layout3(x, y, z, obs, bc, cs, seed, epochs, threads) -> Layout:
+    x, y, z, obs = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, obs))
+    n = len(x)
+    k = n if n < 2 * bc else bc
+    bn = np.zeros(k, dtype=np.int32)
+    acc = np.zeros(k + 1, dtype=np.int32)
+    xn, yn, zn, on = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
+    cx, cy, cz = np.zeros(k), np.zeros(k), np.zeros(k)
+    bco = C.c_int(0)
+    fcc = C.c_int(0)
+    check(lib().bv_layout_build3(dp(x), dp(y), dp(z), dp(obs), n, int(bc), int(cs), int(seed),
+                                 int(epochs), int(threads), ip(bn), ip(acc), dp(xn), dp(yn), dp(zn),
+                                 dp(on), dp(cx), dp(cy), dp(cz), C.byref(bco), C.byref(fcc)))
+    b = bco.value
+    return Layout(bn[:b].copy(), acc[:b + 1].copy(), xn, yn, on, int(cs), cx[:b].copy(),
+                  cy[:b].copy(), None, fcc.value, z=zn, cz=cz[:b].copy())
+
+
 def knn(layout: Layout, device: int = 0) -> np.ndarray:
-    """Conditioning sets on the device (findNearestPoints semantics)."""
+    """Conditioning sets on the device (findNearestPoints semantics; the
+    time_flag key when the layout has a third coordinate)."""
     L = layout.normalized()
     out = np.zeros(L.bc * L.cs, dtype=np.int32)
+    if L.z is not None:
+        check(lib().bv_knn3(dp(L.x), dp(L.y), dp(L.z), L.n, L.bc, L.cs, ip(L.batchNumAccum),
+                            dp(L.cx), dp(L.cy), dp(L.cz), ip(out), int(device)))
+        return out
     check(lib().bv_knn(dp(L.x), dp(L.y), L.n, L.bc, L.cs, ip(L.batchNumAccum), dp(L.cx), dp(L.cy),
                        ip(out), int(device)))
     return out
@@ -166,11 +208,13 @@ class LlhData:
                                 dp(L.y), dp(L.obs),
                                 ip(L.knn_idx) if L.knn_idx is not None else null_i,
                                 dp(L.cx) if L.cx is not None else null_d,
-                                dp(L.cy) if L.cy is not None else null_d)
+                                dp(L.cy) if L.cy is not None else null_d,
+                                dp(L.z) if L.z is not None else null_d,
+                                dp(L.cz) if L.cz is not None else null_d)
         self._h = C.c_void_p()
         check(lib().bv_create(C.byref(self._l), C.byref(o), C.byref(self._h)))
         self.kernel = kernel
-        self.num_params = 4 if nugget else 3
+        self.num_params = (7 if kernel == 4 else 3) + (1 if nugget else 0)
 
     def close(self):
         if self._h:
@@ -194,8 +238,9 @@ class LlhData:
         return self._h
 
     def __call__(self, theta) -> float:
-        """theta = (sigma2, range, nu), plus tau^2 when the handle has a nugget."""
-        th = np.zeros(max(4, len(theta)))
+        """theta = (sigma2, range, nu) -- seven values for the space-time
+        kernel -- plus tau^2 when the handle has a nugget."""
+        th = np.zeros(max(8, len(theta)))
         th[:len(theta)] = np.asarray(theta, dtype=np.float64)
         out = C.c_double(0.0)
         check(lib().bv_llh_eval(self._h, dp(th), C.byref(out)))
@@ -203,7 +248,7 @@ class LlhData:
 
     def eval_host(self, obs, theta, x=None, y=None, knn_idx=None) -> float:
         """End-to-end evaluation from host buffers (copies in, evaluates)."""
-        th = np.zeros(max(4, len(theta)))
+        th = np.zeros(max(8, len(theta)))
         th[:len(theta)] = np.asarray(theta, dtype=np.float64)
         obs = np.ascontiguousarray(obs, dtype=np.float64)
         nd = C.POINTER(C.c_double)()

@@ -65,12 +65,24 @@ typedef struct {
                                   firstClusterCount - 1]); used if knn_idx
                                   is NULL                                    */
     const double *cy;
+    const double *z;           /* [n]    block-ordered third coordinate (the
+                                  reference's time_flag locations_new->z:
+                                  time for the space-time kernel, or depth
+                                  with --3D), NULL for 2-D                    */
+    const double *cz;          /* [bc]   third coordinate of the block
+                                  centroids, when z is set and knn_idx NULL  */
 } bv_layout;
 
 typedef struct {
     int precision;     /* BV_PREC_FP64 | BV_PREC_MIXED                        */
     int kernel;        /* 1,2,3: Matern (the reference's llh evaluates Matern
-                          for all three, include/llh_Xvecchia_batch.h:126-144) */
+                          for all three, include/llh_Xvecchia_batch.h:126-144);
+                          with a 3-D layout (z set) its distances include z
+                          (core_dcmg with z_flag = 1).  4: space-time Matern
+                          (core_dcmg_spacetime_matern, src/ckernel.cpp
+                          :1421-1458), theta = {sigma2, range_spatial,
+                          smooth_spatial, range_time, smooth_time,
+                          separability, aux}; needs a 3-D layout           */
     double dist_scale; /* --dist_scale, default 1.0                           */
     int device;        /* CUDA device ordinal                                 */
     int on_failure;    /* BV_FAIL_NEGINF | BV_FAIL_CONTINUE                   */
@@ -272,6 +284,12 @@ int bv_knn(const double *x, const double *y, int n, int bc, int cs,
            const int *batchNumAccum, const double *cx, const double *cy,
            int *knn_idx, int device);
 
+/* The same for 3-D locations (findNearestPoints with time_flag, the key
+ * sqrt(d^2 + dz^2) of include/nearest_neighbor.h:101-104). */
+int bv_knn3(const double *x, const double *y, const double *z, int n, int bc, int cs,
+            const int *batchNumAccum, const double *cx, const double *cy,
+            const double *cz, int *knn_idx, int device);
+
 /* ------------------------------------------------------- host layout */
 /* The driver's setup on the host (src/test_Xvecchia_batch.cpp:240-352):
  * classic Vecchia when n < 2*bc, else k-means (random_initializer + Lloyd
@@ -303,6 +321,21 @@ int bv_kmeans(const double *x, const double *y, int n, int k, int seed,
 /* GenerateXYLoc (src/ckernel.cpp:43-76): n jittered grid points, glibc
  * rand() seeded with `seed`, Morton-sorted and quantised to 1/65535. */
 int bv_generate_xy(int n, int seed, double *x, double *y);
+
+/* GenerateXYLoc_ST (src/ckernel.cpp:78-118): n jittered grid points (grid
+ * order) repeated over t_slots time slots, z = (slot + 1) / t_slots; the
+ * arrays hold n * t_slots entries. */
+int bv_generate_xyt(int n, int t_slots, int seed, double *x, double *y, double *z);
+
+/* bv_layout_build for 3-D locations (the reference's time_flag set-up:
+ * k-means on (x, y, z), random_reordering_3d, reorderIndex and
+ * cluster_to_batch with z).  z_new[n] and cz[nclusters] receive the
+ * block-ordered third coordinate and the block centroids' one. */
+int bv_layout_build3(const double *x, const double *y, const double *z,
+                     const double *obs, int n, int bc, int cs, int seed, int epochs,
+                     int threads, int *batchNum, int *batchNumAccum, double *x_new,
+                     double *y_new, double *z_new, double *obs_new, double *cx,
+                     double *cy, double *cz, int *bc_out, int *first_cluster_count);
 
 #ifdef __cplusplus
 }

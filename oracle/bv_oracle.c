@@ -513,6 +513,21 @@ typedef struct {
     bvo_dgemm_fn gemm;
 } bvo_la;
 
+/* Covariance generation of the problem's kernel: core_dcmg (2-D, or with
+ * z_flag = 1 when the problem has z) or core_dcmg_spacetime_matern
+ * (include/llh_Xvecchia_batch.h:126-144,179-207). */
+static void bvo_cov(const bvo_problem *p, const double *theta, double *A, int m, int n,
+                    const double *x1, const double *y1, const double *z1,
+                    const double *x2, const double *y2, const double *z2)
+{
+    if (!p->z)
+        bvo_matern(A, m, n, x1, y1, x2, y2, theta, p->dist_scale);
+    else if (p->spacetime)
+        bvo_matern_st(A, m, n, x1, y1, z1, x2, y2, z2, theta);
+    else
+        bvo_matern3(A, m, n, x1, y1, z1, x2, y2, z2, theta, p->dist_scale);
+}
+
 /* One block of llh_Xvecchia_batch (include/llh_Xvecchia_batch.h:117-478). */
 static void bvo_block(const bvo_problem *p, const double *theta, int i,
                       const bvo_la *la, double *work, bvo_block_result *r)
@@ -529,12 +544,14 @@ static void bvo_block(const bvo_problem *p, const double *theta, int i,
     double *mu = zc + cs;                       /* bs                   */
     double *xc = mu + bs;                       /* cs                   */
     double *yc = xc + cs;                       /* cs                   */
+    double *tc = yc + cs;                       /* cs (third coordinate) */
     const double *xb = p->x + off, *yb = p->y + off;
+    const double *tb = p->z ? p->z + off : NULL;
     r->info22 = 0;
     r->info11 = 0;
 
     /* :117-150  Sigma11 */
-    bvo_matern(S11, bs, bs, xb, yb, xb, yb, theta, p->dist_scale);
+    bvo_cov(p, theta, S11, bs, bs, xb, yb, tb, xb, yb, tb);
     /* The nugget extension (not in the reference): tau^2 on the diagonal. */
     if (p->nugget != 0.0)
         for (int j = 0; j < bs; ++j) S11[j + (size_t)j * bs] += p->nugget;
@@ -546,13 +563,14 @@ static void bvo_block(const bvo_problem *p, const double *theta, int i,
         for (int t = 0; t < cs; ++t) {
             xc[t] = p->x[ci[t]];
             yc[t] = p->y[ci[t]];
+            if (p->z) tc[t] = p->z[ci[t]];
             zc[t] = p->obs[ci[t]];
         }
         /* :196-207  Sigma22 (cs x cs, full), Sigma21 (cs x bs) */
-        bvo_matern(S22, cs, cs, xc, yc, xc, yc, theta, p->dist_scale);
+        bvo_cov(p, theta, S22, cs, cs, xc, yc, tc, xc, yc, tc);
         if (p->nugget != 0.0)
             for (int j = 0; j < cs; ++j) S22[j + (size_t)j * cs] += p->nugget;
-        bvo_matern(S21, cs, bs, xc, yc, xb, yb, theta, p->dist_scale);
+        bvo_cov(p, theta, S21, cs, bs, xc, yc, tc, xb, yb, tb);
         /* :295-299 potrf, :320-337 trsm x2, :352-378 gemm x2 */
         if (la) {
             r->info22 = la->potrf(102 /*col-major*/, 'L', cs, S22, cs);
@@ -608,7 +626,7 @@ static double bvo_llh_impl(const bvo_problem *p, const double *theta,
     for (int i = b0; i < b1; ++i)
         if (p->batchNum[i] > maxbs) maxbs = p->batchNum[i];
     size_t wsz = 2 * (size_t)maxbs * maxbs + (size_t)cs * cs +
-                 (size_t)cs * maxbs + 3 * (size_t)maxbs + 3 * (size_t)cs + 8;
+                 (size_t)cs * maxbs + 3 * (size_t)maxbs + 4 * (size_t)cs + 8;
     bvo_block_result *res = per_block;
     bvo_block_result *own = NULL;
     if (!res) {

@@ -101,6 +101,8 @@ typedef struct {
     double dist_scale;        /* --dist_scale, 1.0 by default               */
     double nugget;            /* tau^2 on the diagonal of Sigma11 and Sigma22;
                                  0 = the reference's likelihood (no nugget)  */
+    const double *z;          /* [n] third coordinate (time_flag), or NULL  */
+    int spacetime;            /* 1: core_dcmg_spacetime_matern, theta[7]     */
 } bvo_problem;
 
 /* Per-block result of the restated likelihood. */

@@ -47,7 +47,8 @@ class Problem(C.Structure):
     _fields_ = [("n", C.c_int), ("bc", C.c_int), ("cs", C.c_int),
                 ("batchNum", _I), ("batchNumAccum", _I),
                 ("x", _D), ("y", _D), ("obs", _D), ("knn_idx", _I),
-                ("dist_scale", C.c_double), ("nugget", C.c_double)]
+                ("dist_scale", C.c_double), ("nugget", C.c_double),
+                ("z", _D), ("spacetime", C.c_int)]
 
 
 _lib = None
@@ -243,7 +244,8 @@ def knn_all_fast(x, y, cs, batchNumAccum, cx, cy, threads=0):
 class OracleProblem:
     """Holds numpy arrays alive behind a bvo_problem."""
 
-    def __init__(self, batchNum, batchNumAccum, x, y, obs, knn_idx, cs, dist_scale=1.0, nugget=0.0):
+    def __init__(self, batchNum, batchNumAccum, x, y, obs, knn_idx, cs, dist_scale=1.0, nugget=0.0,
+                 z=None, spacetime=False):
         self.batchNum = np.ascontiguousarray(batchNum, dtype=np.int32)
         self.batchNumAccum = np.ascontiguousarray(batchNumAccum, dtype=np.int32)
         self.x = np.ascontiguousarray(x, dtype=np.float64)
@@ -255,6 +257,10 @@ class OracleProblem:
         self.p = Problem(len(self.x), self.bc, self.cs, _ip(self.batchNum), _ip(self.batchNumAccum),
                          _dp(self.x), _dp(self.y), _dp(self.obs), _ip(self.knn_idx), float(dist_scale),
                          float(nugget))
+        self.z = None if z is None else np.ascontiguousarray(z, dtype=np.float64)
+        if self.z is not None:
+            self.p.z = _dp(self.z)
+            self.p.spacetime = int(bool(spacetime))
 
 
 def llh(prob: OracleProblem, theta, threads: int = 0, per_block: bool = False):

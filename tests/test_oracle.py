@@ -205,3 +205,61 @@ def test_spacetime_and_3d_pins_against_reference(ref):
         c = rng.random(3)
         assert np.array_equal(ref.knn_block3_fast(xs, ys, zs, p, c[0], c[1], c[2], 30),
                               ref.ref_find_nearest3(xs, ys, zs, p, c[0], c[1], c[2], 30))
+
+
+@pytest.mark.parametrize("spacetime", [False, True])
+def test_llh_exact_3d_and_spacetime(oracle, spacetime):
+    """With a third coordinate (3-D Matern, or the space-time kernel), block
+    1 conditioning on all of block 0 gives the exact dense Gaussian density
+    of the same covariance."""
+    scipy_stats = pytest.importorskip("scipy.stats")
+    rng = np.random.default_rng(8)
+    cs, bs1 = 30, 12
+    n = cs + bs1
+    x, y = rng.random(n), rng.random(n)
+    z = np.floor(rng.random(n) * 4 + 1) / 4 if spacetime else rng.random(n)
+    obs = rng.standard_normal(n)
+    bn = np.array([cs, bs1], dtype=np.int32)
+    acc = np.array([0, cs, n], dtype=np.int32)
+    knn = np.concatenate([np.arange(cs), rng.permutation(cs)]).astype(np.int32)
+    P = oracle.OracleProblem(bn, acc, x, y, obs, knn, cs, z=z, spacetime=spacetime)
+    thetas = ([(1.0, 0.3, 0.5, 0.5, 0.9, 0.7, 0.0), (1.3, 0.2, 1.1, 0.3, 0.5, 0.4, 0.2)] if spacetime
+              else [(1.5, 0.3, 0.5), (1.0, 0.25, 0.8)])
+    for th in thetas:
+        S = (oracle.matern_st(x, y, z, x, y, z, th) if spacetime
+             else oracle.matern3(x, y, z, x, y, z, th))
+        exact = scipy_stats.multivariate_normal(mean=np.zeros(n), cov=S).logpdf(obs)
+        v = oracle.llh(P, th)
+        assert abs(v - exact) <= 1e-10 * abs(exact), (th, v, exact)
+
+
+def test_generate_xyt_and_3d_layout_pins(ref, bvlib):
+    """GenerateXYLoc_ST and the time_flag layout steps (k-means on (x, y, z),
+    random_reordering_3d, reorderIndex and cluster_to_batch with z) are
+    bit-identical to the reference's own code."""
+    import ctypes as C
+    for n, t, seed in [(400, 5, 0), (1000, 3, 7)]:
+        a = bvlib.generate_xyt(n, t, seed)
+        b = ref.ref_generate_xyt(n, t, seed)
+        assert all(np.array_equal(u, v) for u, v in zip(a, b))
+    x, y, z = bvlib.generate_xyt(600, 5, 0)
+    obs = np.random.default_rng(0).standard_normal(len(x))
+    n, k, cs = len(x), 150, 40
+    lab = np.zeros(n, np.int32)
+    cx, cy, cz = np.zeros(k), np.zeros(k), np.zeros(k)
+    r = ref.ref()
+    r.ref_kmeans3(ref._dp(x), ref._dp(y), ref._dp(z), n, k, 0, 10, 1, ref._ip(lab), ref._dp(cx),
+                  ref._dp(cy), ref._dp(cz))
+    L = bvlib.build_layout(x, y, obs, k, cs, seed=0, epochs=10, threads=1, z=z)
+    bn, acc = np.zeros(k + 1, np.int32), np.zeros(k + 2, np.int32)
+    xn, yn, zn, on = (np.zeros(n) for _ in range(4))
+    bcx, bcy, bcz = np.zeros(k), np.zeros(k), np.zeros(k)
+    fcc, fcs = C.c_int(), C.c_int()
+    bc = r.ref_layout_from_clusters3(
+        ref._dp(x), ref._dp(y), ref._dp(z), ref._dp(obs), n, k, ref._ip(lab), ref._dp(cx),
+        ref._dp(cy), ref._dp(cz), cs, ref._ip(bn), ref._ip(acc), ref._dp(xn), ref._dp(yn),
+        ref._dp(zn), ref._dp(on), ref._dp(bcx), ref._dp(bcy), ref._dp(bcz), C.byref(fcc),
+        C.byref(fcs))
+    assert bc == L.bc and np.array_equal(bn[:bc], L.batchNum)
+    for a, b in [(xn, L.x), (yn, L.y), (zn, L.z), (on, L.obs), (bcx[:bc], L.cx), (bcz[:bc], L.cz)]:
+        assert np.array_equal(a, b)
