@@ -23,6 +23,10 @@ BV_PREC_MIXED = 1
 BV_LARGE_AUTO = 0
 BV_LARGE_STREAMED = 1
 BV_LARGE_SLAB = 2
+BV_SCHED_AUTO = 0
+BV_SCHED_BUCKETED = 1
+BV_SCHED_PERSISTENT = 2
+BV_SCHED_STREAMED = 3
 BV_FAIL_NEGINF = 0
 BV_FAIL_CONTINUE = 1
 BV_ST_COND_FAIL = 1

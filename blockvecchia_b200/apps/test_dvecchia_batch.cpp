@@ -45,6 +45,10 @@ struct Opts {
     int kernel = 1, num_params = 3, num_loc = 2000;
     double sigma = 1.0, beta = 0.1, nu = 0.5, nugget = 0.0, dist_scale = 1.0;
     double sigma_init = 0.01, beta_init = 0.01, nu_init = 0.01, nugget_init = 0.01;
+    // space-time (include/vecchia_helper_data.h:293-302)
+    double beta_time = 2.2, nu_time = 0.5, sep = 0.5, aux = 0.0;
+    double beta_time_init = 0.01, nu_time_init = 0.01, sep_init = 0.01;
+    int time_flag = 0, t_slots = 0, use_nugget = 0;
     int knn = 1, seed = 0, perf = 0, vecchia_cs = 100, vecchia_bc = 200, maxiter = 1000;
     double tol = 1e-5, lower_bound = 0.01, upper_bound = 3.0;
     int omp_threads = 40, device = 0, precision = BV_PREC_FP64, print_opts = 0;
@@ -57,8 +61,12 @@ struct Opts {
     exit(1);
 }
 
-// "a:b:c[:d]" with "?" keeping the current value.
-void parse_theta(const char *s, double *a, double *b, double *c, double *d)
+// "a:b:c[:d[:e:f]]" with "?" keeping the current value
+// (include/vecchia_helper_data.h:533-577): the fourth value is the nugget,
+// and with six values the fourth to sixth are the space-time range,
+// smoothness and separability.
+void parse_theta(const char *s, double *a, double *b, double *c, double *d, double *bt, double *nt,
+                 double *sp)
 {
     std::vector<std::string> parts;
     std::stringstream ss(s);
@@ -67,6 +75,11 @@ void parse_theta(const char *s, double *a, double *b, double *c, double *d)
     double *dst[4] = {a, b, c, d};
     for (size_t i = 0; i < parts.size() && i < 4; ++i)
         if (parts[i] != "?") *dst[i] = atof(parts[i].c_str());
+    if (parts.size() == 6) {
+        double *st[3] = {bt, nt, sp};
+        for (size_t i = 3; i < 6; ++i)
+            if (parts[i] != "?") *st[i - 3] = atof(parts[i].c_str());
+    }
 }
 
 Opts parse(int argc, char **argv)
@@ -77,11 +90,14 @@ Opts parse(int argc, char **argv)
         const bool has = i + 1 < argc;
         auto next = [&]() -> const char * { return argv[++i]; };
         if (a == "--help" || a == "-h") {
-            printf("Usage: test_dvecchia_batch [--kernel K] [--ikernel s2:range:nu] [--kernel_init s2:range:nu]\n"
+            printf("Usage: test_dvecchia_batch [--kernel K] [--ikernel s2:range:nu[:nugget]] [--kernel_init ...]\n"
                    "  [--vecchia_cs N] [--vecchia_bc N] [--num_loc N] [--knn x] [--perf x] [--seed N]\n"
                    "  [--xy_path F] [--obs_path F] [--tol k (1e-k)] [--maxiter N] [--omp_threads N]\n"
                    "  [--permutation random] [--dist_scale d] [--lower_bound b] [--upper_bound b]\n"
-                   "  [--precision fp64|mixed] [--device N] [--print-opts]\n");
+                   "  [--t_slots N] [--3D x] [--use_nugget 0|1]\n"
+                   "  [--precision fp64|mixed] [--device N] [--print-opts]\n"
+                   "  space-time: --kernel univariate_matern_spacetime_stationary\n"
+                   "              --ikernel s2:range:nu:range_t:nu_t:sep\n");
             exit(0);
         } else if (a == "--xy_path" && has) {
             o.xy_path = next();
@@ -117,13 +133,18 @@ Opts parse(int argc, char **argv)
             } else if (k == "univariate_powexp_nugget_stationary") {
                 o.kernel = 3;
                 o.num_params = 4;
+            } else if (k == "univariate_matern_spacetime_stationary") {
+                o.kernel = 4;
+                o.num_params = 7;
+                o.time_flag = 1;
             } else {
                 die("unsupported kernel: ", k.c_str());
             }
         } else if (a == "--ikernel" && has) {
-            parse_theta(next(), &o.sigma, &o.beta, &o.nu, &o.nugget);
+            parse_theta(next(), &o.sigma, &o.beta, &o.nu, &o.nugget, &o.beta_time, &o.nu_time, &o.sep);
         } else if (a == "--kernel_init" && has) {
-            parse_theta(next(), &o.sigma_init, &o.beta_init, &o.nu_init, &o.nugget_init);
+            parse_theta(next(), &o.sigma_init, &o.beta_init, &o.nu_init, &o.nugget_init,
+                        &o.beta_time_init, &o.nu_time_init, &o.sep_init);
         } else if (a == "--seed" && has) {
             o.seed = atoi(next());
         } else if (a == "--omp_threads" && has) {
@@ -151,12 +172,26 @@ Opts parse(int argc, char **argv)
             o.device = atoi(next());
         } else if (a == "--print-opts") {
             o.print_opts = 1;
-        } else if (a == "--3D" || a == "--earth" || a == "--t_slots") {
-            die("not supported by this build (2-D Euclidean only): ", a.c_str());
+        } else if (a == "--t_slots" && has) {
+            o.t_slots = atoi(next());
+            if (o.t_slots < 0) die("--t_slots must be >= 0");
+        } else if (a == "--3D" && has) {
+            ++i;  // include/vecchia_helper_data.h:445-449: 3-D spatial locations
+            o.time_flag = 1;
+            o.t_slots = 0;
+        } else if (a == "--use_nugget" && has) {
+            // Not in the reference (its likelihood never reads the nugget):
+            // the nugget (fourth --ikernel value) enters the covariance.
+            o.use_nugget = atoi(next()) != 0;
+        } else if (a == "--earth") {
+            die("not supported by this build (Euclidean distances only): ", a.c_str());
         } else {
             die("unknown or incomplete option: ", a.c_str());
         }
     }
+    // src/test_Xvecchia_batch.cpp:107-111
+    if (o.time_flag && o.t_slots != 0 && o.num_loc % o.t_slots != 0)
+        die("Your number of locations cannot be divided by t_slot!");
     return o;
 }
 
@@ -167,20 +202,25 @@ void print_opts(const Opts &o)
            "\"vecchia_cs\": %d, \"vecchia_bc\": %d, \"knn\": %d, \"perf\": %d, \"seed\": %d, "
            "\"tol\": %.17g, \"maxiter\": %d, \"lower_bound\": %.17g, \"upper_bound\": %.17g, "
            "\"dist_scale\": %.17g, \"omp_threads\": %d, \"precision\": %d, \"xy_path\": \"%s\", "
-           "\"obs_path\": \"%s\"}\n",
+           "\"obs_path\": \"%s\", \"time_flag\": %d, \"t_slots\": %d, \"beta_time\": %.17g, "
+           "\"nu_time\": %.17g, \"sep\": %.17g, \"nugget\": %.17g, \"use_nugget\": %d}\n",
            o.kernel, o.num_params, o.num_loc, o.sigma, o.beta, o.nu, o.sigma_init, o.beta_init,
            o.nu_init, o.vecchia_cs, o.vecchia_bc, o.knn, o.perf, o.seed, o.tol, o.maxiter,
            o.lower_bound, o.upper_bound, o.dist_scale, o.omp_threads, o.precision,
-           o.xy_path.c_str(), o.obs_path.c_str());
+           o.xy_path.c_str(), o.obs_path.c_str(), o.time_flag, o.t_slots, o.beta_time, o.nu_time, o.sep,
+           o.nugget, o.use_nugget);
 }
 
-// include/utils.h:27-87: "x,y" per line; one observation per line.
-void load_xy(const std::string &path, int n, std::vector<double> &x, std::vector<double> &y)
+// include/utils.h:27-87: "x,y" per line ("x,y,z" with time_flag); one
+// observation per line.
+void load_xy(const std::string &path, int n, std::vector<double> &x, std::vector<double> &y,
+             std::vector<double> *z)
 {
     std::ifstream f(path);
     if (!f) die("cannot open ", path.c_str());
     x.assign(n, 0.0);
     y.assign(n, 0.0);
+    if (z) z->assign(n, 0.0);
     std::string line;
     int i = 0;
     while (i < n && std::getline(f, line)) {
@@ -190,6 +230,10 @@ void load_xy(const std::string &path, int n, std::vector<double> &x, std::vector
         x[i] = std::stod(t);
         if (!std::getline(ss, t, ',')) die("malformed line in ", path.c_str());
         y[i] = std::stod(t);
+        if (z) {
+            if (!std::getline(ss, t, ',')) die("missing third coordinate in ", path.c_str());
+            (*z)[i] = std::stod(t);
+        }
         ++i;
     }
     if (i < n) die("too few locations in ", path.c_str());
@@ -214,11 +258,11 @@ void load_obs(const std::string &path, int n, std::vector<double> &z)
 // the box.  Stops when every simplex vertex is within tol (relative) of the
 // best one in every coordinate, or after maxeval evaluations.
 double nelder_mead_max(double (*f)(unsigned, const double *, double *, void *), void *data, int d,
-                       std::vector<double> &x, double lb, double ub, double tol, int maxeval,
-                       int *evals)
+                       std::vector<double> &x, const std::vector<double> &lbv,
+                       const std::vector<double> &ubv, double tol, int maxeval, int *evals)
 {
     auto clip = [&](std::vector<double> &v) {
-        for (double &t : v) t = std::min(ub, std::max(lb, t));
+        for (int i = 0; i < d; ++i) v[i] = std::min(ubv[i], std::max(lbv[i], v[i]));
     };
     int ne = 0;
     auto F = [&](std::vector<double> &v) {
@@ -233,8 +277,8 @@ double nelder_mead_max(double (*f)(unsigned, const double *, double *, void *), 
     fv[0] = F(s[0]);
     for (int i = 0; i < d && ne < maxeval; ++i) {
         s[i + 1] = s[0];
-        double step = 0.1 * (ub - lb);
-        if (s[0][i] + step > ub) step = -step;
+        double step = 0.1 * (ubv[i] - lbv[i]);  // 0 for a fixed coordinate
+        if (s[0][i] + step > ubv[i]) step = -step;
         s[i + 1][i] += step;
         fv[i + 1] = F(s[i + 1]);
     }
@@ -311,39 +355,71 @@ int main(int argc, char **argv)
         return 0;
     }
     const int n = o.num_loc;
-    std::vector<double> x, y, z;
-    std::vector<double> theta(3);
+    const bool tf = o.time_flag != 0;
+    std::vector<double> x, y, t3, z;  // t3: third coordinate (time_flag), z: observations
+    // Parameter vector: the kernel's (3, or 7 for space-time), then the
+    // nugget when --use_nugget (src/test_Xvecchia_batch.cpp:156-235).
+    const int np = o.num_params == 7 ? 7 : 3;
+    const int d = np + (o.use_nugget ? 1 : 0);
+    std::vector<double> theta(d, 0.0);
+    auto fill = [&](double s2, double b, double nu, double nug, double bt, double nt, double sp, double ax) {
+        theta[0] = s2;
+        theta[1] = b;
+        theta[2] = nu;
+        if (np == 7) {
+            theta[3] = bt;
+            theta[4] = nt;
+            theta[5] = sp;
+            theta[6] = ax;
+        }
+        if (o.use_nugget) theta[np] = nug;
+    };
     if (o.perf) {
         x.resize(n);
         y.resize(n);
-        if (bv_generate_xy(n, o.seed, x.data(), y.data())) die(bv_last_error());
+        if (tf) {
+            if (o.t_slots <= 0) die("--perf with time_flag needs --t_slots > 0");
+            t3.resize(n);
+            if (bv_generate_xyt(n / o.t_slots, o.t_slots, o.seed, x.data(), y.data(), t3.data()))
+                die(bv_last_error());
+        } else if (bv_generate_xy(n, o.seed, x.data(), y.data())) {
+            die(bv_last_error());
+        }
         z.assign(n, 0.0);  // src/test_Xvecchia_batch.cpp:151-152
-        theta = {o.sigma, o.beta, o.nu};
+        fill(o.sigma, o.beta, o.nu, o.nugget, o.beta_time, o.nu_time, o.sep, o.aux);
     } else {
         if (o.xy_path.empty() || o.obs_path.empty())
             die("--xy_path and --obs_path are required unless --perf is given");
-        load_xy(o.xy_path, n, x, y);
+        load_xy(o.xy_path, n, x, y, tf ? &t3 : nullptr);
         load_obs(o.obs_path, n, z);
-        theta = {o.sigma_init, o.beta_init, o.nu_init};
+        // The auxiliary space-time parameter starts at 0 and is not optimised.
+        fill(o.sigma_init, o.beta_init, o.nu_init, o.nugget_init, o.beta_time_init, o.nu_time_init,
+             o.sep_init, 0.0);
     }
     fprintf(stderr, n < 2 * o.vecchia_bc ? "You are using the classic Vecchia!\n"
                                          : "You are using the cluster Vecchia!\n");
     const int k = (n < 2 * o.vecchia_bc) ? n : o.vecchia_bc;
     std::vector<int> bn(k), acc(k + 1);
-    std::vector<double> xn(n), yn(n), zn(n), cx(k), cy(k);
+    std::vector<double> xn(n), yn(n), zn(n), cx(k), cy(k), tn(tf ? n : 0), ct(tf ? k : 0);
     int bc = 0, fcc = 0;
-    if (bv_layout_build(x.data(), y.data(), z.data(), n, o.vecchia_bc, o.vecchia_cs, o.seed, 50,
-                        o.omp_threads, bn.data(), acc.data(), xn.data(), yn.data(), zn.data(),
-                        cx.data(), cy.data(), &bc, &fcc))
-        die(bv_last_error());
+    const int lrc = tf ? bv_layout_build3(x.data(), y.data(), t3.data(), z.data(), n, o.vecchia_bc,
+                                          o.vecchia_cs, o.seed, 50, o.omp_threads, bn.data(),
+                                          acc.data(), xn.data(), yn.data(), tn.data(), zn.data(),
+                                          cx.data(), cy.data(), ct.data(), &bc, &fcc)
+                       : bv_layout_build(x.data(), y.data(), z.data(), n, o.vecchia_bc, o.vecchia_cs,
+                                         o.seed, 50, o.omp_threads, bn.data(), acc.data(), xn.data(),
+                                         yn.data(), zn.data(), cx.data(), cy.data(), &bc, &fcc);
+    if (lrc) die(bv_last_error());
     fprintf(stderr, "--------------Clustering Done-----------------\n");
     const int cs = o.vecchia_cs;
     std::vector<int> knn((size_t)bc * cs);
     if (cs > 0) {
         if (o.knn) {
-            if (bv_knn(xn.data(), yn.data(), n, bc, cs, acc.data(), cx.data(), cy.data(), knn.data(),
-                       o.device))
-                die(bv_last_error());
+            const int krc = tf ? bv_knn3(xn.data(), yn.data(), tn.data(), n, bc, cs, acc.data(), cx.data(),
+                                         cy.data(), ct.data(), knn.data(), o.device)
+                               : bv_knn(xn.data(), yn.data(), n, bc, cs, acc.data(), cx.data(), cy.data(),
+                                        knn.data(), o.device);
+            if (krc) die(bv_last_error());
         } else {
             // src/test_Xvecchia_batch.cpp:391-404: the cs points before each block.
             for (int t = 0; t < cs; ++t) knn[t] = t;
@@ -371,10 +447,11 @@ int main(int argc, char **argv)
     }
     fprintf(stderr, "--------------Nearest Neighbor Done-----------------\n");
     bv_layout L = {n, bc, cs, bn.data(), acc.data(), xn.data(), yn.data(), zn.data(), knn.data(),
-                   cx.data(), cy.data()};
+                   cx.data(), cy.data(), tf ? tn.data() : nullptr, tf ? ct.data() : nullptr};
     bv_opts bo;
     bv_default_opts(&bo);
     bo.kernel = o.kernel;
+    bo.nugget = o.use_nugget;
     bo.dist_scale = o.dist_scale;
     bo.device = o.device;
     bo.precision = o.precision;
@@ -386,10 +463,19 @@ int main(int argc, char **argv)
     double maxf = -HUGE_VAL;
     int evals = 0;
     bool ok = true;
+    // Bounds (src/test_Xvecchia_batch.cpp:707-720): [lower, upper] for every
+    // parameter; the space-time kernel's time smoothness and separability
+    // are at most 1 and its auxiliary parameter is held at 0.
+    std::vector<double> lb(d, o.lower_bound), ub(d, o.upper_bound);
+    if (np == 7) {
+        ub[4] = 1.0;
+        ub[5] = 1.0;
+        lb[6] = 0.0;
+        ub[6] = 0.0;
+    }
 #ifdef BV_HAVE_NLOPT
-    nlopt_opt opt = nlopt_create(NLOPT_LN_BOBYQA, 3);
+    nlopt_opt opt = nlopt_create(NLOPT_LN_BOBYQA, d);
     nlopt_set_max_objective(opt, bv_llh, h);
-    std::vector<double> lb(3, o.lower_bound), ub(3, o.upper_bound);
     nlopt_set_lower_bounds(opt, lb.data());
     nlopt_set_upper_bounds(opt, ub.data());
     nlopt_set_xtol_rel(opt, o.tol);
@@ -398,28 +484,44 @@ int main(int argc, char **argv)
     nlopt_destroy(opt);
     evals = bv_iterations(h);
 #else
-    maxf = nelder_mead_max(bv_llh, h, 3, theta, o.lower_bound, o.upper_bound, o.tol, o.maxiter,
-                           &evals);
+    maxf = nelder_mead_max(bv_llh, h, d, theta, lb, ub, o.tol, o.maxiter, &evals);
 #endif
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    // src/test_Xvecchia_batch.cpp:733-753 and include/utils.h:155-190.
     if (!ok)
         printf("nlopt failed!\n");
+    else if (np == 7)
+        printf("Found maximum at f(%g, %g, %g, %g, %g, %g) = %0.10g\n", theta[0], theta[1], theta[2],
+               theta[3], theta[4], theta[5], maxf);
+    else if (d == 4)
+        printf("Found maximum at f(%g, %g, %g, %g) = %0.10g\n", theta[0], theta[1], theta[2], theta[3],
+               maxf);
     else
         printf("Found maximum at f(%g, %g, %g) = %0.10g\n", theta[0], theta[1], theta[2], maxf);
-    // include/utils.h:155-171 summary lines and ./log CSV.
     printf("Total Number of Iterations = %d \n", bv_iterations(h));
     printf("Total Optimization Time = %lf secs \n", secs);
-    printf("Model Parameters (Variance, range, smoothness): (%.8f, %.8f, %.8f) -> Loglik: %.18f \n",
-           theta[0], theta[1], theta[2], maxf);
     mkdir("./log", 0755);
     char path[512];
     snprintf(path, sizeof(path), "./log/locs_%d_cs_%d_bc_%d_seed_%d_kernel_%f:%f:%f_random", n, cs,
              o.vecchia_bc, o.seed, o.sigma, o.beta, o.nu);
-    std::ofstream out(path);
-    out << "Iterations, variance, range, smoothness, log-likelihood, time " << std::endl;
-    out << bv_iterations(h) << ", " << theta[0] << ", " << theta[1] << ", " << theta[2] << ", "
-        << std::setprecision(std::numeric_limits<double>::max_digits10) << maxf << ", " << secs
-        << std::endl;
+    if (np == 3 && d == 3) {
+        printf("Model Parameters (Variance, range, smoothness): (%.8f, %.8f, %.8f) -> Loglik: %.18f \n",
+               theta[0], theta[1], theta[2], maxf);
+        std::ofstream out(path);
+        out << "Iterations, variance, range, smoothness, log-likelihood, time " << std::endl;
+        out << bv_iterations(h) << ", " << theta[0] << ", " << theta[1] << ", " << theta[2] << ", "
+            << std::setprecision(std::numeric_limits<double>::max_digits10) << maxf << ", " << secs
+            << std::endl;
+    } else if (np == 3) {
+        printf("Model Parameters (Variance, range, smoothness, nugget): (%.8f, %.8f, %.8f, %.8f) -> "
+               "Loglik: %.18f \n",
+               theta[0], theta[1], theta[2], theta[3], maxf);
+        std::ofstream out(path);
+        out << "Iterations, variance, range, smoothness, nugget, log-likelihood, time " << std::endl;
+        out << bv_iterations(h) << ", " << theta[0] << ", " << theta[1] << ", " << theta[2] << ", "
+            << theta[3] << ", " << std::setprecision(std::numeric_limits<double>::max_digits10) << maxf
+            << ", " << secs << std::endl;
+    }
     bv_status st;
     bv_get_status(h, &st);
     if (st.cond_fail + st.schur_fail)

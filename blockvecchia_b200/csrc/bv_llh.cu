@@ -93,12 +93,15 @@ struct LeanVariant {
     void (*kernel)(LlhArgs);
     int threads, rc;
 };
+// 256 threads, 64-row chunks, two CTAs per SM: measured against 128-thread
+// CTAs (three per SM with 32-row chunks, two with 64) and 32-row chunks at
+// 256 threads on n = 200k, cs = 120 (5.00 ms against 5.09-5.46 ms) and at
+// the cs = 200 shape.
 static const LeanVariant kLeanVariants[] = {
     {llh_lean_kernel_t<256, 64, 2>, 256, 64},
-    {llh_lean_kernel_t<128, 32, 3>, 128, 32},
-    {llh_lean_kernel_t<256, 32, 2>, 256, 32},
-    {llh_lean_kernel_t<128, 64, 2>, 128, 64},
 };
+// Blocks up to this M run the multi-CTA streamed kernel by default.
+constexpr int kLeanMaxM = 160;
 
 static thread_local char g_err[1024] = "";
 
@@ -141,6 +144,8 @@ struct bv_handle {
     unsigned *d_counters = nullptr;  // one per launch
     double *d_slab = nullptr;
     size_t slab_stride = 0;
+    double *d_slab_lean = nullptr;  // per-CTA slabs of the multi-CTA streamed launch
+    int lean_max_m = 0;             // blocks with M <= this run the multi-CTA streamed kernel
     MaternParams *d_mp = nullptr;
     EvalResult *d_res = nullptr;
     MixedWork mixed;  // mixed-precision scratch (bv_llh_mixed.cuh)
@@ -157,6 +162,11 @@ struct bv_handle {
     int block_threads = kThreads;
     struct Launch {
         int begin, end, grid;
+        void (*kernel)(LlhArgs);
+        int threads;
+        size_t smem;
+        double *slab;
+        size_t slab_stride;
     };
     std::vector<Launch> launches;
     cudaStream_t stream = nullptr;
@@ -193,6 +203,7 @@ static void handle_free(bv_handle *h)
     cudaFree(h->d_block_status);
     cudaFree(h->d_counters);
     cudaFree(h->d_slab);
+    cudaFree(h->d_slab_lean);
     cudaFree(h->d_mp);
     cudaFree(h->d_res);
     mixed_free(h->mixed);
@@ -346,58 +357,72 @@ bool bv::use_big_path(const int *batchNum, int bc, int cs, int small_m, int big_
     return n_big > sm_count;
 }
 
-// Multi-CTA streamed schedule: every block on the lean kernel.
-static int plan_lean(bv_handle *h, const cudaDeviceProp &prop, int variant)
+// M of the block at position t of the processing order.
+static int order_m(const bv_handle *h, int t)
 {
-    const LeanVariant &v = kLeanVariants[variant];
+    const int b = h->order[t];
+    return h->batchNum[b] + (b == 0 ? 0 : h->cs);
+}
+
+// The multi-CTA streamed launch over order positions [begin, end), whose
+// largest block has M = max_m.
+static int plan_lean_launch(bv_handle *h, const cudaDeviceProp &prop, int begin, int end, int max_m)
+{
+    const LeanVariant &v = kLeanVariants[0];
     cudaFuncAttributes fa;
     BV_CUDA_TRY(cudaFuncGetAttributes(&fa, v.kernel));
     int optin = 0;
     BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-    const size_t avail = (size_t)optin - fa.sharedSizeBytes;
-    if ((size_t)big_layout(h->max_m, v.rc, h->nz).total > avail) {
-        set_error("plan: blocks of M = %d exceed the streamed schedule's shared memory", h->max_m);
+    const size_t smem = big_layout(max_m, v.rc, h->nz).total;
+    if (smem > (size_t)optin - fa.sharedSizeBytes) {
+        set_error("plan: blocks of M = %d exceed the streamed schedule's shared memory", max_m);
         return BV_E_TOOLARGE;
     }
-    h->kernel = v.kernel;
-    h->block_threads = v.threads;
-    h->smem_bytes = big_layout(h->max_m, v.rc, h->nz).total;
-    h->use_big = true;
-    BV_CUDA_TRY(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)h->smem_bytes));
+    BV_CUDA_TRY(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
-    BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.kernel, v.threads, h->smem_bytes));
+    BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.kernel, v.threads, smem));
     if (occ < 1) {
-        set_error("plan: streamed kernel cannot be resident (smem %zu B)", h->smem_bytes);
+        set_error("plan: streamed kernel cannot be resident (smem %zu B)", smem);
         return BV_E_TOOLARGE;
     }
-    h->grid = prop.multiProcessorCount * occ;
-    h->smem_max_m = 0;
-    h->big_max_m = h->max_m;
-    h->slab_stride = (big_slab_doubles(h->max_m) + 31) & ~(size_t)31;
-    const size_t bytes = h->slab_stride * sizeof(double) * (size_t)h->grid;
-    if (cudaMalloc(&h->d_slab, bytes) != cudaSuccess) {
+    const int grid = std::min(prop.multiProcessorCount * occ, end - begin);
+    const size_t stride = (big_slab_doubles(max_m) + 31) & ~(size_t)31;
+    const size_t bytes = stride * sizeof(double) * (size_t)grid;
+    if (cudaMalloc(&h->d_slab_lean, bytes) != cudaSuccess) {
         cudaGetLastError();
         set_error("plan: cannot allocate %zu B of block slabs", bytes);
         return BV_E_NOMEM;
     }
-    h->launches.clear();
-    if (h->owned > 0) h->launches.push_back({0, h->owned, h->grid});
-    BV_CUDA_TRY(cudaMalloc(&h->d_counters, sizeof(unsigned)));
+    h->launches.push_back({begin, end, grid, v.kernel, v.threads, smem, h->d_slab_lean, stride});
     return BV_OK;
 }
 
+// Which kernel evaluates which blocks.  Blocks are in the processing order
+// (largest first).  Under the default schedule the blocks with M <=
+// kLeanMaxM run the multi-CTA streamed kernel (several blocks per SM, so
+// their pivot chains overlap), the larger ones the persistent one-CTA-per-SM
+// kernel; the split depends on the layout only, so every shard and every
+// evaluation make the same choice.
 static int plan_launches(bv_handle *h)
 {
     cudaDeviceProp prop;
     BV_CUDA_TRY(cudaGetDeviceProperties(&prop, h->device));
-    if (h->opts.schedule >= 2) return plan_lean(h, prop, h->opts.schedule - 2);
     size_t avail = 0;
     int cap_m = 0;
     {
         const int rc = fp64_limits(h->device, &avail, &cap_m, &h->big_max_m, h->nz);
         if (rc) return rc;
     }
+    const int sched = h->opts.schedule;
+    if (sched == BV_SCHED_STREAMED)
+        h->lean_max_m = h->max_m;
+    else if (sched == BV_SCHED_AUTO && h->opts.precision == BV_PREC_FP64)
+        h->lean_max_m = kLeanMaxM;
+    else
+        h->lean_max_m = 0;
+    int split = 0;  // order positions [split, owned) take the streamed kernel
+    while (split < h->owned && order_m(h, split) > h->lean_max_m) ++split;
+    h->launches.clear();
     h->smem_max_m = std::min(cap_m, h->max_m);
     // The cap is per kernel, not per handle: set it to what the device allows
     // so that handles with different block sizes can coexist.
@@ -426,6 +451,7 @@ static int plan_launches(bv_handle *h)
         return BV_E_TOOLARGE;
     }
     h->grid = prop.multiProcessorCount * occ;
+    h->block_threads = kThreads;
     if (h->slab_stride > 0) {
         const size_t bytes = h->slab_stride * sizeof(double) * (size_t)h->grid;
         if (cudaMalloc(&h->d_slab, bytes) != cudaSuccess) {
@@ -434,24 +460,25 @@ static int plan_launches(bv_handle *h)
             return BV_E_NOMEM;
         }
     }
-    h->launches.clear();
-    if (h->opts.schedule == 0) {
-        if (h->owned > 0) h->launches.push_back({0, h->owned, h->grid});
+    if (sched != BV_SCHED_BUCKETED) {
+        if (split > 0)
+            h->launches.push_back({0, split, h->grid, h->kernel, kThreads, h->smem_bytes, h->d_slab,
+                                   h->slab_stride});
     } else {
         // One launch per size bucket of M (width 8), largest first.
         int b = 0;
-        while (b < h->owned) {
-            const int mb = h->batchNum[h->order[b]] + (h->order[b] == 0 ? 0 : h->cs);
-            const int bucket = mb / 8;
+        while (b < split) {
+            const int bucket = order_m(h, b) / 8;
             int e = b;
-            while (e < h->owned) {
-                const int me = h->batchNum[h->order[e]] + (h->order[e] == 0 ? 0 : h->cs);
-                if (me / 8 != bucket) break;
-                ++e;
-            }
-            h->launches.push_back({b, e, std::min(h->grid, e - b)});
+            while (e < split && order_m(h, e) / 8 == bucket) ++e;
+            h->launches.push_back({b, e, std::min(h->grid, e - b), h->kernel, kThreads, h->smem_bytes,
+                                   h->d_slab, h->slab_stride});
             b = e;
         }
+    }
+    if (split < h->owned) {
+        const int rc = plan_lean_launch(h, prop, split, h->owned, order_m(h, split));
+        if (rc) return rc;
     }
     BV_CUDA_TRY(cudaMalloc(&h->d_counters, sizeof(unsigned) * std::max<size_t>(1, h->launches.size())));
     return BV_OK;
@@ -527,8 +554,11 @@ static int enqueue_eval(bv_handle *h, cudaStream_t s)
         }
     } else {
         for (size_t l = 0; l < h->launches.size(); ++l) {
-            LlhArgs a = fp64_args(h->d_counters + l, h->d_order, h->launches[l].begin, h->launches[l].end);
-            h->kernel<<<h->launches[l].grid, h->block_threads, h->smem_bytes, s>>>(a);
+            const bv_handle::Launch &ln = h->launches[l];
+            LlhArgs a = fp64_args(h->d_counters + l, h->d_order, ln.begin, ln.end);
+            a.gslab = ln.slab;
+            a.gslab_stride = ln.slab_stride;
+            ln.kernel<<<ln.grid, ln.threads, ln.smem, s>>>(a);
             BV_CUDA_TRY(cudaGetLastError());
         }
     }
@@ -610,7 +640,7 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
         h->max_m = std::max(h->max_m, h->batchNum[b] + (b == 0 ? 0 : h->cs));
     // Largest blocks first (longest-processing-time order), ties by index;
     // with sharding, every shard_count-th block of that order.
-    if (h->opts.schedule < 0 || h->opts.schedule >= 2 + (int)(sizeof(kLeanVariants) / sizeof(kLeanVariants[0]))) {
+    if (h->opts.schedule < BV_SCHED_AUTO || h->opts.schedule > BV_SCHED_STREAMED) {
         set_error("bv_create: unknown schedule %d", h->opts.schedule);
         handle_free(h);
         return BV_E_INVALID;

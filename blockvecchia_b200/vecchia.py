@@ -172,7 +172,7 @@ def knn(layout: Layout, device: int = 0) -> np.ndarray:
 
 _PREC = {"fp64": _lib.BV_PREC_FP64, "mixed": _lib.BV_PREC_MIXED}
 _FAIL = {"neginf": _lib.BV_FAIL_NEGINF, "continue": _lib.BV_FAIL_CONTINUE}
-_SCHED = {"persistent": 0, "bucketed": 1, "lean0": 2, "lean1": 3, "lean2": 4, "lean3": 5}
+_SCHED = {"auto": 0, "bucketed": 1, "persistent": 2, "streamed": 3}
 _LARGE = {"auto": _lib.BV_LARGE_AUTO, "streamed": _lib.BV_LARGE_STREAMED, "slab": _lib.BV_LARGE_SLAB}
 
 
@@ -182,7 +182,7 @@ class LlhData:
 
     def __init__(self, layout: Layout, precision: str = "fp64", kernel: int = 1,
                  dist_scale: float = 1.0, device: int = 0, on_failure: str = "neginf",
-                 print_iter: bool = False, use_graph: bool = True, schedule: str = "persistent",
+                 print_iter: bool = False, use_graph: bool = True, schedule: str = "auto",
                  mixed_tol: float = 1e-8, shard_count: int = 1, shard_index: int = 0,
                  large_blocks: str = "auto", nugget: bool = False):
         L = layout.normalized()

@@ -32,6 +32,10 @@ extern "C" {
 #define BV_LARGE_AUTO 0     /* large-block path choice (bv_opts.large_blocks) */
 #define BV_LARGE_STREAMED 1 /* left-looking, panels streamed through L2      */
 #define BV_LARGE_SLAB 2     /* shared-memory algorithm on a global slab      */
+#define BV_SCHED_AUTO 0
+#define BV_SCHED_BUCKETED 1
+#define BV_SCHED_PERSISTENT 2
+#define BV_SCHED_STREAMED 3
 #define BV_FAIL_NEGINF 0   /* a failed block makes bv_llh return -HUGE_VAL  */
 #define BV_FAIL_CONTINUE 1 /* keep going like the reference: a non-positive
                               pivot is skipped in the log-determinant        */
@@ -88,8 +92,17 @@ typedef struct {
     int on_failure;    /* BV_FAIL_NEGINF | BV_FAIL_CONTINUE                   */
     int print_iter;    /* print the reference's per-evaluation line           */
     int use_graph;     /* capture one evaluation in a CUDA graph (default 1)  */
-    int schedule;      /* 0 persistent work queue (default), 1 one launch per
-                          size bucket (the comparison baseline)               */
+    int schedule;      /* BV_SCHED_AUTO (default): blocks up to a size limit
+                          (M = cs + bs <= 160) on the multi-CTA streamed
+                          kernel, the larger ones on the persistent
+                          one-CTA-per-SM kernel; BV_SCHED_BUCKETED: the
+                          persistent kernel, one launch per size bucket (the
+                          comparison baseline); BV_SCHED_PERSISTENT: the
+                          persistent kernel for every block;
+                          BV_SCHED_STREAMED: the multi-CTA streamed kernel
+                          for every block.  The two kernels round
+                          differently; each choice depends on the layout
+                          only, so results are reproducible.                 */
     double mixed_tol;  /* mixed path: a block is accepted when the estimated
                           relative error of its refined Sigma22^-1 Sigma21
                           (|dX_last| / |X| times the first step's

@@ -51,7 +51,21 @@ def test_question_mark_keeps_value(exe):
 
 
 @pytest.mark.parametrize("bad", [["--tol", "0"], ["--maxiter", "-3"], ["--upper_bound", "200"],
-                                 ["--permutation", "kdtree"], ["--3D", "1"], ["--kernel", "foo"]])
+                                 ["--permutation", "kdtree"], ["--earth", "1"], ["--kernel", "foo"],
+                                 ["--kernel", "univariate_matern_spacetime_stationary", "--t_slots", "3",
+                                  "--num_loc", "1000", "--perf", "1"]])
 def test_rejected(exe, bad):
     r = subprocess.run([exe, *bad, "--print-opts"], capture_output=True, text=True, timeout=60)
     assert r.returncode != 0 and "error" in r.stderr
+
+
+def test_spacetime_flags(exe):
+    """The space-time kernel's flags (include/vecchia_helper_data.h:505-577):
+    seven parameters, six given by --ikernel (aux stays 0), time slots."""
+    o = _opts(exe, "--kernel", "univariate_matern_spacetime_stationary", "--ikernel",
+              "1.2:0.1:0.5:0.4:0.8:0.6", "--t_slots", "10", "--num_loc", "5000")
+    assert o["kernel"] == 4 and o["num_params"] == 7 and o["time_flag"] == 1 and o["t_slots"] == 10
+    assert (o["sigma"], o["beta"], o["nu"], o["beta_time"], o["nu_time"], o["sep"]) == \
+        (1.2, 0.1, 0.5, 0.4, 0.8, 0.6)
+    o = _opts(exe, "--3D", "1")
+    assert o["time_flag"] == 1 and o["t_slots"] == 0

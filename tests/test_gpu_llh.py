@@ -28,16 +28,19 @@ def _blocks(oracle, L, th):
     return v, per
 
 
-def _check(bv, oracle, L, thetas=THETAS, **kw):
-    with bv.LlhData(L, **kw) as D:
-        for th in thetas:
-            v = D(th)
-            ref, per = _blocks(oracle, L, th)
-            assert abs(v - ref) <= REL * abs(ref), (th, v, ref)
-            bl = D.block_llk()
-            assert np.all(np.abs(bl - per) <= 1e-7 * np.maximum(1.0, np.abs(per))), th
-            st = D.status()
-            assert st["cond_fail"] == 0 and st["schur_fail"] == 0
+def _check(bv, oracle, L, thetas=THETAS, schedules=("auto", "persistent"), **kw):
+    """Both kernels: the default schedule (blocks with M <= 160 on the
+    multi-CTA streamed kernel) and the persistent kernel for every block."""
+    for sched in schedules:
+        with bv.LlhData(L, schedule=sched, **kw) as D:
+            for th in thetas:
+                v = D(th)
+                ref, per = _blocks(oracle, L, th)
+                assert abs(v - ref) <= REL * abs(ref), (sched, th, v, ref)
+                bl = D.block_llk()
+                assert np.all(np.abs(bl - per) <= 1e-7 * np.maximum(1.0, np.abs(per))), (sched, th)
+                st = D.status()
+                assert st["cond_fail"] == 0 and st["schur_fail"] == 0
 
 
 def test_golden_layout(bvlib, oracle, golden_layout):
@@ -107,16 +110,25 @@ def test_edge_blocks(bvlib, oracle):
 
 
 def test_graph_schedule_and_determinism(bvlib, golden_layout):
-    """Graph vs stream launch, persistent vs per-bucket launches: identical bits."""
+    """Graph vs stream launch, persistent vs per-bucket launches, the
+    multi-CTA streamed kernel for all blocks vs the default routing (every
+    block here is small enough for it): identical bits within each kernel;
+    the two kernels agree within the parity bound."""
     L = _layout(bvlib, golden_layout)
     th = (1.0, 0.08, 1.5)
-    vals = []
-    for kw in [dict(), dict(use_graph=False), dict(schedule="bucketed")]:
+    vals = {}
+    for name, kw in [("auto", dict()), ("auto_nograph", dict(use_graph=False)),
+                     ("streamed", dict(schedule="streamed")),
+                     ("persistent", dict(schedule="persistent")),
+                     ("persistent_nograph", dict(schedule="persistent", use_graph=False)),
+                     ("bucketed", dict(schedule="bucketed"))]:
         with bvlib.LlhData(L, **kw) as D:
             a, b = D(th), D(th)
             assert a == b
-            vals.append(a)
-    assert vals[0] == vals[1] == vals[2]
+            vals[name] = a
+    assert vals["auto"] == vals["auto_nograph"] == vals["streamed"]
+    assert vals["persistent"] == vals["persistent_nograph"] == vals["bucketed"]
+    assert abs(vals["auto"] - vals["persistent"]) <= REL * abs(vals["persistent"])
 
 
 def test_shards_sum_to_total(bvlib, golden_layout):
@@ -306,7 +318,7 @@ def test_nugget_served_and_mixed(bvlib):
     path with a nugget stays within its 1e-8 accuracy bound."""
     L = _gen(bvlib, 3000, 200, 100)
     th = (1.0, 0.1, 0.5, 0.05)
-    with bvlib.LlhData(L, nugget=True) as D:
+    with bvlib.LlhData(L, nugget=True, schedule="persistent") as D:
         v = D(th)
     with bvlib.Server() as srv:
         j = srv.open_job(L, nugget=True)

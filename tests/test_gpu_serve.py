@@ -1,7 +1,8 @@
 """Continuous-batching server (bv_server_*): each request's result equals the
-single-job evaluation of the same layout bit for bit, whether the job runs
-alone or mixed with other jobs; HBM admission holds jobs back until they fit;
-and the oracle agrees with the served results to the FP64 parity bound."""
+single-job evaluation of the same layout on the persistent kernel (the
+server's per-block algorithm) bit for bit, whether the job runs alone or
+mixed with other jobs; HBM admission holds jobs back until they fit; and the
+oracle agrees with the served results to the FP64 parity bound."""
 import threading
 
 import numpy as np
@@ -28,7 +29,7 @@ def jobs(bvlib):
     Ls = [_gen(bvlib, *s) for s in specs]
     alone = []
     for L in Ls:
-        with bvlib.LlhData(L) as D:
+        with bvlib.LlhData(L, schedule="persistent") as D:
             alone.append([D(th) for th in THETAS])
     return Ls, alone
 
