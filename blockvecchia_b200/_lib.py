@@ -51,6 +51,8 @@ EXPORTS = {
     "bv_last_error": (C.c_char_p, []),
     "bv_llh_host": (C.c_int, [C.c_void_p, _D, _D, _D, _I, _D, _D]),
     "bv_knn": (C.c_int, [_D, _D, C.c_int, C.c_int, C.c_int, _I, _D, _D, _I, C.c_int]),
+    "bv_knn_subset": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, C.c_int, _I, _D, _D, _D,
+                                C.POINTER(C.c_ubyte), _I, C.c_int]),
     "bv_knn3": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, C.c_int, _I, _D, _D, _D, _I, C.c_int]),
     "bv_layout_build": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                   _I, _I, _D, _D, _D, _D, _D, _I, _I]),

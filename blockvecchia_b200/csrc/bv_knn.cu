@@ -61,6 +61,8 @@ struct KnnArgs {
     int *error;  // first failing block + 1, or 0
     int *heavy;  // blocks whose ties overflow the buffer, for knn_heavy_kernel
     unsigned *heavy_count;
+    const int *list;  // blocks to select for (largest prefix first), or nullptr: all
+    int nlist;
 };
 
 // The argument of the key's final square root for candidate p.
@@ -188,8 +190,14 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
         if (lane == 0) task = atomicAdd(a.counter, 1u);
         task = __shfl_sync(0xffffffffu, task, 0);
         // Largest prefixes first; block 0 is handled by the host (points 0..cs-1).
-        const int i = a.bc - 1 - (int)task;
-        if (i < 1) break;
+        int i;
+        if (a.list) {
+            if ((int)task >= a.nlist) break;
+            i = a.list[task];
+        } else {
+            i = a.bc - 1 - (int)task;
+            if (i < 1) break;
+        }
         const int P = a.acc[i];
         const double cx = a.cx[i], cy = a.cy[i], cz = a.z ? a.cz[i] : 0.0;
         int *out = a.out + (size_t)i * k;
@@ -453,7 +461,7 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
 
 int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, int bc, int cs,
                const int *d_acc, const double *cx, const double *cy, const double *cz, int *d_knn,
-               cudaStream_t s)
+               cudaStream_t s, const unsigned char *mask)
 {
     if (d_z && !cz) {
         set_error("bv_knn: 3-D locations need the centroids' third coordinate");
@@ -479,8 +487,14 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
         fail(e, "cudaMalloc");
         return rc;
     }
-    // counter, error, heavy_count, then the heavy list (bc entries)
-    if ((e = cudaMalloc(&d_counter, sizeof(unsigned) * 3 + sizeof(int) * (size_t)bc)) != cudaSuccess) {
+    // Blocks 1..bc-1 to select for, largest prefix first (all, or the mask's).
+    std::vector<int> list;
+    if (mask) {
+        for (int b = bc - 1; b >= 1; --b)
+            if (mask[b]) list.push_back(b);
+    }
+    // counter, error, heavy_count, the heavy list (bc entries), the block list
+    if ((e = cudaMalloc(&d_counter, sizeof(unsigned) * 3 + sizeof(int) * (size_t)bc * 2)) != cudaSuccess) {
         cudaFree(d_c);
         fail(e, "cudaMalloc");
         return rc;
@@ -488,6 +502,7 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
     d_err = reinterpret_cast<int *>(d_counter + 1);
     unsigned *d_heavy_count = d_counter + 2;
     int *d_heavy = reinterpret_cast<int *>(d_counter + 3);
+    int *d_list = d_heavy + bc;
     KnnHeavyScratch sc{nullptr, nullptr, nullptr};
     do {
         if ((e = cudaMemcpyAsync(d_c, cx, sizeof(double) * bc, cudaMemcpyHostToDevice, s)) ||
@@ -495,7 +510,9 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
             (d_z && (e = cudaMemcpyAsync(d_c + 2 * (size_t)bc, cz, sizeof(double) * bc,
                                          cudaMemcpyHostToDevice, s))) ||
             (e = cudaMemcpyAsync(d_knn, first.data(), sizeof(int) * cs, cudaMemcpyHostToDevice, s)) ||
-            (e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned) * 3, s))) {
+            (e = cudaMemsetAsync(d_counter, 0, sizeof(unsigned) * 3, s)) ||
+            (!list.empty() && (e = cudaMemcpyAsync(d_list, list.data(), sizeof(int) * list.size(),
+                                                   cudaMemcpyHostToDevice, s)))) {
             fail(e, "copy");
             break;
         }
@@ -514,6 +531,8 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
         ka.error = d_err;
         ka.heavy = d_heavy;
         ka.heavy_count = d_heavy_count;
+        ka.list = mask ? d_list : nullptr;
+        ka.nlist = (int)list.size();
         const size_t smem = sizeof(KnnWarpSmem) * kKnnWarps;
         if ((e = cudaFuncSetAttribute(knn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem))) {
@@ -526,7 +545,8 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, knn_kernel, kKnnWarps * 32, smem);
         if (occ < 1) occ = 1;
         int grid = sms * occ;
-        const int need = (bc + kKnnWarps - 1) / kKnnWarps;
+        const int nsel = mask ? (int)list.size() : bc;
+        const int need = (nsel + kKnnWarps - 1) / kKnnWarps;
         if (grid > need) grid = need > 0 ? need : 1;
         knn_kernel<<<grid, kKnnWarps * 32, smem, s>>>(ka);
         if ((e = cudaGetLastError())) {
@@ -577,7 +597,7 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
 
 static int knn_host(const double *x, const double *y, const double *z, int n, int bc, int cs,
                     const int *batchNumAccum, const double *cx, const double *cy, const double *cz,
-                    int *knn_idx, int device)
+                    int *knn_idx, int device, const unsigned char *mask = nullptr)
 {
     using namespace bv;
     if (!x || !y || !batchNumAccum || !cx || !cy || !knn_idx || n <= 0 || bc <= 0 || cs < 0 ||
@@ -619,10 +639,27 @@ static int knn_host(const double *x, const double *y, const double *z, int n, in
             rc = BV_E_CUDA;
             break;
         }
-        rc = knn_device(d_x, d_y, d_z, n, bc, cs, d_acc, cx, cy, cz, d_knn, s);
+        rc = knn_device(d_x, d_y, d_z, n, bc, cs, d_acc, cx, cy, cz, d_knn, s, mask);
         if (rc) break;
-        if ((e = cudaMemcpyAsync(knn_idx, d_knn, sizeof(int) * (size_t)bc * cs, cudaMemcpyDeviceToHost, s)) ||
-            (e = cudaStreamSynchronize(s))) {
+        // Block 0 and the selected blocks' sets back to the caller (the
+        // others' entries stay as the caller had them).
+        for (int b = 0; b < bc; ++b) {
+            if (mask && b > 0 && !mask[b]) continue;
+            int e0 = b, e1 = b + 1;
+            if (!mask)
+                e1 = bc;
+            else
+                while (e1 < bc && mask[e1]) ++e1;
+            if ((e = cudaMemcpyAsync(knn_idx + (size_t)e0 * cs, d_knn + (size_t)e0 * cs,
+                                     sizeof(int) * (size_t)(e1 - e0) * cs, cudaMemcpyDeviceToHost, s))) {
+                set_error("bv_knn: copy back: %s", cudaGetErrorString(e));
+                rc = BV_E_CUDA;
+                break;
+            }
+            b = e1 - 1;
+        }
+        if (rc) break;
+        if ((e = cudaStreamSynchronize(s))) {
             set_error("bv_knn: copy back: %s", cudaGetErrorString(e));
             rc = BV_E_CUDA;
         }
@@ -641,6 +678,17 @@ extern "C" int bv_knn(const double *x, const double *y, int n, int bc, int cs,
                       int device)
 {
     return knn_host(x, y, nullptr, n, bc, cs, batchNumAccum, cx, cy, nullptr, knn_idx, device);
+}
+
+extern "C" int bv_knn_subset(const double *x, const double *y, const double *z, int n, int bc,
+                             int cs, const int *batchNumAccum, const double *cx, const double *cy,
+                             const double *cz, const unsigned char *mask, int *knn_idx, int device)
+{
+    if (!mask) {
+        bv::set_error("bv_knn_subset: mask is required");
+        return BV_E_INVALID;
+    }
+    return knn_host(x, y, z, n, bc, cs, batchNumAccum, cx, cy, cz, knn_idx, device, mask);
 }
 
 extern "C" int bv_knn3(const double *x, const double *y, const double *z, int n, int bc, int cs,

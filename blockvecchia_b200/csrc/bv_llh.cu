@@ -697,8 +697,16 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
         if (L->knn_idx) {
             BV_CUDA_H(cudaMemcpy(h->d_knn, L->knn_idx, bc * cs * sizeof(int), cudaMemcpyHostToDevice));
         } else {
+            // A shard selects only its own blocks' sets (the others are
+            // never read by this handle).
+            std::vector<unsigned char> mine;
+            if (h->opts.shard_count > 1) {
+                mine.assign(h->bc, 0);
+                for (int t = 0; t < h->owned; ++t) mine[h->order[t]] = 1;
+                BV_CUDA_H(cudaMemsetAsync(h->d_knn, 0, bc * cs * sizeof(int), h->stream));
+            }
             BV_TRY_H(knn_device(h->d_x, h->d_y, h->d_z, h->n, h->bc, h->cs, h->d_acc, L->cx, L->cy,
-                                L->cz, h->d_knn, h->stream));
+                                L->cz, h->d_knn, h->stream, mine.empty() ? nullptr : mine.data()));
             BV_CUDA_H(cudaStreamSynchronize(h->stream));
         }
     }

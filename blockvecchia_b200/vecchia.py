@@ -156,11 +156,21 @@ def _build_layout3(x, y, z, obs, bc, cs, seed, epochs, threads) -> Layout:
                   cy[:b].copy(), None, fcc.value, z=zn, cz=cz[:b].copy())
 
 
-def knn(layout: Layout, device: int = 0) -> np.ndarray:
+def knn(layout: Layout, device: int = 0, mask=None) -> np.ndarray:
     """Conditioning sets on the device (findNearestPoints semantics; the
-    time_flag key when the layout has a third coordinate)."""
+    time_flag key when the layout has a third coordinate).  mask (bool per
+    block, e.g. shard_blocks): only those blocks' sets are selected; the
+    other entries are zero."""
     L = layout.normalized()
     out = np.zeros(L.bc * L.cs, dtype=np.int32)
+    if mask is not None:
+        m = np.ascontiguousarray(np.asarray(mask, dtype=bool).astype(np.uint8))
+        nd = C.POINTER(C.c_double)()
+        check(lib().bv_knn_subset(dp(L.x), dp(L.y), dp(L.z) if L.z is not None else nd, L.n, L.bc,
+                                  L.cs, ip(L.batchNumAccum), dp(L.cx), dp(L.cy),
+                                  dp(L.cz) if L.cz is not None else nd,
+                                  m.ctypes.data_as(C.POINTER(C.c_ubyte)), ip(out), int(device)))
+        return out
     if L.z is not None:
         check(lib().bv_knn3(dp(L.x), dp(L.y), dp(L.z), L.n, L.bc, L.cs, ip(L.batchNumAccum),
                             dp(L.cx), dp(L.cy), dp(L.cz), ip(out), int(device)))

@@ -303,6 +303,16 @@ int bv_knn3(const double *x, const double *y, const double *z, int n, int bc, in
             const int *batchNumAccum, const double *cx, const double *cy,
             const double *cz, int *knn_idx, int device);
 
+/* Conditioning sets of a subset of the blocks (one rank's shard, mask from
+ * bv_shard_blocks): blocks b >= 1 with mask[b] != 0 get their sets (and
+ * block 0 its points 0..cs-1); the other entries of knn_idx are left as
+ * they were.  z / cz may be NULL (2-D).  Each rank of a multi-GPU run
+ * selects only its own blocks' sets (the reference selects all on one host,
+ * src/test_Xvecchia_batch.cpp:368-390). */
+int bv_knn_subset(const double *x, const double *y, const double *z, int n, int bc,
+                  int cs, const int *batchNumAccum, const double *cx, const double *cy,
+                  const double *cz, const unsigned char *mask, int *knn_idx, int device);
+
 /* ------------------------------------------------------- host layout */
 /* The driver's setup on the host (src/test_Xvecchia_batch.cpp:240-352):
  * classic Vecchia when n < 2*bc, else k-means (random_initializer + Lloyd

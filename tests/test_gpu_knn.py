@@ -81,3 +81,28 @@ def test_ties_beyond_the_warp_buffer(bvlib, oracle):
     ref = oracle.knn_all(L.x, L.y, cs, L.batchNumAccum, L.cx, L.cy)
     assert np.array_equal(got, ref)
     assert set(got[cs:2 * cs].tolist()) <= set(np.nonzero(L.x[:3200] == 0.5)[0].tolist())
+
+
+def test_knn_subset_per_shard(bvlib, oracle):
+    """Each shard's blocks get exactly the sets of the full selection (the
+    others stay zero), and a sharded handle that selects only its own sets
+    gives the same partial as one given all the sets."""
+    x, y = bvlib.generate_xy(4000, 1)
+    z = np.random.default_rng(1).standard_normal(4000)
+    L = bvlib.build_layout(x, y, z, 300, 60, seed=1, epochs=10)
+    full = bvlib.knn(L)
+    th = (1.0, 0.1, 0.5)
+    for r in range(3):
+        mask = bvlib.shard_blocks(L.batchNum, 60, 3, r)
+        sub = bvlib.knn(L, mask=mask)
+        m = np.repeat(mask, 60)
+        m[:60] = True  # block 0's points 0..cs-1
+        assert np.array_equal(sub[m], full[m])
+        assert not sub[~m].any()
+        L.knn_idx = None
+        with bvlib.LlhData(L, shard_count=3, shard_index=r) as D:
+            a = D(th)
+        L.knn_idx = full
+        with bvlib.LlhData(L, shard_count=3, shard_index=r) as D:
+            b = D(th)
+        assert a == b

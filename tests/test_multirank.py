@@ -1,9 +1,10 @@
 """Sharded evaluation across ranks: world_size-2 gloo processes on CPU.
 
-Each rank evaluates its shard of the blocks (the library's bv_shard_blocks
-rule) -- here with the CPU oracle standing in for the device -- and the
-partials are combined in rank order; the result equals the single-process
-log-likelihood."""
+Each rank takes its shard of the blocks by the library's rule
+(bv_shard_blocks), selects only those blocks' conditioning sets and
+evaluates only those blocks -- here with the CPU oracle standing in for the
+device -- and the partials are combined in rank order over the process
+group; the result equals the single-process log-likelihood."""
 import os
 import socket
 
@@ -33,11 +34,21 @@ def _rank_main(rank, world, port, out):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     g = golden("layout_2000_150_60.npz")
-    mask = bv.shard_blocks(g["batchNum"], 60, world, rank)
+    cs = 60
+    mask = bv.shard_blocks(g["batchNum"], cs, world, rank)
+    # This rank's conditioning sets only (block 0: points 0..cs-1).
+    knn = np.zeros(len(g["batchNum"]) * cs, dtype=np.int32)
+    knn[:cs] = np.arange(cs)
+    for b in np.nonzero(mask)[0]:
+        if b > 0:
+            knn[b * cs:(b + 1) * cs] = O.knn_block_fast(g["x_new"], g["y_new"],
+                                                        int(g["batchNumAccum"][b]), g["cx"][b],
+                                                        g["cy"][b], cs)
+    assert np.array_equal(knn[np.repeat(mask, cs)], g["knn"][np.repeat(mask, cs)])
     P = O.OracleProblem(g["batchNum"], g["batchNumAccum"], g["x_new"], g["y_new"], g["obs_new"],
-                        g["knn"], 60)
+                        knn, cs)
     _, pb = O.llh(P, (1.0, 0.08, 1.5), per_block=True)
-    contrib = -(pb[:, 1] ** 2 + pb[:, 0] + g["batchNum"] * np.log(2 * 3.141592653589793)) * 0.5
+    contrib = O.block_llk(g["batchNum"], pb)
     partial = float(np.sum(contrib[mask]))
     total = combine_partials(partial, group=None)
     out[rank] = total
