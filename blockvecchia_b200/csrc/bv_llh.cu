@@ -93,15 +93,24 @@ struct LeanVariant {
     void (*kernel)(LlhArgs);
     int threads, rc;
 };
-// 256 threads, 64-row chunks, two CTAs per SM: measured against 128-thread
-// CTAs (three per SM with 32-row chunks, two with 64) and 32-row chunks at
-// 256 threads on n = 200k, cs = 120 (5.00 ms against 5.09-5.46 ms) and at
-// the cs = 200 shape.
+// Two CTA sizes, 64-row chunks (32-row chunks and three 128-thread CTAs
+// per SM were measured slower).  n = 200k uniform, bc = 20k, nu = 1.5,
+// kernel ms, persistent kernel / 256-thread / 128-thread streamed CTAs:
+//   cs =  40 (M <=  74):  2.99 / 1.36 / 1.03
+//   cs =  80 (M <= 114):  5.23 / 2.59 / 2.50
+//   cs = 120 (M <= 154):  7.87 / 5.05 / 5.16
+//   cs = 160 (M <= 194): 11.22 / 8.72 / 11.53
+//   cs = 200 (M <= 234): 14.63 / 14.37 / 18.84
+// Both give the same bits (the per-element operations do not depend on the
+// CTA size), so the choice only moves time.
 static const LeanVariant kLeanVariants[] = {
     {llh_lean_kernel_t<256, 64, 2>, 256, 64},
+    {llh_lean_kernel_t<128, 64, 2>, 128, 64},
 };
-// Blocks up to this M run the multi-CTA streamed kernel by default.
-constexpr int kLeanMaxM = 160;
+// Blocks up to this M run the multi-CTA streamed kernel by default; the
+// 128-thread CTAs when no block of the launch exceeds kLeanSmallM.
+constexpr int kLeanMaxM = 200;
+constexpr int kLeanSmallM = 100;
 
 static thread_local char g_err[1024] = "";
 
@@ -368,7 +377,7 @@ static int order_m(const bv_handle *h, int t)
 // largest block has M = max_m.
 static int plan_lean_launch(bv_handle *h, const cudaDeviceProp &prop, int begin, int end, int max_m)
 {
-    const LeanVariant &v = kLeanVariants[0];
+    const LeanVariant &v = kLeanVariants[max_m <= kLeanSmallM ? 1 : 0];
     cudaFuncAttributes fa;
     BV_CUDA_TRY(cudaFuncGetAttributes(&fa, v.kernel));
     int optin = 0;

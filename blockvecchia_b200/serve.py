@@ -63,7 +63,8 @@ class Server:
         null_d = C.POINTER(C.c_double)()
         bl = _lib.BvLayout(L.n, L.bc, L.cs, ip(L.batchNum), ip(L.batchNumAccum), dp(L.x),
                            dp(L.y), dp(L.obs), ip(L.knn_idx) if L.knn_idx is not None
-                           else C.POINTER(C.c_int)(), null_d, null_d)
+                           else C.POINTER(C.c_int)(), null_d, null_d,
+                           dp(L.z) if L.z is not None else null_d, null_d)
         jid = C.c_int()
         jo = _lib.BvJobOpts(float(dist_scale), int(bool(nugget)))
         check(lib().bv_server_open_job_ex(self._s, C.byref(bl), C.byref(jo), C.byref(jid)))

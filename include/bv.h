@@ -93,7 +93,7 @@ typedef struct {
     int print_iter;    /* print the reference's per-evaluation line           */
     int use_graph;     /* capture one evaluation in a CUDA graph (default 1)  */
     int schedule;      /* BV_SCHED_AUTO (default): blocks up to a size limit
-                          (M = cs + bs <= 160) on the multi-CTA streamed
+                          (M = cs + bs <= 200) on the multi-CTA streamed
                           kernel, the larger ones on the persistent
                           one-CTA-per-SM kernel; BV_SCHED_BUCKETED: the
                           persistent kernel, one launch per size bucket (the

@@ -83,3 +83,25 @@ def test_fit_matches_oracle_fit(exe, bvlib, oracle, tmp_path):
     ref_th = np.clip(res.x, 0.01, 3.0)
     assert np.all(np.abs(th - ref_th) <= 1e-3 * np.abs(ref_th)), (th, ref_th)
     assert llk >= -res.fun - 1e-6 * abs(res.fun)
+
+
+def test_fit_c1_matches_oracle_fit(exe, bvlib, oracle, tmp_path):
+    """The small configuration's fit (src/test_Xvecchia_batch.cpp:700-753):
+    n = 20,000 GenerateXYLoc locations, bc = 1,500, cs = 300, from
+    0.1:0.1:0.1 at tolerance 1e-4.  The golden optimum is the same
+    Nelder-Mead driven by the CPU oracle's likelihood
+    (tests/golden/make_fit_golden.py); the device fit must land on it within
+    the optimizer tolerance (1e-3 relative per parameter, 10x the stopping
+    rule's simplex spread) and reach the same maximum (1e-8 relative)."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "fit_c1.npz"))
+    n = 20_000
+    x, y = bvlib.generate_xy(n, 0)
+    np.savetxt(tmp_path / "xy.csv", np.stack([x, y], 1), delimiter=",", fmt="%.17g")
+    np.savetxt(tmp_path / "z.csv", g["obs"], fmt="%.17g")
+    th, llk, out = _run(exe, ["--num_loc", str(n), "--vecchia_bc", "1500", "--vecchia_cs", "300",
+                              "--xy_path", "xy.csv", "--obs_path", "z.csv", "--kernel_init",
+                              "0.1:0.1:0.1", "--tol", "4", "--seed", "0"], tmp_path)
+    ref_th, ref_llk = g["theta"], float(g["llk"])
+    print({"device": th.tolist(), "oracle": ref_th.tolist(), "llk": llk, "oracle_llk": ref_llk})
+    assert np.all(np.abs(th - ref_th) <= 1e-3 * np.abs(ref_th)), (th, ref_th)
+    assert abs(llk - ref_llk) <= 1e-8 * abs(ref_llk), (llk, ref_llk)
