@@ -65,13 +65,15 @@ struct KnnArgs {
     int nlist;
 };
 
-// The argument of the key's final square root for candidate p.
+// The argument of the key's final square root for candidate p (kZ: 3-D
+// locations; the 2-D kernels are separate instantiations).
+template <bool kZ>
 __device__ __forceinline__ double knn_prekey(const KnnArgs &a, int p, double cx, double cy, double cz)
 {
     const double dx = __ldg(a.x + p) - cx;
     const double dy = __ldg(a.y + p) - cy;
     const double s = __fma_rn(dx, dx, __dmul_rn(dy, dy));
-    if (!a.z) return s;
+    if constexpr (!kZ) return s;
     const double d = __dsqrt_rn(s);
     const double dz = cz - __ldg(a.z + p);
     return __fma_rn(d, d, __dmul_rn(dz, dz));
@@ -178,6 +180,7 @@ __device__ __forceinline__ unsigned long long window_hi(unsigned long long skey)
     return (unsigned long long)__double_as_longlong(hi);
 }
 
+template <bool kZ>
 __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
 {
     extern __shared__ __align__(16) unsigned char knn_smem[];
@@ -199,7 +202,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
             if (i < 1) break;
         }
         const int P = a.acc[i];
-        const double cx = a.cx[i], cy = a.cy[i], cz = a.z ? a.cz[i] : 0.0;
+        const double cx = a.cx[i], cy = a.cy[i], cz = kZ ? a.cz[i] : 0.0;
         int *out = a.out + (size_t)i * k;
         if (P < k) {
             if (lane == 0) atomicCAS(a.error, 0, i + 1);
@@ -219,7 +222,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
                 keep[u] = false;
                 key[u] = 0ull;
                 if (p < P) {
-                    const double s = knn_prekey(a, p, cx, cy, cz);
+                    const double s = knn_prekey<kZ>(a, p, cx, cy, cz);
                     key[u] = (unsigned long long)__double_as_longlong(s);
                     keep[u] = key[u] <= lim;
                 }
@@ -332,12 +335,14 @@ struct KnnHeavyScratch {
     int *pos;
 };
 
+template <bool kZ>
 __device__ __forceinline__ unsigned long long knn_skey(const KnnArgs &a, int p, double cx, double cy,
                                                        double cz)
 {
-    return (unsigned long long)__double_as_longlong(knn_prekey(a, p, cx, cy, cz));
+    return (unsigned long long)__double_as_longlong(knn_prekey<kZ>(a, p, cx, cy, cz));
 }
 
+template <bool kZ>
 __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int nheavy, KnnHeavyScratch scr,
                                                                   size_t stride)
 {
@@ -353,7 +358,7 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
     for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
         const int i = a.heavy[h];
         const int P = a.acc[i];
-        const double cx = a.cx[i], cy = a.cy[i], cz = a.z ? a.cz[i] : 0.0;
+        const double cx = a.cx[i], cy = a.cy[i], cz = kZ ? a.cz[i] : 0.0;
         int *out = a.out + (size_t)i * k;
         // 1. Exact k-th smallest squared distance, MSB-first radix select.
         if (tid == 0) {
@@ -366,7 +371,7 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
             __syncthreads();
             const unsigned long long prefix = s_prefix;
             for (int p = tid; p < P; p += kHeavyThreads) {
-                const unsigned long long key = knn_skey(a, p, cx, cy, cz);
+                const unsigned long long key = knn_skey<kZ>(a, p, cx, cy, cz);
                 if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255ull], 1u);
             }
             __syncthreads();
@@ -393,7 +398,7 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
         if (tid == 0) s_count = 0;
         __syncthreads();
         for (int p = tid; p < P; p += kHeavyThreads) {
-            const unsigned long long key = knn_skey(a, p, cx, cy, cz);
+            const unsigned long long key = knn_skey<kZ>(a, p, cx, cy, cz);
             if (key <= hi) {
                 const double d = __dsqrt_rn(__longlong_as_double((long long)key));
                 if (d <= dk) {
@@ -534,7 +539,7 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
         ka.list = mask ? d_list : nullptr;
         ka.nlist = (int)list.size();
         const size_t smem = sizeof(KnnWarpSmem) * kKnnWarps;
-        if ((e = cudaFuncSetAttribute(knn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if ((e = cudaFuncSetAttribute(d_z ? knn_kernel<true> : knn_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem))) {
             fail(e, "attribute");
             break;
@@ -542,13 +547,16 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
         int dev = 0, sms = 0, occ = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, knn_kernel, kKnnWarps * 32, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, d_z ? knn_kernel<true> : knn_kernel<false>, kKnnWarps * 32, smem);
         if (occ < 1) occ = 1;
         int grid = sms * occ;
         const int nsel = mask ? (int)list.size() : bc;
         const int need = (nsel + kKnnWarps - 1) / kKnnWarps;
         if (grid > need) grid = need > 0 ? need : 1;
-        knn_kernel<<<grid, kKnnWarps * 32, smem, s>>>(ka);
+        if (d_z)
+            knn_kernel<true><<<grid, kKnnWarps * 32, smem, s>>>(ka);
+        else
+            knn_kernel<false><<<grid, kKnnWarps * 32, smem, s>>>(ka);
         if ((e = cudaGetLastError())) {
             fail(e, "launch");
             break;
@@ -578,7 +586,10 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
                 fail(e, "cudaMalloc (tie scratch)");
                 break;
             }
-            knn_heavy_kernel<<<g, kHeavyThreads, 0, s>>>(ka, nheavy, sc, (size_t)n);
+            if (d_z)
+                knn_heavy_kernel<true><<<g, kHeavyThreads, 0, s>>>(ka, nheavy, sc, (size_t)n);
+            else
+                knn_heavy_kernel<false><<<g, kHeavyThreads, 0, s>>>(ka, nheavy, sc, (size_t)n);
             if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(s))) {
                 fail(e, "tie pass");
                 break;

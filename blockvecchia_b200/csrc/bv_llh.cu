@@ -32,7 +32,7 @@ namespace bv {
 
 // The fused FP64 kernel: persistent CTAs pull blocks from a work counter
 // (largest first) and evaluate each by the path its size calls for.
-template <bool kBig>
+template <bool kBig, bool kXYZ3>
 __global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel_t(LlhArgs a)
 {
     extern __shared__ __align__(128) double smem[];
@@ -46,20 +46,23 @@ __global__ void __launch_bounds__(kThreads, 1) llh_fp64_kernel_t(LlhArgs a)
         __syncthreads();
         const int task = sh.task;
         if (task >= task_end) break;
-        run_block<kBig>(a, mp, a.order[task], smem, sh);
+        run_block<kBig, kXYZ3>(a, mp, a.order[task], smem, sh);
         __syncthreads();
     }
 }
 
 // Without the streamed large-block path compiled in (every layout whose
 // blocks fit shared memory, and the allocation-free entry point), and with it.
-static void (*const llh_fp64_kernel)(LlhArgs) = llh_fp64_kernel_t<false>;
-static void (*const llh_fp64_big_kernel)(LlhArgs) = llh_fp64_kernel_t<true>;
+// 3-D locations (space-time or --3D) run separate instantiations.
+static void (*const llh_fp64_kernel)(LlhArgs) = llh_fp64_kernel_t<false, false>;
+static void (*const llh_fp64_big_kernel)(LlhArgs) = llh_fp64_kernel_t<true, false>;
+static void (*const llh_fp64_kernel3)(LlhArgs) = llh_fp64_kernel_t<false, true>;
+static void (*const llh_fp64_big_kernel3)(LlhArgs) = llh_fp64_kernel_t<true, true>;
 
 // The streamed (left-looking, panels through L2) path run by small CTAs,
 // several per SM, so that the pivot chains of several blocks overlap on one
 // SM: NT threads per CTA, RC rows per streamed chunk, MINB CTAs per SM.
-template <int NT, int RC, int MINB>
+template <int NT, int RC, int MINB, int NS, bool kXYZ3>
 __global__ void __launch_bounds__(NT, MINB) llh_lean_kernel_t(LlhArgs a)
 {
     extern __shared__ __align__(128) double smem[];
@@ -83,16 +86,21 @@ __global__ void __launch_bounds__(NT, MINB) llh_lean_kernel_t(LlhArgs a)
                 a.block_status[b] = a.status_or;
             }
         } else {
-            process_block_big<NT, RC>(a, mp, b, reinterpret_cast<unsigned char *>(smem), slab, sh);
+            process_block_big<NT, RC, LeanShared, NS, kXYZ3>(a, mp, b,
+                                                             reinterpret_cast<unsigned char *>(smem),
+                                                             slab, sh);
         }
         __syncthreads();
     }
 }
 
 struct LeanVariant {
-    void (*kernel)(LlhArgs);
-    int threads, rc;
+    void (*kernel)(LlhArgs);   // 2-D locations
+    void (*kernel3)(LlhArgs);  // with a third coordinate
+    int threads, rc, ns;
 };
+#define BV_LEAN(NT, RC, MINB, NS) \
+    {llh_lean_kernel_t<NT, RC, MINB, NS, false>, llh_lean_kernel_t<NT, RC, MINB, NS, true>, NT, RC, NS}
 // Two CTA sizes, 64-row chunks (32-row chunks and three 128-thread CTAs
 // per SM were measured slower).  n = 200k uniform, bc = 20k, nu = 1.5,
 // kernel ms, persistent kernel / 256-thread / 128-thread streamed CTAs:
@@ -104,8 +112,12 @@ struct LeanVariant {
 // Both give the same bits (the per-element operations do not depend on the
 // CTA size), so the choice only moves time.
 static const LeanVariant kLeanVariants[] = {
-    {llh_lean_kernel_t<256, 64, 2>, 256, 64},
-    {llh_lean_kernel_t<128, 64, 2>, 128, 64},
+    BV_LEAN(256, 64, 2, 2),
+    BV_LEAN(128, 64, 2, 2),
+    BV_LEAN(256, 32, 2, 4),
+    BV_LEAN(256, 64, 2, 3),
+    BV_LEAN(128, 32, 2, 4),
+    BV_LEAN(256, 16, 2, 4),
 };
 // Blocks up to this M run the multi-CTA streamed kernel by default; the
 // 128-thread CTAs when no block of the launch exceeds kLeanSmallM.
@@ -377,19 +389,22 @@ static int order_m(const bv_handle *h, int t)
 // largest block has M = max_m.
 static int plan_lean_launch(bv_handle *h, const cudaDeviceProp &prop, int begin, int end, int max_m)
 {
-    const LeanVariant &v = kLeanVariants[max_m <= kLeanSmallM ? 1 : 0];
+    int vi = max_m <= kLeanSmallM ? 1 : 0;
+    if (const char *ev = getenv("BV_LEAN_VARIANT_EXPERIMENT")) vi = atoi(ev);
+    const LeanVariant &v = kLeanVariants[vi];
+    void (*const kern)(LlhArgs) = h->nz ? v.kernel3 : v.kernel;
     cudaFuncAttributes fa;
-    BV_CUDA_TRY(cudaFuncGetAttributes(&fa, v.kernel));
+    BV_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
     int optin = 0;
     BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-    const size_t smem = big_layout(max_m, v.rc, h->nz).total;
+    const size_t smem = big_layout(max_m, v.rc, h->nz, v.ns).total;
     if (smem > (size_t)optin - fa.sharedSizeBytes) {
         set_error("plan: blocks of M = %d exceed the streamed schedule's shared memory", max_m);
         return BV_E_TOOLARGE;
     }
-    BV_CUDA_TRY(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BV_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
-    BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.kernel, v.threads, smem));
+    BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, v.threads, smem));
     if (occ < 1) {
         set_error("plan: streamed kernel cannot be resident (smem %zu B)", smem);
         return BV_E_TOOLARGE;
@@ -402,7 +417,7 @@ static int plan_lean_launch(bv_handle *h, const cudaDeviceProp &prop, int begin,
         set_error("plan: cannot allocate %zu B of block slabs", bytes);
         return BV_E_NOMEM;
     }
-    h->launches.push_back({begin, end, grid, v.kernel, v.threads, smem, h->d_slab_lean, stride});
+    h->launches.push_back({begin, end, grid, kern, v.threads, smem, h->d_slab_lean, stride});
     return BV_OK;
 }
 
@@ -435,17 +450,16 @@ static int plan_launches(bv_handle *h)
     h->smem_max_m = std::min(cap_m, h->max_m);
     // The cap is per kernel, not per handle: set it to what the device allows
     // so that handles with different block sizes can coexist.
-    BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)avail));
-    BV_CUDA_TRY(cudaFuncSetAttribute(llh_fp64_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)avail));
+    for (auto k : {llh_fp64_kernel, llh_fp64_big_kernel, llh_fp64_kernel3, llh_fp64_big_kernel3})
+        BV_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)avail));
     // Decided on the whole layout (not the shard), so every shard and the
     // server take the same path for a given block.
     h->use_big = (h->opts.large_blocks == BV_LARGE_STREAMED) ||
                  (h->opts.large_blocks == BV_LARGE_AUTO &&
                   use_big_path(h->batchNum.data(), h->bc, h->cs, cap_m, h->big_max_m,
                                prop.multiProcessorCount));
-    h->kernel = h->use_big ? llh_fp64_big_kernel : llh_fp64_kernel;
+    h->kernel = h->use_big ? (h->nz ? llh_fp64_big_kernel3 : llh_fp64_big_kernel)
+                           : (h->nz ? llh_fp64_kernel3 : llh_fp64_kernel);
     if (h->use_big) {
         h->smem_bytes = big_launch_smem(h->max_m, cap_m, h->big_max_m, h->nz);
         h->slab_stride = big_slab_stride(h->max_m, cap_m, h->big_max_m, h->nz);

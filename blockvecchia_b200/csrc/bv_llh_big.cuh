@@ -39,6 +39,8 @@
 namespace bv {
 
 constexpr int kBigRC = 256;              // rows per streamed chunk
+constexpr int kBigStages = 2;            // streamed chunks in flight
+constexpr int kMaxStages = 4;
 
 __host__ __device__ inline int big_panels(int M) { return (M + kNB - 1) / kNB; }
 
@@ -56,14 +58,14 @@ __host__ __device__ inline size_t big_panel_base(int q, int Mp)
 
 // Shared-memory layout (bytes): X, Y, Z (observations), T (third
 // coordinate, 3-D locations only; nz = 1) (M doubles each), Pcur, Pnext (Mp
-// x 16 doubles), two stages of (rc + 16) x 16 doubles, two mbarriers.
+// x 16 doubles), ns stages of (rc + 16) x 16 doubles, ns mbarriers.
 struct BigLayout {
-    unsigned o_X, o_Y, o_Z, o_T, o_cur, o_next, o_stage0, o_stage1, o_bar, total;
+    unsigned o_X, o_Y, o_Z, o_T, o_cur, o_next, o_stage[kMaxStages], o_bar, total;
 };
 
 __host__ __device__ inline unsigned big_align(unsigned v) { return (v + 127u) & ~127u; }
 
-__host__ __device__ inline BigLayout big_layout(int M, int rc = kBigRC, int nz = 0)
+__host__ __device__ inline BigLayout big_layout(int M, int rc = kBigRC, int nz = 0, int ns = kBigStages)
 {
     BigLayout l;
     const unsigned Mp = (unsigned)M + 1;
@@ -74,9 +76,11 @@ __host__ __device__ inline BigLayout big_layout(int M, int rc = kBigRC, int nz =
     l.o_T = o;      if (nz) o = big_align(o + 8u * M);
     l.o_cur = o;    o = big_align(o + 128u * Mp);
     l.o_next = o;   o = big_align(o + 128u * Mp);
-    l.o_stage0 = o; o = big_align(o + 128u * (rc + 16));
-    l.o_stage1 = o; o = big_align(o + 128u * (rc + 16));
-    l.o_bar = o;    o = o + 16;
+    for (int st = 0; st < kMaxStages; ++st) {
+        l.o_stage[st] = o;
+        if (st < ns) o = big_align(o + 128u * (rc + 16));
+    }
+    l.o_bar = o;    o = o + 8u * ns;
     l.total = o;
     return l;
 }
@@ -138,11 +142,16 @@ __device__ __forceinline__ void update_warps_sync()
 // nugget on the diagonal), the observation of point j on row M.  Same
 // argument order and the same nugget addition as the shared-memory path's
 // generation, so the entries are identical.
+template <bool kXYZ3>
 __device__ __forceinline__ double big_entry(const double *X, const double *Y, const double *Z,
                                             const double *T, int M, int i, int j, const MaternParams &mp)
 {
     if (i >= M) return Z[j];
-    const double c = T ? cov_xyz(X[i], Y[i], T[i], X[j], Y[j], T[j], mp) : matern(X[i], Y[i], X[j], Y[j], mp);
+    double c;
+    if constexpr (kXYZ3)
+        c = cov_xyz(X[i], Y[i], T[i], X[j], Y[j], T[j], mp);
+    else
+        c = matern(X[i], Y[i], X[j], Y[j], mp);
     return (i == j && mp.nugget != 0.0) ? c + mp.nugget : c;
 }
 
@@ -195,10 +204,11 @@ __device__ __forceinline__ void panel_update_tiles(double *dst, int dst_r0, cons
 
 // One block by the streamed path, run by a CTA of NT threads (warp 0
 // factors, the other NT/32 - 1 warps generate and update), with RC rows per
-// streamed chunk.  smem: the dynamic area (big_layout(M, RC).total bytes);
-// slab: this CTA's global slab (big_slab_doubles(M) doubles).  Every
-// element's operations and their order are the same for every NT and RC.
-template <int NT, int RC, typename SH>
+// streamed chunk and NS chunks in flight.  smem: the dynamic area
+// (big_layout(M, RC, nz, NS).total bytes); slab: this CTA's global slab
+// (big_slab_doubles(M) doubles).  Every element's operations and their
+// order are the same for every NT, RC and NS.
+template <int NT, int RC, typename SH, int NS = kBigStages, bool kXYZ3 = false>
 static __device__ __noinline__ void process_block_big(const LlhArgs &a, const MaternParams &mp, int b,
                                                       unsigned char *smem, double *slab, SH &sh)
 {
@@ -209,15 +219,16 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
     const int mc = (b == 0) ? 0 : a.cs;
     const int M = mc + bs, Mp = M + 1;
     const int P = big_panels(M);
-    const BigLayout l = big_layout(M, RC, a.z ? 1 : 0);
+    const BigLayout l = big_layout(M, RC, kXYZ3 ? 1 : 0, NS);
     double *X = reinterpret_cast<double *>(smem + l.o_X);
     double *Y = reinterpret_cast<double *>(smem + l.o_Y);
     double *Z = reinterpret_cast<double *>(smem + l.o_Z);
-    double *T = a.z ? reinterpret_cast<double *>(smem + l.o_T) : nullptr;
+    double *T = kXYZ3 ? reinterpret_cast<double *>(smem + l.o_T) : nullptr;
     double *cur = reinterpret_cast<double *>(smem + l.o_cur);
     double *nxt = reinterpret_cast<double *>(smem + l.o_next);
-    double *stage[2] = {reinterpret_cast<double *>(smem + l.o_stage0),
-                        reinterpret_cast<double *>(smem + l.o_stage1)};
+    double *stage[NS];
+#pragma unroll
+    for (int st = 0; st < NS; ++st) stage[st] = reinterpret_cast<double *>(smem + l.o_stage[st]);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + l.o_bar);
 
     const int *kidx = a.knn + (size_t)b * a.cs;
@@ -226,18 +237,17 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         X[t] = __ldg(a.x + src);
         Y[t] = __ldg(a.y + src);
         Z[t] = __ldg(a.obs + src);
-        if (T) T[t] = __ldg(a.z + src);
+        if constexpr (kXYZ3) T[t] = __ldg(a.z + src);
     }
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int st = 0; st < NS; ++st) mbar_init(&bar[st], 1);
         fence_mbar_init();
     }
     __syncthreads();
     // Panel 0 into Pcur.
     for (int e = tid; e < Mp * 16; e += kT) {
         const int r = e >> 4, c = e & 15;
-        const double v = (c < M && r >= c) ? big_entry(X, Y, Z, T, M, r, c, mp) : 0.0;
+        const double v = (c < M && r >= c) ? big_entry<kXYZ3>(X, Y, Z, T, M, r, c, mp) : 0.0;
         cur[r * 16 + swz(r, c)] = v;
     }
     __syncthreads();
@@ -277,7 +287,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
             for (int e = tid - 32; e < nrows * 16; e += kT - 32) {
                 const int r = n0 + (e >> 4), c = e & 15;
                 const int j = n0 + c;
-                const double v = (c < kb1 && r >= j) ? big_entry(X, Y, Z, T, M, r, j, mp) : 0.0;
+                const double v = (c < kb1 && r >= j) ? big_entry<kXYZ3>(X, Y, Z, T, M, r, j, mp) : 0.0;
                 nxt[(r - n0) * 16 + swz(r, c)] = v;
             }
             update_warps_sync<NT>();
@@ -286,7 +296,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
             const bool producer = (tid == 32);
             auto issue = [&](int it) {
                 const int ch = it / p, q = it - ch * p;
-                const int s = it & 1;
+                const int s = it % NS;
                 const int r0 = n0 + ch * RC, r1 = min(Mp, r0 + RC);
                 const int nb = min(kNB, Mp - n0);
                 const double *pq = slab + big_panel_base(q, Mp);
@@ -298,16 +308,18 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
             };
             // The producer (thread 32) counts the copies it issued per stage
             // and the phases it saw complete, to drain after a timeout.
-            int issued[2] = {0, 0}, landed[2] = {0, 0};
+            int issued[NS], landed[NS];
+#pragma unroll
+            for (int st = 0; st < NS; ++st) issued[st] = landed[st] = 0;
             if (producer) {
-                for (int it = 0; it < min(2, items); ++it) {
+                for (int it = 0; it < min(NS, items); ++it) {
                     issue(it);
-                    issued[it & 1]++;
+                    issued[it % NS]++;
                 }
             }
             for (int it = 0; it < items; ++it) {
                 const int ch = it / p;
-                const int s = it & 1;
+                const int s = it % NS;
                 const int r0 = n0 + ch * RC, r1 = min(Mp, r0 + RC);
                 const unsigned par = (phase_bits >> s) & 1u;
                 if (!timed_out) {
@@ -320,16 +332,16 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
                 panel_update_tiles(nxt, n0, stage[s], r0, stage[s] + RC * 16, n0, r0, r1, 1,
                                    kW - 1);
                 update_warps_sync<NT>();
-                if (producer && !timed_out && it + 2 < items) {
+                if (producer && !timed_out && it + NS < items) {
                     fence_proxy_async_shared();
-                    issue(it + 2);
+                    issue(it + NS);
                     issued[s]++;
                 }
             }
             if (producer && timed_out) {
                 // Copies still in flight must land before this shared memory
                 // is used again: wait (bounded) for each stage's last phase.
-                for (int s = 0; s < 2; ++s)
+                for (int s = 0; s < NS; ++s)
                     if (issued[s] > landed[s]) mbar_wait_bounded(&bar[s], (unsigned)(issued[s] - 1) & 1u);
             }
         }
@@ -420,8 +432,8 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         a.block_llk[b] = v;
         a.block_status[b] = s2 | a.status_or;
         // The barriers are re-initialised for the next block.
-        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar[0])) : "memory");
-        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar[1])) : "memory");
+        for (int st = 0; st < NS; ++st)
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar[st])) : "memory");
     }
 }
 
@@ -430,7 +442,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
 // shared-memory algorithm on this CTA's global slab.
 // kBig = false compiles the shared-memory and slab paths only, so layouts
 // without large blocks run the same code as before the streamed path existed.
-template <bool kBig>
+template <bool kBig, bool kXYZ3 = false>
 __device__ __forceinline__ void run_block(const LlhArgs &a, const MaternParams &mp, int b, double *smem,
                                           BlockShared &sh)
 {
@@ -444,16 +456,18 @@ __device__ __forceinline__ void run_block(const LlhArgs &a, const MaternParams &
             a.block_status[b] = a.status_or;
         }
     } else if (M <= a.smem_max_m) {
-        const int nc = a.z ? 3 : 2;  // coordinate arrays before the matrix
-        process_block(a, mp, b, smem, smem + M, a.z ? smem + 2 * M : nullptr, smem + nc * M, sh);
+        constexpr int nc = kXYZ3 ? 3 : 2;  // coordinate arrays before the matrix
+        process_block<kXYZ3>(a, mp, b, smem, smem + M, kXYZ3 ? smem + 2 * M : nullptr, smem + nc * M,
+                             sh);
     } else {
         double *slab = a.gslab + (size_t)blockIdx.x * a.gslab_stride;
         if (kBig && M <= a.big_max_m) {
-            process_block_big<kThreads, kBigRC>(a, mp, b, reinterpret_cast<unsigned char *>(smem), slab,
-                                                sh);
+            process_block_big<kThreads, kBigRC, BlockShared, kBigStages, kXYZ3>(
+                a, mp, b, reinterpret_cast<unsigned char *>(smem), slab, sh);
         } else {
-            const int nc = a.z ? 3 : 2;
-            process_block(a, mp, b, slab, slab + M, a.z ? slab + 2 * M : nullptr, slab + nc * M, sh);
+            constexpr int nc = kXYZ3 ? 3 : 2;
+            process_block<kXYZ3>(a, mp, b, slab, slab + M, kXYZ3 ? slab + 2 * M : nullptr,
+                                 slab + nc * M, sh);
         }
     }
 }

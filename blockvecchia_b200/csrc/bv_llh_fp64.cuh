@@ -267,18 +267,15 @@ __device__ __forceinline__ void generate_t(double *A, const double *X, const dou
     }
 }
 
-// Out of line, so the 2-D kernels' register allocation does not carry it.
-static __device__ __noinline__ void generate_xyz(double *A, const double *X, const double *Y,
-                                                 const double *T, int M, const MaternParams &mp)
-{
-    generate_t<kXYZ>(A, X, Y, T, M, mp);
-}
-
+// kXYZ: locations with a third coordinate (T); the 2-D kernels are
+// separate instantiations, so their code and register allocation carry
+// nothing of the 3-D path.
+template <bool kXYZ3>
 __device__ __forceinline__ void generate(double *A, const double *X, const double *Y, const double *T,
                                          int M, const MaternParams &mp)
 {
-    if (T) {
-        generate_xyz(A, X, Y, T, M, mp);
+    if constexpr (kXYZ3) {
+        generate_t<kXYZ>(A, X, Y, T, M, mp);
         return;
     }
     switch (mp.nu_kind) {
@@ -1037,7 +1034,8 @@ __device__ __forceinline__ void cholesky_pp(double *A, int M, int mc, BlockShare
 }
 
 // One block, with its matrix at A (shared memory or the global slab); T
-// holds the third coordinate of 3-D locations (nullptr for 2-D).
+// holds the third coordinate of 3-D locations (kXYZ3; unused for 2-D).
+template <bool kXYZ3>
 __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternParams &mp, int b,
                                               double *X, double *Y, double *T, double *A,
                                               BlockShared &sh)
@@ -1055,11 +1053,11 @@ __device__ __forceinline__ void process_block(const LlhArgs &a, const MaternPara
         const int src = (t < mc) ? __ldg(kidx + t) : off + (t - mc);
         X[t] = __ldg(a.x + src);
         Y[t] = __ldg(a.y + src);
-        if (T) T[t] = __ldg(a.z + src);
+        if constexpr (kXYZ3) T[t] = __ldg(a.z + src);
         A[poff(t, Mp) + M] = __ldg(a.obs + src);
     }
     __syncthreads();
-    generate(A, X, Y, T, M, mp);
+    generate<kXYZ3>(A, X, Y, T, M, mp);
     __syncthreads();
     if (mp.nugget != 0.0) {
         // Nugget: tau^2 on the diagonal of Sigma22 and Sigma11 (a point with

@@ -47,7 +47,8 @@ def test_ill_conditioned_falls_back_to_fp64(bvlib):
     beyond 1/eps32); the fallback reproduces the FP64 path exactly."""
     L = _gen(bvlib, 6000, 600, 80)
     th = (1.0, 0.05, 2.5)
-    with bvlib.LlhData(L) as D:
+    # The fallback pass runs the persistent kernel.
+    with bvlib.LlhData(L, schedule="persistent") as D:
         v64 = D(th)
         b64 = D.block_llk()
     with bvlib.LlhData(L, precision="mixed", on_failure="continue") as M:
