@@ -496,9 +496,9 @@ def run_ours(args):
                          "skips the FP32 pass when most would fail)"}
     serve = None
     if world == 1 and args.serve_sample > 0:
-        # Near the server's capacity for this job mix (~40 evaluations/s), so
-        # requests queue and batches form: 6.5 jobs/s x 6 evaluations.
-        serve = serve_workload(args.serve_sample, 6, 6.5, 2, repeats=3)
+        # At the server's capacity: 16 fitting jobs in flight at all times
+        # (closed loop), so requests queue and batches form.
+        serve = serve_workload(args.serve_sample, 6, 0.0, 2, repeats=3, concurrency=16)
         serve.pop("clocks", None)
 
     # FP64: fused kernel + reduction; mixed: probe, decision, mixed pass,
@@ -626,7 +626,7 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ serving
 
-def serve_workload(jobs, evals, rate, inflight, seed=20241, repeats=1):
+def serve_workload(jobs, evals, rate, inflight, seed=20241, repeats=1, concurrency=0):
     """Serving workload: independent fitting jobs with Poisson arrivals.  Per
     job: n log-uniform in 5,000-500,000 locations uniform on [0,1]^2, nu from
     {0.5, 1.5, 2.5}, sigma2 uniform in 0.5-2, range uniform in 0.02-0.2, cs
@@ -635,7 +635,9 @@ def serve_workload(jobs, evals, rate, inflight, seed=20241, repeats=1):
     issues `evals` sequential evaluations (the first at the true parameters,
     then optimizer-like probes around them, nu included, so the general-nu
     Bessel path runs too) and closes the job.  Returns throughput and request
-    latency (submit to result) percentiles."""
+    latency (submit to result) percentiles.  concurrency > 0: closed loop
+    instead -- that many clients, each running one job after another (jobs
+    taken in order), so the offered load is whatever the server sustains."""
     from concurrent.futures import ThreadPoolExecutor
 
     import torch
@@ -650,7 +652,7 @@ def serve_workload(jobs, evals, rate, inflight, seed=20241, repeats=1):
     s2 = g.uniform(0.5, 2.0, J)
     rg = g.uniform(0.02, 0.2, J)
     css = g.choice([60, 120, 300], J)
-    arrivals = np.cumsum(g.exponential(1.0 / rate, J))
+    arrivals = np.cumsum(g.exponential(1.0 / rate, J)) if rate > 0 else np.zeros(J)
 
     t_prep = time.perf_counter()
     draws = []
@@ -697,7 +699,22 @@ def serve_workload(jobs, evals, rate, inflight, seed=20241, repeats=1):
             srv.close_job(j)
             results[i] = (out, time.perf_counter())
 
-        threads = [threading.Thread(target=client, args=(i,)) for i in range(J)]
+        if concurrency > 0:
+            nxt = [0]
+            lock = threading.Lock()
+
+            def worker():
+                while True:
+                    with lock:
+                        i = nxt[0]
+                        nxt[0] += 1
+                    if i >= J:
+                        return
+                    arrivals[i] = time.perf_counter() - t0  # starts now
+                    client(i)
+            threads = [threading.Thread(target=worker) for _ in range(concurrency)]
+        else:
+            threads = [threading.Thread(target=client, args=(i,)) for i in range(J)]
         for t in threads:
             t.start()
         for t in threads:
@@ -736,10 +753,12 @@ def serve_workload(jobs, evals, rate, inflight, seed=20241, repeats=1):
         "values_identical_across_repeats": bool(same),
         "nonfinite_llk": bad,
         "prep_s": round(prep_s, 1),
-        "workload": f"{J} jobs, Poisson arrivals at {rate}/s, n log-uniform 5k-500k, "
-                    f"cs in {{60,120,300}}, bc=n/10, nu in {{0.5,1.5,2.5}}, {E} sequential "
-                    f"evaluations per job, {inflight} batches in flight, the same sample run "
-                    f"{len(runs)} times (median and [min, max] reported)",
+        "workload": (f"{J} jobs, " + (f"{concurrency} concurrent clients (closed loop: a client "
+                                       f"starts the next job when its job ends)" if concurrency > 0
+                                       else f"Poisson arrivals at {rate}/s") +
+                     f", n log-uniform 5k-500k, cs in {{60,120,300}}, bc=n/10, nu in {{0.5,1.5,2.5}}, "
+                     f"{E} sequential evaluations per job, {inflight} batches in flight, the same "
+                     f"sample run {len(runs)} times (median and [min, max] reported)"),
         "total_points": int(ns.sum()),
         "clocks": clk,
     }
@@ -748,7 +767,7 @@ def serve_workload(jobs, evals, rate, inflight, seed=20241, repeats=1):
 
 def run_serve(args):
     r = serve_workload(args.serve_jobs, args.serve_evals, args.serve_rate, args.serve_inflight,
-                       repeats=args.serve_repeats)
+                       repeats=args.serve_repeats, concurrency=args.serve_concurrency)
     out = {
         "metric": "serve p50/p99 ms and evals/s, mixed-size concurrent fitting jobs",
         "value": r["evals_per_s"], "unit": "evals/s", "n_gpus": 1, "higher_is_better": True,
@@ -778,6 +797,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=8.0, help="job arrivals per second")
     ap.add_argument("--serve-inflight", type=int, default=2)
     ap.add_argument("--serve-repeats", type=int, default=1)
+    ap.add_argument("--serve-concurrency", type=int, default=0,
+                    help="closed loop with this many concurrent clients (0: Poisson arrivals)")
     ap.add_argument("--case", choices=sorted(WORKLOADS), default="c3",
                     help="c3: the headline workload (default); c3-small: profiling case")
     ap.add_argument("--write-layout", action="store_true",

@@ -118,6 +118,8 @@ static const LeanVariant kLeanVariants[] = {
     BV_LEAN(256, 64, 2, 3),
     BV_LEAN(128, 32, 2, 4),
     BV_LEAN(256, 16, 2, 4),
+    BV_LEAN(256, 64, 2, 0),
+    BV_LEAN(128, 64, 3, 0),
 };
 // Blocks up to this M run the multi-CTA streamed kernel by default; the
 // 128-thread CTAs when no block of the launch exceeds kLeanSmallM.

@@ -202,9 +202,104 @@ __device__ __forceinline__ void panel_update_tiles(double *dst, int dst_r0, cons
     }
 }
 
+// The left-looking update of panel p+1 without staging: nxt rows [n0, Mp)
+// (local row = i - n0) take panels q = 0..p-1 read straight from this CTA's
+// slab (L2), each panel's rank-16 product formed from zero and subtracted on
+// its own, in q order -- per element the same operations in the same order
+// as the staged update, so the same bits.  Warps [w0, w0 + nw) own 8-row
+// tiles (tile t on warp t mod nw) and keep up to kDT of them in registers
+// across all q, so the warps never wait for one another; the next panel's
+// fragments are loaded while the current one is applied.
+constexpr int kDT = 4;
+
+__device__ __forceinline__ void load_frags(const double *slab, int Mp, int q, int n0, int i0, int ntile,
+                                           int nw, int r8, int c4, double (&bf)[4][2],
+                                           double (&af)[kDT][4])
+{
+    const double *pq = slab + big_panel_base(q, Mp);
+    const int q0 = q * kNB;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+        for (int nj = 0; nj < 2; ++nj) {
+            const int r = n0 + 8 * nj + r8, k = 4 * kk + c4;
+            bf[kk][nj] = (r < Mp) ? __ldcg(pq + (size_t)(r - q0) * 16 + swz(r, k)) : 0.0;
+        }
+#pragma unroll
+    for (int m = 0; m < kDT; ++m) {
+        const int ia = i0 + 8 * nw * m + r8;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+            af[m][kk] = (m < ntile && ia < Mp) ? __ldcg(pq + (size_t)(ia - q0) * 16 + swz(ia, 4 * kk + c4))
+                                               : 0.0;
+    }
+}
+
+__device__ __forceinline__ void panel_update_direct(double *nxt, int n0, const double *slab, int Mp, int p,
+                                                    int w0, int nw)
+{
+    const int warp = (threadIdx.x >> 5) - w0, lane = threadIdx.x & 31;
+    if (warp < 0 || warp >= nw || p == 0) return;
+    const int r8 = lane >> 2, c4 = lane & 3;
+    const int ntiles = (Mp - n0 + 7) >> 3;
+    for (int t0 = warp; t0 < ntiles; t0 += nw * kDT) {
+        const int ntile = min(kDT, (ntiles - t0 + nw - 1) / nw);  // tiles t0, t0 + nw, ...
+        const int i0 = n0 + 8 * t0;
+        double d[kDT][2][2];
+#pragma unroll
+        for (int m = 0; m < kDT; ++m) {
+            const int ia = i0 + 8 * nw * m + r8;
+#pragma unroll
+            for (int nj = 0; nj < 2; ++nj)
+#pragma unroll
+                for (int e = 0; e < 2; ++e)
+                    d[m][nj][e] = (m < ntile && ia < Mp) ? nxt[(ia - n0) * 16 + swz(ia, 8 * nj + 2 * c4 + e)] : 0.0;
+        }
+        double bf[4][2], af[kDT][4], bn[4][2], an[kDT][4];
+        load_frags(slab, Mp, 0, n0, i0, ntile, nw, r8, c4, bf, af);
+        for (int q = 0; q < p; ++q) {
+            if (q + 1 < p) load_frags(slab, Mp, q + 1, n0, i0, ntile, nw, r8, c4, bn, an);
+#pragma unroll
+            for (int m = 0; m < kDT; ++m) {
+                if (m < ntile) {
+                    double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+                        for (int nj = 0; nj < 2; ++nj) dmma_8x8x4(acc[nj][0], acc[nj][1], af[m][kk], bf[kk][nj]);
+#pragma unroll
+                    for (int nj = 0; nj < 2; ++nj)
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) d[m][nj][e] -= acc[nj][e];
+                }
+            }
+            if (q + 1 < p) {
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+#pragma unroll
+                    for (int nj = 0; nj < 2; ++nj) bf[kk][nj] = bn[kk][nj];
+#pragma unroll
+                    for (int m = 0; m < kDT; ++m) af[m][kk] = an[m][kk];
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < kDT; ++m) {
+            const int ia = i0 + 8 * nw * m + r8;
+            if (m < ntile && ia < Mp) {
+#pragma unroll
+                for (int nj = 0; nj < 2; ++nj)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) nxt[(ia - n0) * 16 + swz(ia, 8 * nj + 2 * c4 + e)] = d[m][nj][e];
+            }
+        }
+    }
+}
+
 // One block by the streamed path, run by a CTA of NT threads (warp 0
 // factors, the other NT/32 - 1 warps generate and update), with RC rows per
-// streamed chunk and NS chunks in flight.  smem: the dynamic area
+// streamed chunk and NS chunks in flight (NS = 0: no staging, the warps read
+// the slab directly, panel_update_direct).  smem: the dynamic area
 // (big_layout(M, RC, nz, NS).total bytes); slab: this CTA's global slab
 // (big_slab_doubles(M) doubles).  Every element's operations and their
 // order are the same for every NT, RC and NS.
@@ -226,7 +321,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
     double *T = kXYZ3 ? reinterpret_cast<double *>(smem + l.o_T) : nullptr;
     double *cur = reinterpret_cast<double *>(smem + l.o_cur);
     double *nxt = reinterpret_cast<double *>(smem + l.o_next);
-    double *stage[NS];
+    double *stage[NS > 0 ? NS : 1];
 #pragma unroll
     for (int st = 0; st < NS; ++st) stage[st] = reinterpret_cast<double *>(smem + l.o_stage[st]);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + l.o_bar);
@@ -291,6 +386,9 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
                 nxt[(r - n0) * 16 + swz(r, c)] = v;
             }
             update_warps_sync<NT>();
+            if constexpr (NS == 0) {
+                panel_update_direct(nxt, n0, slab, Mp, p, 1, kW - 1);
+            } else {
             const int nchunk = (nrows + RC - 1) / RC;
             const int items = nchunk * p;       // (chunk, q), q fastest
             const bool producer = (tid == 32);
@@ -343,6 +441,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
                 // is used again: wait (bounded) for each stage's last phase.
                 for (int s = 0; s < NS; ++s)
                     if (issued[s] > landed[s]) mbar_wait_bounded(&bar[s], (unsigned)(issued[s] - 1) & 1u);
+            }
             }
         }
         __syncthreads();
