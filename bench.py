@@ -61,6 +61,15 @@ WORKLOADS = {
     "c2": dict(name="n=200k uniform, nu=1.5 sigma2=1 range=0.08, bc=20k, cs=120",
                n=200_000, bc=20_000, cs=120, sigma2=1.0, range=0.08, nu=1.5, seed=0,
                kmeans_epochs=50, rff_features=1024),
+    # The general-nu stress configuration: 2M points from a 50-component
+    # Gaussian mixture, cs = 300 (streamed path), nu = 0.8 (Bessel K_nu),
+    # nugget 0.01.  The oracle checks a sample of blocks (a whole CPU
+    # evaluation takes hours).
+    "c5": dict(name="n=2M Gaussian mixture (50 comps), nu=0.8 sigma2=1 range=0.1 nugget=0.01, "
+                    "bc=200k, cs=300",
+               n=2_000_000, bc=200_000, cs=300, sigma2=1.0, range=0.1, nu=0.8, nugget=0.01,
+               seed=0, kmeans_epochs=50, rff_features=1024, locations="mixture",
+               oracle_sample=400),
     # The small configuration's shape (cs = 300: the streamed large-block path).
     "c1": dict(name="n=20k uniform, nu=0.5 sigma2=1.5 range=0.1, bc=1.5k, cs=300",
                n=20_000, bc=1_500, cs=300, sigma2=1.5, range=0.1, nu=0.5, seed=0,
@@ -76,6 +85,28 @@ WORKLOAD = WORKLOADS["c3"]
 def make_locations(n, seed):
     rng = np.random.default_rng(seed)
     return rng.random(n), rng.random(n)
+
+
+def mixture_locations(n, seed, components=50):
+    """A 2-D Gaussian mixture: component centres uniform on [0,1]^2, standard
+    deviations uniform in [0.01, 0.05], equal weights (not clipped)."""
+    g = np.random.default_rng(seed)
+    centers = g.random((components, 2))
+    stds = g.uniform(0.01, 0.05, components)
+    comp = g.integers(0, components, n)
+    pts = centers[comp] + g.standard_normal((n, 2)) * stds[comp, None]
+    return pts[:, 0].copy(), pts[:, 1].copy()
+
+
+def workload_locations(w):
+    if w.get("locations") == "mixture":
+        return mixture_locations(w["n"], w["seed"])
+    return make_locations(w["n"], w["seed"])
+
+
+def workload_theta(w):
+    th = (w["sigma2"], w["range"], w["nu"])
+    return th + ((w["nugget"],) if w.get("nugget") else ())
 
 
 def rff_draw(x, y, sigma2, rng_, nu, features, seed, device=None):
@@ -180,7 +211,10 @@ DATA = os.path.join(ROOT, "bench_data")
 
 def _recipe(w):
     keys = ("n", "bc", "cs", "sigma2", "range", "nu", "seed", "kmeans_epochs", "rff_features")
-    return {k: w[k] for k in keys}
+    r = {k: w[k] for k in keys}
+    if w.get("locations"):
+        r["locations"] = w["locations"]
+    return r
 
 
 def layout_path(w):
@@ -192,7 +226,7 @@ def write_layout(w):
     ordering, first-block merge, block reordering) and save it with the
     locations and observations, block-ordered."""
     import blockvecchia_b200 as bv
-    x, y = make_locations(w["n"], w["seed"])
+    x, y = workload_locations(w)
     obs = rff_draw(x, y, w["sigma2"], w["range"], w["nu"], w["rff_features"], w["seed"])
     L = bv.build_layout(x, y, obs, w["bc"], w["cs"], seed=w["seed"], epochs=w["kmeans_epochs"])
     os.makedirs(DATA, exist_ok=True)
@@ -255,7 +289,45 @@ def chunk_bounds(flops, k):
     return list(zip(cuts[:-1], cuts[1:]))
 
 
-def oracle_parity(L, theta, dev_blocks, dev_status, dev_total, threads):
+def oracle_parity_sample(L, theta, dev_blocks, dev_knn, flops, count, threads, nugget=0.0):
+    """For workloads too large for a whole CPU evaluation: a contiguous
+    sample of blocks from the middle of the order, their conditioning sets
+    recomputed by the oracle (must equal the device's bit for bit) and their
+    contributions by the oracle (with the same nugget); the sample's time,
+    extrapolated by algorithmic FLOPs, is the CPU baseline."""
+    from oracle import oracle as O
+    O.build(ref=False)
+    cs, bc = L.cs, L.bc
+    b0 = bc // 2
+    b1 = min(bc, b0 + count)
+    knn = np.array(dev_knn, copy=True)
+    same = True
+    for b in range(b0, b1):
+        ref = O.knn_block_fast(L.x, L.y, int(L.batchNumAccum[b]), L.cx[b], L.cy[b], cs)
+        same = same and np.array_equal(ref, dev_knn[b * cs:(b + 1) * cs])
+        knn[b * cs:(b + 1) * cs] = ref
+    P = O.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, knn, cs, nugget=nugget)
+    t0 = time.perf_counter()
+    _, pb = O.llh_blas(P, theta[:3], threads=threads, block_begin=b0, block_end=b1, per_block=True)
+    dt = time.perf_counter() - t0
+    ref_blocks = O.block_llk(L.batchNum, pb)[b0:b1]
+    dev = dev_blocks[b0:b1]
+    ok = (pb[b0:b1, 2] == 0) & (pb[b0:b1, 3] == 0)
+    rel = np.abs(dev - ref_blocks) / np.maximum(1.0, np.abs(ref_blocks))
+    frac = float(flops[b0:b1].sum() / flops.sum())
+    parity = {"sample_blocks": [int(b0), int(b1)], "knn_bit_exact": bool(same),
+              "rel_err_sample_sum": abs(float(dev[ok].sum()) - float(ref_blocks[ok].sum())) /
+              abs(float(ref_blocks[ok].sum())),
+              "max_block_rel_diff": float(rel[ok].max()) if ok.any() else None,
+              "blocks_over_1e-10": int((rel[ok] > 1e-10).sum()),
+              "failed_blocks_oracle": int((~ok).sum()), "nugget": nugget}
+    cpu = {"value": frac / dt, "unit": "evals/s", "cores": threads, "kind": "port",
+           "sample": f"blocks {b0}..{b1 - 1} ({frac * 100:.2f}% of the evaluation's flops) in {dt:.1f} s, "
+                     "extrapolated by flops"}
+    return parity, cpu
+
+
+def oracle_parity(L, theta, dev_blocks, dev_status, dev_total, threads, nugget=0.0):
     """One whole evaluation by the CPU oracle (timed: the CPU baseline) and
     its comparison with the device evaluation of the same blocks: the total,
     and per block, split into blocks where either side met a non-positive
@@ -263,7 +335,7 @@ def oracle_parity(L, theta, dev_blocks, dev_status, dev_total, threads):
     column, the device zeroes it and continues) and the rest."""
     from oracle import oracle as O
     O.build(ref=False)
-    P = O.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, L.knn_idx, L.cs)
+    P = O.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, L.knn_idx, L.cs, nugget=nugget)
     t0 = time.perf_counter()
     ref_total, pb = O.llh_blas(P, theta, threads=threads, per_block=True)
     dt = time.perf_counter() - t0
@@ -344,7 +416,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     w = WORKLOAD
-    theta = (w["sigma2"], w["range"], w["nu"])
+    theta = workload_theta(w)
 
     t_setup = time.perf_counter()
     d = load_layout(w)
@@ -355,6 +427,7 @@ def run_ours(args):
     L.knn_idx = bv.knn(L, device=local)
     setup_knn_s = time.perf_counter() - t_knn
     D = bv.LlhData(L, precision=args.precision, device=local, on_failure="continue",
+                   nugget=bool(w.get("nugget")),
                    shard_count=world, shard_index=rank)
     stream = torch.cuda.Stream(device=local)
     D.set_stream(stream.cuda_stream)
@@ -453,14 +526,21 @@ def run_ours(args):
     if world == 1 and not args.no_cpu_baseline:
         dev_blocks = D.block_llk()
         dev_status = D.block_status()
-        parity, cpu = oracle_parity(L, theta, dev_blocks, dev_status, v, host_threads())
+        if w.get("oracle_sample"):
+            parity, cpu = oracle_parity_sample(L, theta, dev_blocks, L.knn_idx, flops,
+                                               w["oracle_sample"], host_threads(),
+                                               nugget=w.get("nugget", 0.0))
+        else:
+            parity, cpu = oracle_parity(L, theta, dev_blocks, dev_status, v, host_threads(),
+                                        nugget=w.get("nugget", 0.0))
 
     # Mixed precision on the same workload (the FP64 path is the reference):
     # timed like the FP64 loop, plus the range sweep's relative error and
     # fallback counts.
     mixed = None
     if world == 1 and not args.no_mixed and args.precision == "fp64":
-        with bv.LlhData(L, precision="mixed", device=local, on_failure="continue") as Mx:
+        with bv.LlhData(L, precision="mixed", device=local, on_failure="continue",
+                        nugget=bool(w.get("nugget"))) as Mx:
             Mx.set_stream(stream.cuda_stream)
             for _ in range(args.warmup):
                 step_mx = Mx(theta)
@@ -478,7 +558,7 @@ def run_ours(args):
             stm = Mx.status()
             sweep = []
             for rg_ in (0.02, 0.05, 0.1, 0.2, 0.3):
-                th_ = (w["sigma2"], rg_, w["nu"])
+                th_ = (w["sigma2"], rg_, w["nu"]) + tuple(theta[3:])
                 v64_ = D(th_)
                 s64_ = D.status()
                 vm_ = Mx(th_)
@@ -572,7 +652,7 @@ def run_reference(args):
     if rank != 0:
         return
     w = WORKLOAD
-    theta = (w["sigma2"], w["range"], w["nu"])
+    theta = workload_theta(w)
     d = load_layout(w, child_build=True)
     from oracle import oracle as O
     O.build(ref=False)
@@ -581,7 +661,8 @@ def run_reference(args):
     t0 = time.perf_counter()
     knn = O.knn_all_fast(d["x"], d["y"], cs, d["batchNumAccum"], d["cx"], d["cy"], threads=threads)
     knn_s = time.perf_counter() - t0
-    P = O.OracleProblem(d["batchNum"], d["batchNumAccum"], d["x"], d["y"], d["obs"], knn, cs)
+    P = O.OracleProblem(d["batchNum"], d["batchNumAccum"], d["x"], d["y"], d["obs"], knn, cs,
+                        nugget=w.get("nugget", 0.0))
     bc = len(d["batchNum"])
     flops = block_flops(d["batchNum"], cs)
     chunks = chunk_bounds(flops, args.steps)

@@ -120,6 +120,9 @@ static const LeanVariant kLeanVariants[] = {
     BV_LEAN(256, 16, 2, 4),
     BV_LEAN(256, 64, 2, 0),
     BV_LEAN(128, 64, 3, 0),
+    BV_LEAN(128, 64, 4, 0),
+    BV_LEAN(192, 64, 2, 0),
+    BV_LEAN(96, 64, 5, 0),
 };
 // Blocks up to this M run the multi-CTA streamed kernel by default; the
 // 128-thread CTAs when no block of the launch exceeds kLeanSmallM.
