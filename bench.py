@@ -583,7 +583,7 @@ def run_ours(args):
 
     # FP64: fused kernel + reduction; mixed: probe, decision, mixed pass,
     # FP64 fallback pass, reduction.
-    launches_per_eval = 2 if args.precision == "fp64" else 5
+    launches_per_eval = int(st["launches"])
     value = args.steps / (ms / 1e3)
     out = {
         "metric": METRIC,

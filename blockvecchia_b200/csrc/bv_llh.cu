@@ -101,33 +101,28 @@ struct LeanVariant {
 };
 #define BV_LEAN(NT, RC, MINB, NS) \
     {llh_lean_kernel_t<NT, RC, MINB, NS, false>, llh_lean_kernel_t<NT, RC, MINB, NS, true>, NT, RC, NS}
-// Two CTA sizes, 64-row chunks (32-row chunks and three 128-thread CTAs
-// per SM were measured slower).  n = 200k uniform, bc = 20k, nu = 1.5,
-// kernel ms, persistent kernel / 256-thread / 128-thread streamed CTAs:
-//   cs =  40 (M <=  74):  2.99 / 1.36 / 1.03
-//   cs =  80 (M <= 114):  5.23 / 2.59 / 2.50
-//   cs = 120 (M <= 154):  7.87 / 5.05 / 5.16
-//   cs = 160 (M <= 194): 11.22 / 8.72 / 11.53
-//   cs = 200 (M <= 234): 14.63 / 14.37 / 18.84
-// Both give the same bits (the per-element operations do not depend on the
-// CTA size), so the choice only moves time.
+// The left-looking update reads the earlier panels straight from the slab
+// (no staging), so the CTAs can be small and several blocks share an SM.
+// Kernel ms, n = 200k uniform, bc = 20k, nu = 1.5 (first column: the
+// persistent kernel; then 96-thread CTAs x5 per SM, 128 x3, 192 x2):
+//   cs =  40 (M <=  74):  2.54 / 0.88 / 1.01 / 1.36
+//   cs =  80 (M <= 114):  4.48 / 2.37 / 2.27 / 2.66
+//   cs = 120 (M <= 154):  6.88 / 5.46 / 4.61 / 5.06
+//   cs = 160 (M <= 194):  9.99 / 11.6 / 8.21 / 8.39
+//   cs = 200 (M <= 234): 13.62 / 21.2 / 13.38 / 13.18
+//   cs = 240 (M <= 274): 26.26 / 38.2 / 23.68 / 19.40
+//   cs = 300 (M <= 334): 41.08 / 65.7 / 39.14 / 32.27
+// and at the headline shape (n = 1M, cs = 200, nu = 2.5): 68.0 / - / 65.6
+// / 65.7.  Staged variants (chunks copied to shared memory by bulk copies,
+// 2-4 in flight, 256- and 128-thread CTAs) measured 70-122 ms there.  All
+// give the same bits (the per-element operations do not depend on the CTA
+// size).
 static const LeanVariant kLeanVariants[] = {
-    BV_LEAN(256, 64, 2, 2),
-    BV_LEAN(128, 64, 2, 2),
-    BV_LEAN(256, 32, 2, 4),
-    BV_LEAN(256, 64, 2, 3),
-    BV_LEAN(128, 32, 2, 4),
-    BV_LEAN(256, 16, 2, 4),
-    BV_LEAN(256, 64, 2, 0),
-    BV_LEAN(128, 64, 3, 0),
-    BV_LEAN(128, 64, 4, 0),
-    BV_LEAN(192, 64, 2, 0),
     BV_LEAN(96, 64, 5, 0),
+    BV_LEAN(128, 64, 3, 0),
+    BV_LEAN(192, 64, 2, 0),
 };
-// Blocks up to this M run the multi-CTA streamed kernel by default; the
-// 128-thread CTAs when no block of the launch exceeds kLeanSmallM.
-constexpr int kLeanMaxM = 200;
-constexpr int kLeanSmallM = 100;
+static int lean_variant(int max_m) { return max_m <= 96 ? 0 : (max_m <= 234 ? 1 : 2); }
 
 static thread_local char g_err[1024] = "";
 
@@ -394,9 +389,7 @@ static int order_m(const bv_handle *h, int t)
 // largest block has M = max_m.
 static int plan_lean_launch(bv_handle *h, const cudaDeviceProp &prop, int begin, int end, int max_m)
 {
-    int vi = max_m <= kLeanSmallM ? 1 : 0;
-    if (const char *ev = getenv("BV_LEAN_VARIANT_EXPERIMENT")) vi = atoi(ev);
-    const LeanVariant &v = kLeanVariants[vi];
+    const LeanVariant &v = kLeanVariants[lean_variant(max_m)];
     void (*const kern)(LlhArgs) = h->nz ? v.kernel3 : v.kernel;
     cudaFuncAttributes fa;
     BV_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
@@ -427,11 +420,12 @@ static int plan_lean_launch(bv_handle *h, const cudaDeviceProp &prop, int begin,
 }
 
 // Which kernel evaluates which blocks.  Blocks are in the processing order
-// (largest first).  Under the default schedule the blocks with M <=
-// kLeanMaxM run the multi-CTA streamed kernel (several blocks per SM, so
-// their pivot chains overlap), the larger ones the persistent one-CTA-per-SM
-// kernel; the split depends on the layout only, so every shard and every
-// evaluation make the same choice.
+// (largest first).  Under the default schedule every block whose two panels
+// fit the multi-CTA streamed kernel's shared memory (M up to ~780) runs that
+// kernel (several blocks per SM, so their pivot chains overlap); larger ones
+// run the persistent one-CTA-per-SM kernel on a global slab.  The split
+// depends on the layout only, so every shard and every evaluation make the
+// same choice.
 static int plan_launches(bv_handle *h)
 {
     cudaDeviceProp prop;
@@ -443,12 +437,26 @@ static int plan_launches(bv_handle *h)
         if (rc) return rc;
     }
     const int sched = h->opts.schedule;
-    if (sched == BV_SCHED_STREAMED)
-        h->lean_max_m = h->max_m;
-    else if (sched == BV_SCHED_AUTO && h->opts.precision == BV_PREC_FP64)
-        h->lean_max_m = kLeanMaxM;
+    // The multi-CTA streamed kernel takes every block whose panels fit its
+    // shared memory (by default and under BV_SCHED_STREAMED); the mixed
+    // path's FP64 fallback and BV_SCHED_PERSISTENT / BUCKETED keep the
+    // persistent kernel.
+    int lean_limit = 0;
+    {
+        int optin = 0;
+        BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+        cudaFuncAttributes fa;
+        BV_CUDA_TRY(cudaFuncGetAttributes(&fa, kLeanVariants[2].kernel));
+        lean_limit = big_max_m_for_bytes((size_t)optin - fa.sharedSizeBytes, 64, h->nz, 0);
+    }
+    if ((sched == BV_SCHED_STREAMED || sched == BV_SCHED_AUTO) && h->opts.precision == BV_PREC_FP64)
+        h->lean_max_m = lean_limit;
     else
         h->lean_max_m = 0;
+    if (sched == BV_SCHED_STREAMED && h->max_m > lean_limit) {
+        set_error("plan: blocks of M = %d exceed the streamed schedule's limit %d", h->max_m, lean_limit);
+        return BV_E_TOOLARGE;
+    }
     int split = 0;  // order positions [split, owned) take the streamed kernel
     while (split < h->owned && order_m(h, split) > h->lean_max_m) ++split;
     h->launches.clear();
@@ -843,6 +851,9 @@ static int eval_locked(bv_handle *h, const double *theta, double *llk)
     s.nonfinite = r.nonfinite;
     s.flags_or = r.flags_or;
     s.failed = r.failed;
+    // FP64: the fused launches and the reduction; mixed: probe, decision,
+    // mixed pass, FP64 fallback pass and the reduction.
+    s.launches = h->opts.precision == BV_PREC_MIXED ? 5 : (int)h->launches.size() + 1;
     s.llk = r.llk;
     s.device_ms = ms;
     s.kernel_ms = kms;

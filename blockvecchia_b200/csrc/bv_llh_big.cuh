@@ -86,12 +86,12 @@ __host__ __device__ inline BigLayout big_layout(int M, int rc = kBigRC, int nz =
 }
 
 // Largest M whose streamed-path layout fits in `bytes` of dynamic shared memory.
-inline int big_max_m_for_bytes(size_t bytes, int rc = kBigRC, int nz = 0)
+inline int big_max_m_for_bytes(size_t bytes, int rc = kBigRC, int nz = 0, int ns = kBigStages)
 {
     int lo = 1, hi = 8192;
     while (lo < hi) {
         const int mid = (lo + hi + 1) / 2;
-        if (big_layout(mid, rc, nz).total <= bytes)
+        if (big_layout(mid, rc, nz, ns).total <= bytes)
             lo = mid;
         else
             hi = mid - 1;

@@ -92,17 +92,18 @@ typedef struct {
     int on_failure;    /* BV_FAIL_NEGINF | BV_FAIL_CONTINUE                   */
     int print_iter;    /* print the reference's per-evaluation line           */
     int use_graph;     /* capture one evaluation in a CUDA graph (default 1)  */
-    int schedule;      /* BV_SCHED_AUTO (default): blocks up to a size limit
-                          (M = cs + bs <= 200) on the multi-CTA streamed
-                          kernel, the larger ones on the persistent
-                          one-CTA-per-SM kernel; BV_SCHED_BUCKETED: the
-                          persistent kernel, one launch per size bucket (the
-                          comparison baseline); BV_SCHED_PERSISTENT: the
-                          persistent kernel for every block;
-                          BV_SCHED_STREAMED: the multi-CTA streamed kernel
-                          for every block.  The two kernels round
-                          differently; each choice depends on the layout
-                          only, so results are reproducible.                 */
+    int schedule;      /* BV_SCHED_AUTO (default): every block whose panels
+                          fit (M = cs + bs up to ~780) on the multi-CTA
+                          streamed kernel (several blocks per SM), larger
+                          ones on the persistent one-CTA-per-SM kernel;
+                          BV_SCHED_BUCKETED: the persistent kernel, one
+                          launch per size bucket (the comparison baseline);
+                          BV_SCHED_PERSISTENT: the persistent kernel for
+                          every block (the server's algorithm);
+                          BV_SCHED_STREAMED: the streamed kernel for every
+                          block (an error if one does not fit).  The two
+                          kernels round differently; each choice depends on
+                          the layout only, so results are reproducible.    */
     double mixed_tol;  /* mixed path: a block is accepted when the estimated
                           relative error of its refined Sigma22^-1 Sigma21
                           (|dX_last| / |X| times the first step's
@@ -137,6 +138,7 @@ typedef struct {
     int failed;          /* blocks with a failed pivot in either factor
                             (cond_fail and schur_fail may count one block
                             twice; this counts it once)                      */
+    int launches;        /* kernel launches per evaluation                   */
 } bv_status;
 
 typedef struct bv_handle bv_handle;

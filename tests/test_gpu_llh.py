@@ -213,13 +213,14 @@ def test_handles_with_different_block_sizes_coexist(bvlib, oracle, golden_layout
 ])
 @pytest.mark.parametrize("path", ["streamed", "slab", "auto"])
 def test_large_blocks(bvlib, oracle, n, bc, cs, theta, path):
-    """Blocks larger than one SM's shared memory, by both large-block paths,
-    against the oracle at the FP64 parity bound."""
+    """Blocks larger than one SM's shared memory on the persistent kernel, by
+    both of its large-block paths, against the oracle at the FP64 parity
+    bound (the default schedule's streamed kernel is covered by _check)."""
     L = _gen(bvlib, n, bc, cs)
     assert int(L.batchNum.max()) + cs > 236
     P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, L.knn_idx, L.cs)
     ref, pb = oracle.llh(P, theta, per_block=True)
-    with bvlib.LlhData(L, large_blocks=path) as D:
+    with bvlib.LlhData(L, large_blocks=path, schedule="persistent") as D:
         v = D(theta)
         st = D.status()
         bl = D.block_llk()
@@ -234,8 +235,8 @@ def test_large_blocks_deterministic_and_served(bvlib):
     blocks) is deterministic and the server gives the same bits."""
     L = _gen(bvlib, 8000, 400, 300, seed=2)
     th = (1.0, 0.08, 1.5)
-    with bvlib.LlhData(L, on_failure="continue") as D, \
-            bvlib.LlhData(L, on_failure="continue", use_graph=False) as E:
+    with bvlib.LlhData(L, on_failure="continue", schedule="persistent") as D, \
+            bvlib.LlhData(L, on_failure="continue", use_graph=False, schedule="persistent") as E:
         v = [D(th) for _ in range(2)] + [E(th)]
     assert v[0] == v[1] == v[2]
     with bvlib.Server(on_failure="continue") as srv:
