@@ -606,10 +606,10 @@ def run_ours(args):
         "e2e": {"value": args.steps / (ms_e2e / 1e3), "unit": "evals/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": 48},
         "roofline": {"bound": "tensor", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
-                     "frac": achieved_tf / peak_tf, "traffic": traffic_per_launch(L),
+                     "frac": achieved_tf / peak_tf, "traffic": traffic_per_launch(st),
                      "peak_source": "FP64 DGEMM 8192^3 (cuBLAS via torch) measured in this run; "
                                     "MEASURED_PEAKS.json has no FP64 figure",
-                     "kernel": "llh_fp64_kernel (fused Matern + augmented Cholesky, mma.sync f64)",
+                     "kernel": kernel_name(st),
                      "flops_per_launch": my_flops, "kernel_ms_per_launch": kernel_ms / args.steps},
         "cpu_baseline": cpu,
         "parity_vs_oracle": parity,
@@ -625,16 +625,34 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def traffic_per_launch(L):
+def kernel_name(st):
+    """The fused kernel(s) the evaluation ran, from the library's split."""
+    bc = int(st["blocks"])
+    lean = "llh_lean_kernel_t (multi-CTA streamed: fused Matern + augmented Cholesky, mma.sync f64)"
+    pers = "llh_fp64_kernel_t (persistent: fused Matern + augmented Cholesky, mma.sync f64)"
+    n = int(st.get("streamed_blocks", 0))
+    if n == bc:
+        return lean
+    if n == 0:
+        return pers
+    return f"{lean} for {n} blocks + {pers} for {bc - n}"
+
+
+def traffic_per_launch(st):
     """DRAM bytes per launch of the fused kernel from the committed ncu
-    summary (profiles/llh_fp64_kernel.json: bytes per block measured on a
-    smaller case), scaled by blocks; None when absent."""
-    p = os.path.join(ROOT, "profiles", "llh_fp64_kernel.json")
+    summary of the kernel that ran (profiles/<kernel>.json: bytes per block
+    measured on a smaller case), scaled by blocks; None when absent or when
+    the evaluation split its blocks over both kernels."""
+    n, bc = int(st.get("streamed_blocks", 0)), int(st["blocks"])
+    name = "llh_lean_kernel" if n == bc else ("llh_fp64_kernel" if n == 0 else None)
+    if name is None:
+        return None
+    p = os.path.join(ROOT, "profiles", name + ".json")
     if not os.path.exists(p):
         return None
     try:
         d = json.load(open(p))
-        return float(d["dram_bytes_per_block"]) * int(L.bc)
+        return float(d["dram_bytes_per_block"]) * bc
     except Exception:
         return None
 

@@ -102,7 +102,7 @@ class BvStatus(C.Structure):
     _fields_ = [("blocks", C.c_int), ("cond_fail", C.c_int), ("schur_fail", C.c_int),
                 ("fp32_fallback", C.c_int), ("nonfinite", C.c_int), ("flags_or", C.c_uint),
                 ("llk", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double),
-                ("failed", C.c_int), ("launches", C.c_int)]
+                ("failed", C.c_int), ("launches", C.c_int), ("streamed_blocks", C.c_int)]
 
 
 class BvJobOpts(C.Structure):

@@ -167,6 +167,7 @@ struct bv_handle {
     size_t slab_stride = 0;
     double *d_slab_lean = nullptr;  // per-CTA slabs of the multi-CTA streamed launch
     int lean_max_m = 0;             // blocks with M <= this run the multi-CTA streamed kernel
+    int streamed_blocks = 0;        // of the owned blocks, how many that is
     MaternParams *d_mp = nullptr;
     EvalResult *d_res = nullptr;
     MixedWork mixed;  // mixed-precision scratch (bv_llh_mixed.cuh)
@@ -459,6 +460,7 @@ static int plan_launches(bv_handle *h)
     }
     int split = 0;  // order positions [split, owned) take the streamed kernel
     while (split < h->owned && order_m(h, split) > h->lean_max_m) ++split;
+    h->streamed_blocks = h->owned - split;
     h->launches.clear();
     h->smem_max_m = std::min(cap_m, h->max_m);
     // The cap is per kernel, not per handle: set it to what the device allows
@@ -854,6 +856,7 @@ static int eval_locked(bv_handle *h, const double *theta, double *llk)
     // FP64: the fused launches and the reduction; mixed: probe, decision,
     // mixed pass, FP64 fallback pass and the reduction.
     s.launches = h->opts.precision == BV_PREC_MIXED ? 5 : (int)h->launches.size() + 1;
+    s.streamed_blocks = h->opts.precision == BV_PREC_MIXED ? 0 : h->streamed_blocks;
     s.llk = r.llk;
     s.device_ms = ms;
     s.kernel_ms = kms;

@@ -139,6 +139,9 @@ typedef struct {
                             (cond_fail and schur_fail may count one block
                             twice; this counts it once)                      */
     int launches;        /* kernel launches per evaluation                   */
+    int streamed_blocks; /* FP64 path: blocks on the multi-CTA streamed
+                            kernel (the rest on the persistent kernel);
+                            0 for the mixed path                             */
 } bv_status;
 
 typedef struct bv_handle bv_handle;

@@ -29,8 +29,9 @@ def _blocks(oracle, L, th):
 
 
 def _check(bv, oracle, L, thetas=THETAS, schedules=("auto", "persistent"), **kw):
-    """Both kernels: the default schedule (blocks with M <= 200 on the
-    multi-CTA streamed kernel) and the persistent kernel for every block."""
+    """Both kernels: the default schedule (every block whose panels fit in
+    shared memory on the multi-CTA streamed kernel, larger ones on the
+    persistent kernel) and the persistent kernel for every block."""
     for sched in schedules:
         with bv.LlhData(L, schedule=sched, **kw) as D:
             for th in thetas:
