@@ -43,6 +43,20 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+
+def finite_json(o):
+    """JSON text of o with every non-finite float written as null (strict
+    JSON has no NaN or Infinity)."""
+    def clean(v):
+        if isinstance(v, float) and not math.isfinite(v):
+            return None
+        if isinstance(v, dict):
+            return {k: clean(x) for k, x in v.items()}
+        if isinstance(v, (list, tuple)):
+            return [clean(x) for x in v]
+        return v
+    return json.dumps(clean(o))
+
 METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] \
     if os.path.exists(os.path.join(ROOT, "BASELINE.json")) else \
     "loglik evals/s n=1M cs=200, mixed vs FP64 at rel err<=1e-8; serve p50/p99 ms"
@@ -619,7 +633,7 @@ def run_ours(args):
         "mixed": mixed,
         "serve": serve,
     }
-    print(json.dumps(out))
+    print(finite_json(out))
     D.close()
     if world > 1:
         dist.destroy_process_group()
@@ -717,10 +731,13 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "llk": llk,
+        # Blocks whose LAPACK potrf fails make the OpenBLAS evaluation NaN
+        # (the device path zeroes the failed pivot and goes on).
+        "llk": llk if np.isfinite(llk) else None,
+        "llk_note": None if np.isfinite(llk) else "not finite: some blocks' potrf failed",
         "setup": {"layout": d["source"], "knn_oracle_s": round(knn_s, 1)},
     }
-    print(json.dumps(out))
+    print(finite_json(out))
 
 
 # ------------------------------------------------------------------ serving
@@ -875,7 +892,7 @@ def run_serve(args):
         "clocks": r.pop("clocks"),
     }
     out.update({k: v for k, v in r.items() if k not in ("workload", "total_points")})
-    print(json.dumps(out))
+    print(finite_json(out))
 
 
 def main():

@@ -63,6 +63,12 @@ EXPORTS = {
     "bv_generate_xyt": (C.c_int, [C.c_int, C.c_int, C.c_int, _D, _D, _D]),
     "bv_layout_build3": (C.c_int, [_D, _D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.c_int, _I, _I, _D, _D, _D, _D, _D, _D, _D, _I, _I]),
+    "bv_layout_build_ex": (C.c_int, [_D, _D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     C.c_int, C.c_int, _I, _I, _D, _D, _D, _D, _D, _D, _D, _I, _I]),
+    "bv_layout_from_clusters_ex": (C.c_int, [_D, _D, _D, _D, C.c_int, C.c_int, _I, _D, _D, _D,
+                                             C.c_int, C.c_int, _I, _I, _D, _D, _D, _D, _D, _D, _D,
+                                             _I, _I]),
+    "bv_order_centroids": (C.c_int, [C.c_int, C.c_int, _D, _D, _D]),
     "bv_shard_blocks": (C.c_int, [_I, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_ubyte)]),
     "bv_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "bv_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -52,25 +53,25 @@ def build(clean: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     if clean and os.path.isdir(BUILD):
         shutil.rmtree(BUILD)
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
-    changed = False
+    objs, jobs = [], []
     for s in CU_SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(BUILD, s + ".o")
         if _stale(obj, src) or ptxas_v:
-            cmd = [NVCC] + NVFLAGS + (["-Xptxas", "-v"] if ptxas_v else []) + ["-c", src, "-o", obj]
-            r = _run(cmd)
-            if verbose or ptxas_v:
-                sys.stdout.write(r.stdout + r.stderr)
-            changed = True
+            jobs.append([NVCC] + NVFLAGS + (["-Xptxas", "-v"] if ptxas_v else []) + ["-c", src, "-o", obj])
         objs.append(obj)
     for s in CPP_SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(BUILD, s + ".o")
         if _stale(obj, src):
-            _run([CXX] + CXXFLAGS + ["-c", src, "-o", obj])
-            changed = True
+            jobs.append([CXX] + CXXFLAGS + ["-c", src, "-o", obj])
         objs.append(obj)
+    # The translation units compile independently: all at once.
+    with ThreadPoolExecutor(max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for r in ex.map(_run, jobs):
+            if verbose or ptxas_v:
+                sys.stdout.write(r.stdout + r.stderr)
+    changed = bool(jobs)
     if changed or not os.path.exists(LIB):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"])
         changed = True

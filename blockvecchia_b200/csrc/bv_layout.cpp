@@ -2,8 +2,9 @@
 //
 // Produces the layout the reference's driver builds before optimisation
 // (src/test_Xvecchia_batch.cpp:240-352): locations, k-means clusters, a
-// random centroid order, block 0 merged until it holds >= cs points, blocks
-// of ascending original point index.  The reference's steps are O(n*bc)
+// centroid order (random by default; Morton, kd-tree, Hilbert or
+// maximum-minimum distance), block 0 merged until it holds >= cs points,
+// blocks of ascending original point index.  The reference's steps are O(n*bc)
 // (cluster_to_batch, include/vecchia_helper_method.h:63-92), O(bc^2)
 // (reorderIndex :128-160) and O(n*bc*epochs) (kmean_par, src/kmeans.cpp:59-145);
 // here the same results come from bucketing, hashing and a uniform-grid exact
@@ -57,6 +58,20 @@ inline double kdist3(double px, double py, double pz, double cx, double cy, doub
 {
     const double d0 = px - cx, d1 = py - cy, d2 = pz - cz;
     return std::fma(d2, d2, std::fma(d1, d1, d0 * d0));
+}
+
+// Squared distance as reorderIndex writes it (include/vecchia_helper_method.h:
+// 138-144: dx*dx + dy*dy, then += dz*dz), contracted by the same build as
+// fma(dx, dx, dy*dy) and fma(dz, dz, that).
+inline double rdist(double px, double py, double cx, double cy)
+{
+    const double dx = px - cx, dy = py - cy;
+    return std::fma(dx, dx, dy * dy);
+}
+inline double rdist3(double px, double py, double pz, double cx, double cy, double cz)
+{
+    const double dz = pz - cz;
+    return std::fma(dz, dz, rdist(px, py, cx, cy));
 }
 
 // Bit patterns of a point's coordinates, for exact-equality hashing.
@@ -130,6 +145,9 @@ struct CentroidGrid {
     }
     // Nearest centroid of (px, py[, pz]); the grid is over (x, y), whose
     // distance bounds the 3-D one from below, so the search stays exact.
+    // kReorder: the squared distance as reorderIndex evaluates it instead of
+    // the k-means one.
+    template <bool kReorder = false>
     int nearest(double px, double py, const std::vector<double> &cx,
                 const std::vector<double> &cy, double pz = 0.0,
                 const std::vector<double> *cz = nullptr) const
@@ -149,8 +167,11 @@ struct CentroidGrid {
             const int cidx = yy * G + xx;
             for (int q = start[cidx]; q < start[cidx + 1]; ++q) {
                 const int c = items[q];
-                const double d = cz ? kdist3(px, py, pz, cx[c], cy[c], (*cz)[c])
-                                    : kdist(px, py, cx[c], cy[c]);
+                double d;
+                if constexpr (kReorder)
+                    d = cz ? rdist3(px, py, pz, cx[c], cy[c], (*cz)[c]) : rdist(px, py, cx[c], cy[c]);
+                else
+                    d = cz ? kdist3(px, py, pz, cx[c], cy[c], (*cz)[c]) : kdist(px, py, cx[c], cy[c]);
                 if (d < best || (d == best && c < bi)) {
                     best = d;
                     bi = c;
@@ -178,6 +199,341 @@ struct CentroidGrid {
         return bi;
     }
 };
+
+// ------------------------------------------------------- centroid orderings
+// The reference's --permutation choices (src/test_Xvecchia_batch.cpp:286-314),
+// each rewriting the centroid coordinates in place in its order: random
+// (include/ckernel.h:177-202, 3-D :811-840), Morton (:148-174, 3-D :842-868),
+// kd-tree (:205-300, 3-D :725-935), Hilbert (:326-432, 3-D :582-705 and
+// :870-895) and maximum-minimum distance (:435-523, 3-D :937-1000).  Morton
+// and Hilbert leave the coordinates quantised to k / 65535, as there.
+
+// 16-bit quantisation (uint16_t)(v * 65535 + .5), the product and the sum
+// contracted into one fma by the reference's build.  Coordinates outside
+// [0, 1] have no defined quantisation there; they are rejected here.
+inline bool quant16(double v, uint16_t &q)
+{
+    if (!(v >= 0.0 && v <= 1.0)) return false;
+    q = (uint16_t)std::fma(v, 65535.0, 0.5);
+    return true;
+}
+
+// Bit b of v to bit 4b (Morton 3-D keys: x at 4b, y at 4b+1, z at 4b+2) and
+// back; bit b to bit 3b (Hilbert 3-D keys) and back.
+uint64_t spread16_by4(uint64_t v)
+{
+    uint64_t r = 0;
+    for (int b = 0; b < 16; ++b) r |= ((v >> b) & 1ull) << (4 * b);
+    return r;
+}
+uint64_t gather16_by4(uint64_t v)
+{
+    uint64_t r = 0;
+    for (int b = 0; b < 16; ++b) r |= ((v >> (4 * b)) & 1ull) << b;
+    return r;
+}
+uint64_t spread16_by3(uint64_t v)
+{
+    uint64_t r = 0;
+    for (int b = 0; b < 16; ++b) r |= ((v >> b) & 1ull) << (3 * b);
+    return r;
+}
+uint64_t gather16_by3(uint64_t v)
+{
+    uint64_t r = 0;
+    for (int b = 0; b < 16; ++b) r |= ((v >> (3 * b)) & 1ull) << b;
+    return r;
+}
+
+// The reference's Hilbert transforms, as its code computes them (they are
+// not the textbook transform: in the first coordinate's step the branch
+// without the bit swaps x with itself, i.e. does nothing, and the decoder
+// below does not invert the encoder).  Keys interleave the transformed
+// coordinates most significant bit first, x ahead of y (ahead of z).
+uint32_t hilbert2_key(uint32_t x, uint32_t y)
+{
+    for (uint32_t q = 1u << 15; q > 1; q >>= 1) {
+        const uint32_t p = q - 1;
+        if (x & q) x ^= p;
+        if (y & q) {
+            x ^= p;
+        } else {
+            const uint32_t t = (x ^ y) & p;
+            x ^= t;
+            y ^= t;
+        }
+    }
+    y ^= x;
+    uint32_t t = 0;
+    for (uint32_t q = 1u << 15; q > 1; q >>= 1)
+        if (y & q) t ^= q - 1;
+    x ^= t;
+    y ^= t;
+    return (spread16(x & 0xffffu) << 1) | spread16(y & 0xffffu);
+}
+void hilbert2_point(uint32_t key, uint16_t &ox, uint16_t &oy)
+{
+    uint32_t x = gather16(key >> 1), y = gather16(key);
+    const uint32_t t0 = y >> 1;
+    y ^= x;
+    x ^= t0;
+    for (uint32_t q = 2; q != (1u << 16); q <<= 1) {
+        const uint32_t p = q - 1;
+        if (y & q) {
+            x ^= p;
+        } else {
+            const uint32_t t = (x ^ y) & p;
+            x ^= t;
+            y ^= t;
+        }
+        if (x & q) x ^= p;
+    }
+    ox = (uint16_t)x;
+    oy = (uint16_t)y;
+}
+uint64_t hilbert3_key(uint64_t x, uint64_t y, uint64_t z)
+{
+    for (uint64_t q = 1u << 15; q > 1; q >>= 1) {
+        const uint64_t p = q - 1;
+        if (x & q) x ^= p;
+        if (y & q) {
+            x ^= p;
+        } else {
+            const uint64_t t = (x ^ y) & p;
+            x ^= t;
+            y ^= t;
+        }
+        if (z & q) {
+            x ^= p;
+        } else {
+            const uint64_t t = (x ^ z) & p;
+            x ^= t;
+            z ^= t;
+        }
+    }
+    y ^= x;
+    z ^= y;
+    uint64_t t = 0;
+    for (uint64_t q = 1u << 15; q > 1; q >>= 1)
+        if (z & q) t ^= q - 1;
+    x ^= t;
+    y ^= t;
+    z ^= t;
+    return (spread16_by3(x & 0xffffu) << 2) | (spread16_by3(y & 0xffffu) << 1) |
+           spread16_by3(z & 0xffffu);
+}
+void hilbert3_point(uint64_t key, uint16_t &ox, uint16_t &oy, uint16_t &oz)
+{
+    uint64_t x = gather16_by3(key >> 2), y = gather16_by3(key >> 1), z = gather16_by3(key);
+    const uint64_t t0 = z >> 1;
+    z ^= y;
+    y ^= x;
+    x ^= t0;
+    for (uint64_t q = 2; q != (1ull << 16); q <<= 1) {
+        const uint64_t p = q - 1;
+        if (z & q) {
+            x ^= p;
+        } else {
+            const uint64_t t = (x ^ z) & p;
+            x ^= t;
+            z ^= t;
+        }
+        if (y & q) {
+            x ^= p;
+        } else {
+            const uint64_t t = (x ^ y) & p;
+            x ^= t;
+            y ^= t;
+        }
+        if (x & q) x ^= p;
+    }
+    ox = (uint16_t)x;
+    oy = (uint16_t)y;
+    oz = (uint16_t)z;
+}
+
+// kd-tree order: sort by x (depth 0), split at len / 2, recurse on both
+// halves with the next axis (y, then z in 3-D), and read the leaves left to
+// right -- which is the array after the recursive sorts.  The sorts are
+// glibc's qsort on records of the reference's shape (coordinates plus an
+// unused weight), so that records with equal keys end in the same order.
+struct KdRec2 {
+    double x, y, w;
+};
+struct KdRec3 {
+    double x, y, z, w;
+};
+template <typename R, int kAxis>
+int kd_cmp(const void *a, const void *b)
+{
+    const double u = reinterpret_cast<const double *>(a)[kAxis];
+    const double v = reinterpret_cast<const double *>(b)[kAxis];
+    return u < v ? -1 : (u == v ? 0 : 1);
+}
+template <typename R, int kDims>
+void kd_order(R *d, int len, int depth)
+{
+    if (len <= 1) return;
+    const int axis = depth % kDims;
+    qsort(d, (size_t)len, sizeof(R), axis == 0 ? kd_cmp<R, 0> : (axis == 1 ? kd_cmp<R, 1> : kd_cmp<R, 2>));
+    const int mid = len / 2;
+    kd_order<R, kDims>(d, mid, depth + 1);
+    kd_order<R, kDims>(d + mid, len - mid, depth + 1);
+}
+
+// Maximum-minimum distance order: the centroid nearest the mean first (the
+// first strictly below the cap), then repeatedly the one whose distance to
+// the chosen set is largest (first strict maximum; distances capped at 2,
+// 3 in 3-D), the last one remaining at the end.  The reference recomputes
+// every minimum over the chosen set at each step (O(n^3)); the running
+// minimum kept here takes the same values in O(n^2).  Squared distances as
+// its pow(d, 2) sums compile: fma(dx, dx, dy*dy) (and fma(dz, dz, .)).
+int mmd_order(int n, double *x, double *y, double *z)
+{
+    const double cap = z ? 3.0 : 2.0;
+    double xm = 0, ym = 0, zm = 0;
+    for (int i = 0; i < n; ++i) {
+        xm = xm + x[i];
+        ym = ym + y[i];
+        if (z) zm = zm + z[i];
+    }
+    xm = xm / n;
+    ym = ym / n;
+    if (z) zm = zm / n;
+    auto d2 = [&](double ax, double ay, double az, double bx, double by, double bz) {
+        return z ? rdist3(ax, ay, az, bx, by, bz) : rdist(ax, ay, bx, by);
+    };
+    std::vector<int> res(n), flag(n, 0);
+    double best = cap;
+    int first = -1;
+    for (int i = 0; i < n; ++i) {
+        const double d = d2(x[i], y[i], z ? z[i] : 0.0, xm, ym, zm);
+        if (d < best) {
+            best = d;
+            first = i;
+        }
+    }
+    if (first < 0) return BV_E_INVALID;  // no centroid within the cap of the mean
+    res[0] = first;
+    flag[first] = 1;
+    std::vector<double> mind(n, cap);
+    for (int j = 1; j < n - 1; ++j) {
+        const int r = res[j - 1];
+        double mx = 0.0;
+        int arg = n;
+        for (int i = 0; i < n; ++i) {
+            if (flag[i]) continue;
+            const double d = d2(x[i], y[i], z ? z[i] : 0.0, x[r], y[r], z ? z[r] : 0.0);
+            if (d < mind[i]) mind[i] = d;
+            if (mx < mind[i]) {
+                mx = mind[i];
+                arg = i;
+            }
+        }
+        if (arg == n) return BV_E_INVALID;  // the rest coincide with chosen centroids
+        res[j] = arg;
+        flag[arg] = 1;
+    }
+    if (n > 1)
+        for (int i = 0; i < n; ++i)
+            if (!flag[i]) res[n - 1] = i;
+    std::vector<double> ox(n), oy(n), oz(z ? n : 0);
+    for (int i = 0; i < n; ++i) {
+        ox[i] = x[res[i]];
+        oy[i] = y[res[i]];
+        if (z) oz[i] = z[res[i]];
+    }
+    std::memcpy(x, ox.data(), sizeof(double) * n);
+    std::memcpy(y, oy.data(), sizeof(double) * n);
+    if (z) std::memcpy(z, oz.data(), sizeof(double) * n);
+    return BV_OK;
+}
+
+// The ordering named by `ordering` (BV_ORDER_*), in place; z = NULL: 2-D.
+int order_centroids(int ordering, int n, double *x, double *y, double *z)
+{
+    switch (ordering) {
+    case BV_ORDER_RANDOM:
+        srand(42);
+        for (int i = n - 1; i > 0; --i) {
+            const int j = rand() % (i + 1);
+            std::swap(x[i], x[j]);
+            std::swap(y[i], y[j]);
+            if (z) std::swap(z[i], z[j]);
+        }
+        return BV_OK;
+    case BV_ORDER_MORTON:
+    case BV_ORDER_HILBERT: {
+        const bool hil = ordering == BV_ORDER_HILBERT;
+        std::vector<uint64_t> key(n);
+        for (int i = 0; i < n; ++i) {
+            uint16_t qx, qy, qz = 0;
+            if (!quant16(x[i], qx) || !quant16(y[i], qy) || (z && !quant16(z[i], qz))) {
+                bv::set_error("%s ordering: centroid %d lies outside the unit %s",
+                              hil ? "Hilbert" : "Morton", i, z ? "cube" : "square");
+                return BV_E_INVALID;
+            }
+            if (z)
+                key[i] = hil ? hilbert3_key(qx, qy, qz)
+                             : (spread16_by4(qz) << 2) + (spread16_by4(qy) << 1) + spread16_by4(qx);
+            else
+                key[i] = hil ? hilbert2_key(qx, qy) : (uint64_t)((spread16(qy) << 1) + spread16(qx));
+        }
+        // Equal keys decode to equal points: any sort gives the same arrays.
+        std::sort(key.begin(), key.end());
+        for (int i = 0; i < n; ++i) {
+            uint16_t qx, qy, qz = 0;
+            if (z && hil) {
+                hilbert3_point(key[i], qx, qy, qz);
+            } else if (z) {
+                qx = (uint16_t)gather16_by4(key[i]);
+                qy = (uint16_t)gather16_by4(key[i] >> 1);
+                qz = (uint16_t)gather16_by4(key[i] >> 2);
+            } else if (hil) {
+                hilbert2_point((uint32_t)key[i], qx, qy);
+            } else {
+                qx = (uint16_t)gather16((uint32_t)key[i]);
+                qy = (uint16_t)gather16((uint32_t)key[i] >> 1);
+            }
+            x[i] = (double)qx / (double)UINT16_MAX;
+            y[i] = (double)qy / (double)UINT16_MAX;
+            if (z) z[i] = (double)qz / (double)UINT16_MAX;
+        }
+        return BV_OK;
+    }
+    case BV_ORDER_KDTREE:
+        if (z) {
+            std::vector<KdRec3> d(n);
+            for (int i = 0; i < n; ++i) d[i] = {x[i], y[i], z[i], 0.0};
+            kd_order<KdRec3, 3>(d.data(), n, 0);
+            for (int i = 0; i < n; ++i) {
+                x[i] = d[i].x;
+                y[i] = d[i].y;
+                z[i] = d[i].z;
+            }
+        } else {
+            std::vector<KdRec2> d(n);
+            for (int i = 0; i < n; ++i) d[i] = {x[i], y[i], 0.0};
+            kd_order<KdRec2, 2>(d.data(), n, 0);
+            for (int i = 0; i < n; ++i) {
+                x[i] = d[i].x;
+                y[i] = d[i].y;
+            }
+        }
+        return BV_OK;
+    case BV_ORDER_MMD:
+        if (mmd_order(n, x, y, z)) {
+            bv::set_error("MMD ordering: no centroid within distance %s of the mean, or centroids "
+                          "that coincide (the reference's loop has no defined result there)",
+                          z ? "sqrt(3)" : "sqrt(2)");
+            return BV_E_INVALID;
+        }
+        return BV_OK;
+    default:
+        bv::set_error("unknown centroid ordering %d", ordering);
+        return BV_E_INVALID;
+    }
+}
 
 }  // namespace
 
@@ -353,7 +709,7 @@ extern "C" int bv_kmeans(const double *x, const double *y, int n, int k, int see
 static int layout_from_clusters_impl(const double *x, const double *y, const double *z,
                                      const double *obs, int n, int k, const int *labels_in,
                                      const double *ccx, const double *ccy, const double *ccz,
-                                     int cs, int *batchNum, int *batchNumAccum, double *x_new,
+                                     int cs, int ordering, int *batchNum, int *batchNumAccum, double *x_new,
                                      double *y_new, double *z_new, double *obs_new, double *cx,
                                      double *cy, double *cz, int *bc_out, int *first_cluster_count)
 {
@@ -374,35 +730,56 @@ static int layout_from_clusters_impl(const double *x, const double *y, const dou
         }
         clusterNum[labels[p]]++;
     }
-    // random_reordering (include/ckernel.h:177-202): srand(42), Fisher-Yates
-    // from the end with rand() % (i+1).
+    // The centroid ordering (random_reordering by default: srand(42),
+    // Fisher-Yates from the end with rand() % (i+1)).
     std::vector<double> px(ccx, ccx + k), py(ccy, ccy + k), pz(k, 0.0);
     if (z) pz.assign(ccz, ccz + k);
-    srand(42);
-    for (int i = k - 1; i > 0; --i) {
-        const int j = rand() % (i + 1);
-        std::swap(px[i], px[j]);
-        std::swap(py[i], py[j]);
-        std::swap(pz[i], pz[j]);
+    {
+        const int rc = order_centroids(ordering, k, px.data(), py.data(), z ? pz.data() : nullptr);
+        if (rc) return rc;
     }
-    // reorderIndex (include/vecchia_helper_method.h:128-160): index of the
-    // first original centroid at zero distance = lowest index with the same
-    // coordinates.  Where several centroids coincide (clusters of duplicated
-    // locations) the reference maps all of them to that lowest index, so one
-    // cluster's points are taken twice and the other's are lost; here the
-    // k-th shuffled occurrence of a coordinate pair maps to the k-th original
-    // with it, which is the same map whenever the centroids are distinct and
-    // otherwise puts every point in exactly one block.
-    // Coordinates compared by value (-0 and +0 are at zero distance).
-    std::unordered_map<Key3, std::vector<int>, Key3Hash> first_at;
-    first_at.reserve((size_t)k * 2);
-    for (int j = 0; j < k; ++j)  // ascending j
-        first_at[key3(ccx[j], ccy[j], z ? ccz[j] : 0.0, true)].push_back(j);
-    std::unordered_map<Key3, int, Key3Hash> taken;
     std::vector<int> perm(k);
-    for (int i = 0; i < k; ++i) {
-        const Key3 key = key3(px[i], py[i], pz[i], true);
-        perm[i] = first_at.at(key)[taken[key]++];
+    if (ordering != BV_ORDER_MORTON && ordering != BV_ORDER_HILBERT) {
+        // reorderIndex (include/vecchia_helper_method.h:128-160) after an
+        // ordering that permutes the centroids: index of the first original
+        // centroid at zero distance = lowest index with the same coordinates.
+        // Where several centroids coincide (clusters of duplicated locations)
+        // the reference maps all of them to that lowest index and stops on the
+        // repeated index; here the k-th reordered occurrence of a coordinate
+        // pair maps to the k-th original with it, which is the same map
+        // whenever the centroids are distinct and otherwise puts every point
+        // in exactly one block.  Coordinates compared by value (-0 and +0 are
+        // at zero distance).
+        std::unordered_map<Key3, std::vector<int>, Key3Hash> first_at;
+        first_at.reserve((size_t)k * 2);
+        for (int j = 0; j < k; ++j)  // ascending j
+            first_at[key3(ccx[j], ccy[j], z ? ccz[j] : 0.0, true)].push_back(j);
+        std::unordered_map<Key3, int, Key3Hash> taken;
+        for (int i = 0; i < k; ++i) {
+            const Key3 key = key3(px[i], py[i], pz[i], true);
+            perm[i] = first_at.at(key)[taken[key]++];
+        }
+    } else {
+        // reorderIndex after a quantising ordering: the nearest original
+        // centroid (lowest index among equal distances), which must be a
+        // different one for every reordered centroid (:154-159).
+        const std::vector<double> ox(ccx, ccx + k), oy(ccy, ccy + k);
+        std::vector<double> oz;
+        if (z) oz.assign(ccz, ccz + k);
+        CentroidGrid grid;
+        grid.build(ox, oy);
+        std::vector<int> seen(k, -1);
+        for (int i = 0; i < k; ++i) {
+            perm[i] = grid.nearest<true>(px[i], py[i], ox, oy, pz[i], z ? &oz : nullptr);
+            if (seen[perm[i]] >= 0) {
+                bv::set_error("bv_layout_from_clusters: the %s ordering maps centroids %d and %d to "
+                              "cluster %d (the reference stops here too)",
+                              ordering == BV_ORDER_MORTON ? "Morton" : "Hilbert", seen[perm[i]], i,
+                              perm[i]);
+                return BV_E_INVALID;
+            }
+            seen[perm[i]] = i;
+        }
     }
     // firstbatch (:95-108)
     int fcs = 0, fcc = 0, acc_sz = 0;
@@ -487,12 +864,12 @@ extern "C" int bv_layout_from_clusters(const double *x, const double *y, const d
                                        int *first_cluster_count)
 {
     return layout_from_clusters_impl(x, y, nullptr, obs, n, k, labels_in, ccx, ccy, nullptr, cs,
-                                     batchNum, batchNumAccum, x_new, y_new, nullptr, obs_new, cx,
+                                     BV_ORDER_RANDOM, batchNum, batchNumAccum, x_new, y_new, nullptr, obs_new, cx,
                                      cy, nullptr, bc_out, first_cluster_count);
 }
 
 static int layout_build_impl(const double *x, const double *y, const double *z, const double *obs,
-                             int n, int bc, int cs, int seed, int epochs, int threads,
+                             int n, int bc, int cs, int seed, int epochs, int threads, int ordering,
                              int *batchNum, int *batchNumAccum, double *x_new, double *y_new,
                              double *z_new, double *obs_new, double *cx, double *cy, double *cz,
                              int *bc_out, int *first_cluster_count)
@@ -518,7 +895,7 @@ static int layout_build_impl(const double *x, const double *y, const double *z, 
         if (rc) return rc;
     }
     return layout_from_clusters_impl(x, y, z, obs, n, k, labels.data(), ccx.data(), ccy.data(),
-                                     z ? ccz.data() : nullptr, cs, batchNum, batchNumAccum, x_new,
+                                     z ? ccz.data() : nullptr, cs, ordering, batchNum, batchNumAccum, x_new,
                                      y_new, z_new, obs_new, cx, cy, cz, bc_out,
                                      first_cluster_count);
 }
@@ -528,7 +905,8 @@ extern "C" int bv_layout_build(const double *x, const double *y, const double *o
                                int *batchNumAccum, double *x_new, double *y_new, double *obs_new,
                                double *cx, double *cy, int *bc_out, int *first_cluster_count)
 {
-    return layout_build_impl(x, y, nullptr, obs, n, bc, cs, seed, epochs, threads, batchNum,
+    return layout_build_impl(x, y, nullptr, obs, n, bc, cs, seed, epochs, threads, BV_ORDER_RANDOM,
+                             batchNum,
                              batchNumAccum, x_new, y_new, nullptr, obs_new, cx, cy, nullptr, bc_out,
                              first_cluster_count);
 }
@@ -543,7 +921,46 @@ extern "C" int bv_layout_build3(const double *x, const double *y, const double *
         bv::set_error("bv_layout_build3: z, z_new and cz are required");
         return BV_E_INVALID;
     }
-    return layout_build_impl(x, y, z, obs, n, bc, cs, seed, epochs, threads, batchNum,
+    return layout_build_impl(x, y, z, obs, n, bc, cs, seed, epochs, threads, BV_ORDER_RANDOM,
+                             batchNum,
                              batchNumAccum, x_new, y_new, z_new, obs_new, cx, cy, cz, bc_out,
                              first_cluster_count);
+}
+
+extern "C" int bv_layout_build_ex(const double *x, const double *y, const double *z,
+                                  const double *obs, int n, int bc, int cs, int seed, int epochs,
+                                  int threads, int ordering, int *batchNum, int *batchNumAccum,
+                                  double *x_new, double *y_new, double *z_new, double *obs_new,
+                                  double *cx, double *cy, double *cz, int *bc_out,
+                                  int *first_cluster_count)
+{
+    if (z && (!z_new || !cz)) {
+        bv::set_error("bv_layout_build_ex: z needs z_new and cz");
+        return BV_E_INVALID;
+    }
+    return layout_build_impl(x, y, z, obs, n, bc, cs, seed, epochs, threads, ordering, batchNum,
+                             batchNumAccum, x_new, y_new, z_new, obs_new, cx, cy, cz, bc_out,
+                             first_cluster_count);
+}
+
+extern "C" int bv_layout_from_clusters_ex(const double *x, const double *y, const double *z,
+                                          const double *obs, int n, int k, const int *labels,
+                                          const double *ccx, const double *ccy, const double *ccz,
+                                          int cs, int ordering, int *batchNum, int *batchNumAccum,
+                                          double *x_new, double *y_new, double *z_new,
+                                          double *obs_new, double *cx, double *cy, double *cz,
+                                          int *bc_out, int *first_cluster_count)
+{
+    return layout_from_clusters_impl(x, y, z, obs, n, k, labels, ccx, ccy, ccz, cs, ordering,
+                                     batchNum, batchNumAccum, x_new, y_new, z_new, obs_new, cx, cy,
+                                     cz, bc_out, first_cluster_count);
+}
+
+extern "C" int bv_order_centroids(int ordering, int n, double *x, double *y, double *z)
+{
+    if (n <= 0 || !x || !y) {
+        bv::set_error("bv_order_centroids: invalid argument");
+        return BV_E_INVALID;
+    }
+    return order_centroids(ordering, n, x, y, z);
 }

@@ -93,67 +93,87 @@ def kmeans(x, y, k: int, seed: int = 0, epochs: int = 50, threads: int = 0):
     return labels, cx, cy
 
 
-def layout_from_clusters(x, y, obs, labels, ccx, ccy, cs: int) -> Layout:
+ORDERINGS = {"random": 0, "morton": 1, "kdtree": 2, "hilbert": 3, "mmd": 4}
+
+
+def _ordering(ordering) -> int:
+    if isinstance(ordering, str):
+        if ordering not in ORDERINGS:
+            raise ValueError(f"ordering must be one of {sorted(ORDERINGS)}")
+        return ORDERINGS[ordering]
+    return int(ordering)
+
+
+def layout_from_clusters(x, y, obs, labels, ccx, ccy, cs: int, z=None, ccz=None,
+                         ordering="random") -> Layout:
+    """The layout steps after clustering (labels per point, centroids)."""
     x, y, obs = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, obs))
     labels = np.ascontiguousarray(labels, dtype=np.int32)
     ccx = np.ascontiguousarray(ccx, dtype=np.float64)
     ccy = np.ascontiguousarray(ccy, dtype=np.float64)
+    zc = None if z is None else np.ascontiguousarray(z, dtype=np.float64)
+    cczc = None if ccz is None else np.ascontiguousarray(ccz, dtype=np.float64)
     n, k = len(x), len(ccx)
     bn = np.zeros(k, dtype=np.int32)
     acc = np.zeros(k + 1, dtype=np.int32)
     xn, yn, on = np.zeros(n), np.zeros(n), np.zeros(n)
     cx, cy = np.zeros(k), np.zeros(k)
+    zn = np.zeros(n) if zc is not None else None
+    cz = np.zeros(k) if zc is not None else None
+    nd = C.POINTER(C.c_double)()
+    opt = lambda a: dp(a) if a is not None else nd  # noqa: E731
     bc = C.c_int(0)
     fcc = C.c_int(0)
-    check(lib().bv_layout_from_clusters(dp(x), dp(y), dp(obs), n, k, ip(labels), dp(ccx), dp(ccy),
-                                        int(cs), ip(bn), ip(acc), dp(xn), dp(yn), dp(on), dp(cx),
-                                        dp(cy), C.byref(bc), C.byref(fcc)))
+    check(lib().bv_layout_from_clusters_ex(dp(x), dp(y), opt(zc), dp(obs), n, k, ip(labels), dp(ccx),
+                                           dp(ccy), opt(cczc), int(cs), _ordering(ordering), ip(bn),
+                                           ip(acc), dp(xn), dp(yn), opt(zn), dp(on), dp(cx), dp(cy),
+                                           opt(cz), C.byref(bc), C.byref(fcc)))
     b = bc.value
     return Layout(bn[:b].copy(), acc[:b + 1].copy(), xn, yn, on, int(cs), cx[:b].copy(),
-                  cy[:b].copy(), None, fcc.value)
+                  cy[:b].copy(), None, fcc.value, z=zn,
+                  cz=cz[:b].copy() if cz is not None else None)
 
 
 def build_layout(x, y, obs, bc: int, cs: int, seed: int = 0, epochs: int = 50,
-                 threads: int = 0, z=None) -> Layout:
+                 threads: int = 0, z=None, ordering="random") -> Layout:
     """The driver's setup: classic Vecchia if n < 2*bc, else k-means; then the
-    random centroid order, first-block merge and block reordering.  With z
-    (a third coordinate: time or depth) every step is the reference's
-    time_flag variant."""
-    if z is not None:
-        return _build_layout3(x, y, z, obs, bc, cs, seed, epochs, threads)
-    x, y, obs = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, obs))
+    centroid order (the reference's --permutation: random, morton, kdtree,
+    hilbert or mmd), first-block merge and block reordering.  With z (a third
+    coordinate: time or depth) every step is the reference's time_flag
+    variant."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, obs)]
+    x, y, obs = arrs
+    zc = None if z is None else np.ascontiguousarray(z, dtype=np.float64)
     n = len(x)
     k = n if n < 2 * bc else bc
     bn = np.zeros(k, dtype=np.int32)
     acc = np.zeros(k + 1, dtype=np.int32)
     xn, yn, on = np.zeros(n), np.zeros(n), np.zeros(n)
     cx, cy = np.zeros(k), np.zeros(k)
+    zn = np.zeros(n) if zc is not None else None
+    cz = np.zeros(k) if zc is not None else None
+    nd = C.POINTER(C.c_double)()
+    opt = lambda a: dp(a) if a is not None else nd  # noqa: E731
     bco = C.c_int(0)
     fcc = C.c_int(0)
-    check(lib().bv_layout_build(dp(x), dp(y), dp(obs), n, int(bc), int(cs), int(seed), int(epochs),
-                                int(threads), ip(bn), ip(acc), dp(xn), dp(yn), dp(on), dp(cx),
-                                dp(cy), C.byref(bco), C.byref(fcc)))
+    check(lib().bv_layout_build_ex(dp(x), dp(y), opt(zc), dp(obs), n, int(bc), int(cs), int(seed),
+                                   int(epochs), int(threads), _ordering(ordering), ip(bn), ip(acc),
+                                   dp(xn), dp(yn), opt(zn), dp(on), dp(cx), dp(cy), opt(cz),
+                                   C.byref(bco), C.byref(fcc)))
     b = bco.value
     return Layout(bn[:b].copy(), acc[:b + 1].copy(), xn, yn, on, int(cs), cx[:b].copy(),
-                  cy[:b].copy(), None, fcc.value)
+                  cy[:b].copy(), None, fcc.value, z=zn,
+                  cz=cz[:b].copy() if cz is not None else None)
 
 
-def _build_layout3(x, y, z, obs, bc, cs, seed, epochs, threads) -> Layout:
-    x, y, z, obs = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, obs))
-    n = len(x)
-    k = n if n < 2 * bc else bc
-    bn = np.zeros(k, dtype=np.int32)
-    acc = np.zeros(k + 1, dtype=np.int32)
-    xn, yn, zn, on = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
-    cx, cy, cz = np.zeros(k), np.zeros(k), np.zeros(k)
-    bco = C.c_int(0)
-    fcc = C.c_int(0)
-    check(lib().bv_layout_build3(dp(x), dp(y), dp(z), dp(obs), n, int(bc), int(cs), int(seed),
-                                 int(epochs), int(threads), ip(bn), ip(acc), dp(xn), dp(yn), dp(zn),
-                                 dp(on), dp(cx), dp(cy), dp(cz), C.byref(bco), C.byref(fcc)))
-    b = bco.value
-    return Layout(bn[:b].copy(), acc[:b + 1].copy(), xn, yn, on, int(cs), cx[:b].copy(),
-                  cy[:b].copy(), None, fcc.value, z=zn, cz=cz[:b].copy())
+def order_centroids(x, y, z=None, ordering="random"):
+    """One centroid ordering alone (copies; z None for 2-D)."""
+    x = np.array(x, dtype=np.float64)
+    y = np.array(y, dtype=np.float64)
+    z = None if z is None else np.array(z, dtype=np.float64)
+    check(lib().bv_order_centroids(_ordering(ordering), len(x), dp(x), dp(y),
+                                   dp(z) if z is not None else C.POINTER(C.c_double)()))
+    return (x, y) if z is None else (x, y, z)
 
 
 def knn(layout: Layout, device: int = 0, mask=None) -> np.ndarray:

@@ -365,6 +365,41 @@ int bv_layout_build3(const double *x, const double *y, const double *z,
                      double *y_new, double *z_new, double *obs_new, double *cx,
                      double *cy, double *cz, int *bc_out, int *first_cluster_count);
 
+/* Centroid orderings: the reference's --permutation (random, the default;
+ * morton, kdtree, hilbert, mmd: src/test_Xvecchia_batch.cpp:286-314 and
+ * include/ckernel.h:148-1000, the 3-D variants for 3-D locations).  Morton
+ * and Hilbert quantise the centroids to k / 65535 (they need coordinates in
+ * [0, 1]); reorderIndex then maps each reordered centroid to its nearest
+ * original one, and two centroids mapped to one cluster are an error, as
+ * they stop the reference. */
+#define BV_ORDER_RANDOM  0
+#define BV_ORDER_MORTON  1
+#define BV_ORDER_KDTREE  2
+#define BV_ORDER_HILBERT 3
+#define BV_ORDER_MMD     4
+
+/* bv_layout_build / bv_layout_build3 with a centroid ordering; z, z_new and
+ * cz NULL for 2-D locations. */
+int bv_layout_build_ex(const double *x, const double *y, const double *z,
+                       const double *obs, int n, int bc, int cs, int seed, int epochs,
+                       int threads, int ordering, int *batchNum, int *batchNumAccum,
+                       double *x_new, double *y_new, double *z_new, double *obs_new,
+                       double *cx, double *cy, double *cz, int *bc_out,
+                       int *first_cluster_count);
+
+/* bv_layout_from_clusters with an optional third coordinate and a centroid
+ * ordering. */
+int bv_layout_from_clusters_ex(const double *x, const double *y, const double *z,
+                               const double *obs, int n, int k, const int *labels,
+                               const double *ccx, const double *ccy, const double *ccz,
+                               int cs, int ordering, int *batchNum, int *batchNumAccum,
+                               double *x_new, double *y_new, double *z_new,
+                               double *obs_new, double *cx, double *cy, double *cz,
+                               int *bc_out, int *first_cluster_count);
+
+/* The ordering alone, in place on n centroids (z = NULL: 2-D). */
+int bv_order_centroids(int ordering, int n, double *x, double *y, double *z);
+
 #ifdef __cplusplus
 }
 #endif

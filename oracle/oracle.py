@@ -111,6 +111,11 @@ def ref():
         L.ref_layout_from_clusters3.restype = C.c_int
         L.ref_layout_from_clusters3.argtypes = [_D, _D, _D, _D, C.c_int, C.c_int, _I, _D, _D, _D,
                                                 C.c_int, _I, _I, _D, _D, _D, _D, _D, _D, _D, _I, _I]
+        L.ref_order_centroids.argtypes = [C.c_int, C.c_int, _D, _D, _D]
+        L.ref_layout_from_clusters_ord.restype = C.c_int
+        L.ref_layout_from_clusters_ord.argtypes = [_D, _D, _D, _D, C.c_int, C.c_int, _I, _D, _D, _D,
+                                                   C.c_int, C.c_int, _I, _I, _D, _D, _D, _D, _D, _D,
+                                                   _D, _I, _I]
         L.ref_kmeans.restype = C.c_int
         L.ref_kmeans.argtypes = [_D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _I, _D, _D]
         L.ref_layout_from_clusters.restype = C.c_int
@@ -393,3 +398,48 @@ def ref_layout_from_clusters(x, y, obs, labels, cx, cy, cs):
     return dict(batchNum=bn[:bc].copy(), batchNumAccum=acc[:bc + 1].copy(), x=xn, y=yn, obs=on,
                 cx=bcx[:bc].copy(), cy=bcy[:bc].copy(), first_cluster_count=fcc.value,
                 first_cluster_size=fcs.value)
+
+
+def ref_order_centroids(x, y, z=None, ordering=0):
+    """The reference's centroid ordering (0 random, 1 morton, 2 kdtree,
+    3 hilbert, 4 mmd), on copies."""
+    x = np.array(x, dtype=np.float64)
+    y = np.array(y, dtype=np.float64)
+    z = None if z is None else np.array(z, dtype=np.float64)
+    ref().ref_order_centroids(int(ordering), len(x), _dp(x), _dp(y),
+                              _dp(z) if z is not None else C.POINTER(C.c_double)())
+    return (x, y) if z is None else (x, y, z)
+
+
+def ref_layout_from_clusters_ord(x, y, obs, labels, cx, cy, cs, ordering, z=None, cz=None):
+    """The reference's layout steps with a centroid ordering; None where its
+    reorderIndex would stop on a repeated cluster."""
+    x, y, obs = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, obs))
+    labels = np.ascontiguousarray(labels, dtype=np.int32)
+    cx = np.ascontiguousarray(cx, dtype=np.float64)
+    cy = np.ascontiguousarray(cy, dtype=np.float64)
+    nd = C.POINTER(C.c_double)()
+    zc = None if z is None else np.ascontiguousarray(z, dtype=np.float64)
+    czc = None if cz is None else np.ascontiguousarray(cz, dtype=np.float64)
+    n, k = len(x), len(cx)
+    bn = np.zeros(k + 1, dtype=np.int32)
+    acc = np.zeros(k + 2, dtype=np.int32)
+    xn, yn, zn, on = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
+    bcx, bcy, bcz = np.zeros(k), np.zeros(k), np.zeros(k)
+    fcc = C.c_int(0)
+    fcs = C.c_int(0)
+    tf = zc is not None
+    bc = ref().ref_layout_from_clusters_ord(_dp(x), _dp(y), _dp(zc) if tf else nd, _dp(obs), n, k,
+                                            _ip(labels), _dp(cx), _dp(cy), _dp(czc) if tf else nd,
+                                            int(cs), int(ordering), _ip(bn), _ip(acc), _dp(xn),
+                                            _dp(yn), _dp(zn) if tf else nd, _dp(on), _dp(bcx),
+                                            _dp(bcy), _dp(bcz) if tf else nd, C.byref(fcc),
+                                            C.byref(fcs))
+    if bc < 0:
+        return None
+    out = dict(batchNum=bn[:bc].copy(), batchNumAccum=acc[:bc + 1].copy(), x=xn, y=yn, obs=on,
+               cx=bcx[:bc].copy(), cy=bcy[:bc].copy(), first_cluster_count=fcc.value,
+               first_cluster_size=fcs.value)
+    if tf:
+        out.update(z=zn, cz=bcz[:bc].copy())
+    return out

@@ -181,6 +181,73 @@ int ref_kmeans(const double *x, const double *y, int n, int k, int seed,
  * Outputs (caller-allocated): batchNum[nclusters], batchNumAccum[nclusters+1],
  * x/y/obs_new[n], block centroids bcx/bcy[nclusters] (block i uses centroid
  * locsCentroid[i + firstClusterCount - 1]).  Returns batchCount. */
+/* The reference's centroid orderings (src/test_Xvecchia_batch.cpp:286-314),
+ * in place; z NULL for 2-D.  ordering: 0 random, 1 morton, 2 kdtree,
+ * 3 hilbert, 4 mmd. */
+void ref_order_centroids(int ordering, int n, double *x, double *y, double *z)
+{
+    location l = {x, y, z};
+    const bool tf = z != nullptr;
+    switch (ordering) {
+    case 0: tf ? random_reordering_3d(n, &l) : random_reordering(n, &l); break;
+    case 1: tf ? zsort_locations_morton_3d(n, &l) : zsort_reordering(n, &l); break;
+    case 2: tf ? zsort_locations_kdtree_3d(n, &l) : zsort_locations_kdtree(n, &l); break;
+    case 3: tf ? zsort_locations_hilbert_3d(n, &l) : zsort_locations_hilbert(n, &l); break;
+    case 4: tf ? zsort_locations_mmd_3d(n, &l) : zsort_locations_mmd(n, &l); break;
+    default: break;
+    }
+}
+
+/* Whether reorderIndex (include/vecchia_helper_method.h:128-160) would map
+ * two reordered centroids to one original one (where the reference calls
+ * exit): the same nearest scan, run here first so that the glue can return
+ * instead. */
+static bool reorder_would_repeat(const location *cent, const std::vector<Point> &pts, int k, bool tf)
+{
+    std::vector<char> hit(k, 0);
+    for (int i = 0; i < k; ++i) {
+        double best = DBL_MAX;
+        int arg = 0;
+        for (int j = 0; j < k; ++j) {
+            double dx = cent->x[i] - pts[j].coordinates[0];
+            double dy = cent->y[i] - pts[j].coordinates[1];
+            double d = dx * dx + dy * dy;
+            if (tf) {
+                double dz = cent->z[i] - pts[j].coordinates[2];
+                d += dz * dz;
+            }
+            if (d < best) {
+                best = d;
+                arg = j;
+            }
+        }
+        if (hit[arg]) return true;
+        hit[arg] = 1;
+    }
+    return false;
+}
+
+static int layout_from_clusters_glue(const double *x, const double *y, const double *z,
+                                     const double *obs, int n, int nclusters, const int *labels,
+                                     const double *cx, const double *cy, const double *cz, int cs,
+                                     int ordering, int *batchNum, int *batchNumAccum,
+                                     double *x_new, double *y_new, double *z_new, double *obs_new,
+                                     double *bcx, double *bcy, double *bcz,
+                                     int *first_cluster_count, int *first_cluster_size);
+
+int ref_layout_from_clusters_ord(const double *x, const double *y, const double *z,
+                                 const double *obs, int n, int nclusters, const int *labels,
+                                 const double *cx, const double *cy, const double *cz, int cs,
+                                 int ordering, int *batchNum, int *batchNumAccum, double *x_new,
+                                 double *y_new, double *z_new, double *obs_new, double *bcx,
+                                 double *bcy, double *bcz, int *first_cluster_count,
+                                 int *first_cluster_size)
+{
+    return layout_from_clusters_glue(x, y, z, obs, n, nclusters, labels, cx, cy, cz, cs, ordering,
+                                     batchNum, batchNumAccum, x_new, y_new, z_new, obs_new, bcx,
+                                     bcy, bcz, first_cluster_count, first_cluster_size);
+}
+
 int ref_layout_from_clusters3(const double *x, const double *y, const double *z,
                               const double *obs, int n, int nclusters,
                               const int *labels, const double *cx,
@@ -189,6 +256,19 @@ int ref_layout_from_clusters3(const double *x, const double *y, const double *z,
                               double *y_new, double *z_new, double *obs_new,
                               double *bcx, double *bcy, double *bcz,
                               int *first_cluster_count, int *first_cluster_size)
+{
+    return layout_from_clusters_glue(x, y, z, obs, n, nclusters, labels, cx, cy, cz, cs, 0,
+                                     batchNum, batchNumAccum, x_new, y_new, z_new, obs_new, bcx,
+                                     bcy, bcz, first_cluster_count, first_cluster_size);
+}
+
+static int layout_from_clusters_glue(const double *x, const double *y, const double *z,
+                                     const double *obs, int n, int nclusters, const int *labels,
+                                     const double *cx, const double *cy, const double *cz, int cs,
+                                     int ordering, int *batchNum, int *batchNumAccum,
+                                     double *x_new, double *y_new, double *z_new, double *obs_new,
+                                     double *bcx, double *bcy, double *bcz,
+                                     int *first_cluster_count, int *first_cluster_size)
 {
     const bool tf = z != nullptr;
     location l = {(double *)x, (double *)y, (double *)z};
@@ -214,10 +294,15 @@ int ref_layout_from_clusters3(const double *x, const double *y, const double *z,
         if (tf) cent.z[i] = centroids[i].coordinates[2];
         permIndex[i] = centroids[i].cluster;
     }
-    if (tf)                                                             /* :288 */
-        random_reordering_3d(nclusters, &cent);
-    else
-        random_reordering(nclusters, &cent);
+    ref_order_centroids(ordering, nclusters, cent.x, cent.y, cent.z);   /* :286-314 */
+    if (reorder_would_repeat(&cent, centroids, nclusters, tf)) {
+        delete[] clusterNum;
+        free(permIndex);
+        free(cent.x);
+        free(cent.y);
+        free(cent.z);
+        return -1;
+    }
     reorderIndex(&cent, centroids, permIndex, nclusters, tf);           /* :319 */
     int fcs = 0, fcc = 0;
     firstbatch(nclusters, clusterNum, permIndex, &fcs, &fcc, cs);       /* :323 */

@@ -110,3 +110,93 @@ def test_layout_with_many_duplicated_locations(bvlib):
     y = np.clip(0.5 + 0.4 * rng.standard_normal(n), 0, 1)
     L = bvlib.build_layout(x, y, np.arange(n, dtype=np.float64), 3000, 40, seed=0, epochs=5)
     assert np.array_equal(np.sort(L.obs.astype(np.int64)), np.arange(n))
+
+
+# ------------------------------------------------------- centroid orderings
+
+ORDER_NAMES = ["random", "morton", "kdtree", "hilbert", "mmd"]
+
+
+@pytest.mark.parametrize("name", ["unif2", "unif3", "grid2"])
+def test_orderings_golden(bvlib, name):
+    """Each --permutation ordering equals the reference's (fixtures from its
+    own code): uniform 2-D/3-D centroids and a grid with repeated
+    coordinates (equal kd-tree keys)."""
+    g = golden("orderings.npz")
+    x, y = g[f"{name}_x"], g[f"{name}_y"]
+    z = g[f"{name}_z"] if f"{name}_z" in g else None
+    for o, oname in enumerate(ORDER_NAMES):
+        if f"{name}_o{o}_x" not in g:
+            continue
+        got = bvlib.order_centroids(x, y, z, oname)
+        for c, v in zip("xyz", got):
+            assert np.array_equal(v, g[f"{name}_o{o}_{c}"]), (name, oname, c)
+
+
+@pytest.mark.parametrize("o", range(5))
+def test_layout_orderings_golden(bvlib, golden_layout, o):
+    g, r = golden_layout, golden("orderings.npz")
+    L = bvlib.layout_from_clusters(g["x"], g["y"], g["obs"], g["labels"], g["kcx"], g["kcy"], 60,
+                                   ordering=ORDER_NAMES[o])
+    for key, mine in [("batchNum", L.batchNum), ("batchNumAccum", L.batchNumAccum), ("x", L.x),
+                      ("y", L.y), ("obs", L.obs), ("cx", L.cx), ("cy", L.cy)]:
+        assert np.array_equal(mine, r[f"layout_o{o}_{key}"]), (ORDER_NAMES[o], key)
+    assert L.first_cluster_count == int(r[f"layout_o{o}_fcc"])
+
+
+@pytest.mark.parametrize("n,dim3", [(1, False), (2, True), (7, False), (300, True), (1000, False)])
+def test_orderings_live_vs_reference(bvlib, ref, n, dim3):
+    rng = np.random.default_rng(n)
+    x, y = rng.random(n), rng.random(n)
+    z = rng.random(n) if dim3 else None
+    for o, oname in enumerate(ORDER_NAMES):
+        if o == 4 and n > 600:
+            continue  # the reference's MMD is O(n^3)
+        want = ref.ref_order_centroids(x, y, z, o)
+        got = bvlib.order_centroids(x, y, z, oname)
+        assert all(np.array_equal(a, b) for a, b in zip(want, got)), (n, dim3, oname)
+
+
+@pytest.mark.parametrize("dim3", [False, True])
+def test_layout_orderings_live_vs_reference(bvlib, ref, dim3):
+    n, k, cs = 3000, 200, 60
+    rng = np.random.default_rng(5)
+    x, y = rng.random(n), rng.random(n)
+    obs = rng.standard_normal(n)
+    labels, cx, cy = ref.ref_kmeans(x, y, k, 0, 10, 1)
+    z, cz = (rng.random(n), rng.random(k)) if dim3 else (None, None)
+    for o, oname in enumerate(ORDER_NAMES):
+        R = ref.ref_layout_from_clusters_ord(x, y, obs, labels, cx, cy, cs, o, z=z, cz=cz)
+        M = bvlib.layout_from_clusters(x, y, obs, labels, cx, cy, cs, z=z, ccz=cz, ordering=oname)
+        keys = ["batchNum", "batchNumAccum", "x", "y", "obs", "cx", "cy"] + (["z", "cz"] if dim3 else [])
+        for key in keys:
+            assert np.array_equal(getattr(M, key), R[key]), (oname, key)
+
+
+def test_quantising_orderings_reject_collisions(bvlib, ref):
+    """Two centroids that quantise to one 16-bit point map to one cluster:
+    the reference's reorderIndex stops there, the library returns an error."""
+    rng = np.random.default_rng(9)
+    n, k = 400, 40
+    x, y = rng.random(n), rng.random(n)
+    obs = rng.standard_normal(n)
+    labels = (np.arange(n) % k).astype(np.int32)
+    cx, cy = rng.random(k), rng.random(k)
+    cx[1], cy[1] = cx[0] + 1e-7, cy[0]
+    for o, oname in [(1, "morton"), (3, "hilbert")]:
+        assert ref.ref_layout_from_clusters_ord(x, y, obs, labels, cx, cy, 20, o) is None
+        with pytest.raises(bvlib.BvError, match="maps centroids"):
+            bvlib.layout_from_clusters(x, y, obs, labels, cx, cy, 20, ordering=oname)
+    # Outside the unit square the 16-bit quantisation is undefined: rejected.
+    with pytest.raises(bvlib.BvError, match="outside the unit"):
+        bvlib.order_centroids(np.array([0.5, 1.5]), np.array([0.5, 0.5]), None, "morton")
+
+
+def test_build_layout_ordering_argument(bvlib):
+    x, y = bvlib.generate_xy(3000, 1)
+    obs = np.random.default_rng(1).standard_normal(3000)
+    a = bvlib.build_layout(x, y, obs, 200, 40, seed=0, epochs=5, ordering="kdtree")
+    b = bvlib.build_layout(x, y, obs, 200, 40, seed=0, epochs=5, ordering=2)
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.cx, b.cx)
+    with pytest.raises(ValueError):
+        bvlib.build_layout(x, y, obs, 200, 40, ordering="zigzag")
