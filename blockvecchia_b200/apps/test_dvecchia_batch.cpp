@@ -7,7 +7,7 @@
 // --omp_threads --permutation --dist_scale --lower_bound --upper_bound.
 // --perf evaluates once at --ikernel with zero observations on GenerateXYLoc
 // locations and writes the blocks' points and conditioning points to
-// ./log/points_Random.csv and ./log/neighbors_Random.csv; otherwise the
+// ./log/points_<Ordering>.csv and ./log/neighbors_<Ordering>.csv; otherwise the
 // locations/observations CSVs are fitted from --kernel_init.  The objective
 // is bv_llh (the NLopt signature of llh_Xvecchia_batch); NLopt BOBYQA is used
 // when <nlopt.h> exists at build time, else a bounded Nelder-Mead (Nelder &
@@ -53,7 +53,20 @@ struct Opts {
     double tol = 1e-5, lower_bound = 0.01, upper_bound = 3.0;
     int omp_threads = 40, device = 0, precision = BV_PREC_FP64, print_opts = 0;
     std::string xy_path, obs_path, permutation = "random";
+    int ordering = BV_ORDER_RANDOM;
 };
+
+// --permutation names (include/vecchia_helper_data.h:456-476) and the
+// perf-mode dump suffixes (src/test_Xvecchia_batch.cpp:409-435).
+struct OrderName {
+    const char *flag, *dump;
+    int ordering;
+};
+const OrderName kOrders[] = {{"random", "Random", BV_ORDER_RANDOM},
+                             {"morton", "Morton", BV_ORDER_MORTON},
+                             {"kdtree", "KDtree", BV_ORDER_KDTREE},
+                             {"hilbert", "Hilbert", BV_ORDER_HILBERT},
+                             {"mmd", "MMD", BV_ORDER_MMD}};
 
 [[noreturn]] void die(const char *msg, const char *arg = "")
 {
@@ -93,7 +106,7 @@ Opts parse(int argc, char **argv)
             printf("Usage: test_dvecchia_batch [--kernel K] [--ikernel s2:range:nu[:nugget]] [--kernel_init ...]\n"
                    "  [--vecchia_cs N] [--vecchia_bc N] [--num_loc N] [--knn x] [--perf x] [--seed N]\n"
                    "  [--xy_path F] [--obs_path F] [--tol k (1e-k)] [--maxiter N] [--omp_threads N]\n"
-                   "  [--permutation random] [--dist_scale d] [--lower_bound b] [--upper_bound b]\n"
+                   "  [--permutation random|morton|kdtree|hilbert|mmd] [--dist_scale d] [--lower_bound b] [--upper_bound b]\n"
                    "  [--t_slots N] [--3D x] [--use_nugget 0|1]\n"
                    "  [--precision fp64|mixed] [--device N] [--print-opts]\n"
                    "  space-time: --kernel univariate_matern_spacetime_stationary\n"
@@ -164,7 +177,12 @@ Opts parse(int argc, char **argv)
             if (!(o.upper_bound < 100)) die("--upper_bound must be < 100");
         } else if (a == "--permutation" && has) {
             o.permutation = next();
-            if (o.permutation != "random") die("only --permutation random is supported: ", o.permutation.c_str());
+            o.ordering = -1;
+            for (const auto &k : kOrders)
+                if (o.permutation == k.flag) o.ordering = k.ordering;
+            // The reference prints "Other ordering is being developed." and stops.
+            if (o.ordering < 0) die("unknown --permutation (random, morton, kdtree, hilbert, mmd): ",
+                                    o.permutation.c_str());
         } else if (a == "--precision" && has) {
             const std::string p = next();
             o.precision = (p == "mixed") ? BV_PREC_MIXED : BV_PREC_FP64;
@@ -203,12 +221,13 @@ void print_opts(const Opts &o)
            "\"tol\": %.17g, \"maxiter\": %d, \"lower_bound\": %.17g, \"upper_bound\": %.17g, "
            "\"dist_scale\": %.17g, \"omp_threads\": %d, \"precision\": %d, \"xy_path\": \"%s\", "
            "\"obs_path\": \"%s\", \"time_flag\": %d, \"t_slots\": %d, \"beta_time\": %.17g, "
-           "\"nu_time\": %.17g, \"sep\": %.17g, \"nugget\": %.17g, \"use_nugget\": %d}\n",
+           "\"nu_time\": %.17g, \"sep\": %.17g, \"nugget\": %.17g, \"use_nugget\": %d, "
+           "\"permutation\": \"%s\", \"ordering\": %d}\n",
            o.kernel, o.num_params, o.num_loc, o.sigma, o.beta, o.nu, o.sigma_init, o.beta_init,
            o.nu_init, o.vecchia_cs, o.vecchia_bc, o.knn, o.perf, o.seed, o.tol, o.maxiter,
            o.lower_bound, o.upper_bound, o.dist_scale, o.omp_threads, o.precision,
            o.xy_path.c_str(), o.obs_path.c_str(), o.time_flag, o.t_slots, o.beta_time, o.nu_time, o.sep,
-           o.nugget, o.use_nugget);
+           o.nugget, o.use_nugget, o.permutation.c_str(), o.ordering);
 }
 
 // include/utils.h:27-87: "x,y" per line ("x,y,z" with time_flag); one
@@ -402,13 +421,11 @@ int main(int argc, char **argv)
     std::vector<int> bn(k), acc(k + 1);
     std::vector<double> xn(n), yn(n), zn(n), cx(k), cy(k), tn(tf ? n : 0), ct(tf ? k : 0);
     int bc = 0, fcc = 0;
-    const int lrc = tf ? bv_layout_build3(x.data(), y.data(), t3.data(), z.data(), n, o.vecchia_bc,
-                                          o.vecchia_cs, o.seed, 50, o.omp_threads, bn.data(),
-                                          acc.data(), xn.data(), yn.data(), tn.data(), zn.data(),
-                                          cx.data(), cy.data(), ct.data(), &bc, &fcc)
-                       : bv_layout_build(x.data(), y.data(), z.data(), n, o.vecchia_bc, o.vecchia_cs,
-                                         o.seed, 50, o.omp_threads, bn.data(), acc.data(), xn.data(),
-                                         yn.data(), zn.data(), cx.data(), cy.data(), &bc, &fcc);
+    const int lrc = bv_layout_build_ex(x.data(), y.data(), tf ? t3.data() : nullptr, z.data(), n,
+                                       o.vecchia_bc, o.vecchia_cs, o.seed, 50, o.omp_threads,
+                                       o.ordering, bn.data(), acc.data(), xn.data(), yn.data(),
+                                       tf ? tn.data() : nullptr, zn.data(), cx.data(), cy.data(),
+                                       tf ? ct.data() : nullptr, &bc, &fcc);
     if (lrc) die(bv_last_error());
     fprintf(stderr, "--------------Clustering Done-----------------\n");
     const int cs = o.vecchia_cs;
@@ -428,16 +445,19 @@ int main(int argc, char **argv)
         }
     }
     if (o.perf) {
-        // src/test_Xvecchia_batch.cpp:405-451 with random ordering (the only
-        // ordering here): every block's points with the block's index, then
-        // every block's cs conditioning points with the block's index (block
-        // 0's are the first cs points, as the reference fills them at :359-361).
+        // src/test_Xvecchia_batch.cpp:405-451: every block's points with the
+        // block's index, then every block's cs conditioning points with the
+        // block's index (block 0's are the first cs points, as the reference
+        // fills them at :359-361); file names carry the ordering.
         mkdir("./log", 0755);
-        std::ofstream pts("./log/points_Random.csv");
+        std::string suffix = "Random";
+        for (const auto &k : kOrders)
+            if (k.ordering == o.ordering) suffix = k.dump;
+        std::ofstream pts("./log/points_" + suffix + ".csv");
         pts << "x,y,cluster\n";
         for (int i = 0; i < bc; ++i)
             for (int j = 0; j < bn[i]; ++j) pts << xn[acc[i] + j] << "," << yn[acc[i] + j] << "," << i << "\n";
-        std::ofstream nbr("./log/neighbors_Random.csv");
+        std::ofstream nbr("./log/neighbors_" + suffix + ".csv");
         nbr << "x,y,cluster\n";
         for (size_t t = 0; t < (size_t)bc * cs; ++t) {
             const int src = (t < (size_t)cs) ? (int)t : knn[t];

@@ -51,7 +51,7 @@ def test_question_mark_keeps_value(exe):
 
 
 @pytest.mark.parametrize("bad", [["--tol", "0"], ["--maxiter", "-3"], ["--upper_bound", "200"],
-                                 ["--permutation", "kdtree"], ["--earth", "1"], ["--kernel", "foo"],
+                                 ["--permutation", "zigzag"], ["--earth", "1"], ["--kernel", "foo"],
                                  ["--kernel", "univariate_matern_spacetime_stationary", "--t_slots", "3",
                                   "--num_loc", "1000", "--perf", "1"]])
 def test_rejected(exe, bad):
@@ -69,3 +69,11 @@ def test_spacetime_flags(exe):
         (1.2, 0.1, 0.5, 0.4, 0.8, 0.6)
     o = _opts(exe, "--3D", "1")
     assert o["time_flag"] == 1 and o["t_slots"] == 0
+
+
+@pytest.mark.parametrize("name,code", [("random", 0), ("morton", 1), ("kdtree", 2), ("hilbert", 3),
+                                       ("mmd", 4)])
+def test_permutation_flag(exe, name, code):
+    """--permutation (include/vecchia_helper_data.h:456-476)."""
+    o = _opts(exe, "--permutation", name)
+    assert o["permutation"] == name and o["ordering"] == code

@@ -58,6 +58,25 @@ def test_perf_mode_matches_oracle(exe, bvlib, oracle, tmp_path):
     assert nbr[1:] == [f"{g(L.x[s])},{g(L.y[s])},{t // cs}" for t, s in enumerate(src)]
 
 
+@pytest.mark.parametrize("name,suffix", [("morton", "Morton"), ("kdtree", "KDtree"), ("mmd", "MMD")])
+def test_perf_mode_orderings(exe, bvlib, oracle, tmp_path, name, suffix):
+    """--perf with another centroid ordering: the layout of that ordering,
+    the likelihood against the oracle, the dumps named for the ordering."""
+    n, bc, cs = 3000, 200, 60
+    _, llk, _ = _run(exe, ["--num_loc", str(n), "--vecchia_bc", str(bc), "--vecchia_cs", str(cs),
+                           "--ikernel", "1.5:0.1:0.5", "--perf", "1", "--seed", "0",
+                           "--permutation", name], tmp_path)
+    x, y = bvlib.generate_xy(n, 0)
+    L = bvlib.build_layout(x, y, np.zeros(n), bc, cs, seed=0, epochs=50, ordering=name)
+    knn = oracle.knn_all(L.x, L.y, cs, L.batchNumAccum, L.cx, L.cy)
+    P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, knn, cs)
+    ref = oracle.llh(P, (1.5, 0.1, 0.5))
+    assert abs(llk - ref) <= 1e-10 * abs(ref)
+    pts = (tmp_path / "log" / f"points_{suffix}.csv").read_text().splitlines()
+    assert pts[0] == "x,y,cluster" and len(pts) == n + 1
+    assert (tmp_path / "log" / f"neighbors_{suffix}.csv").exists()
+
+
 def test_fit_matches_oracle_fit(exe, bvlib, oracle, tmp_path):
     """A fit from 0.1:0.1:0.1 on an exact GP draw; the optimum agrees with a
     Nelder-Mead maximisation of the oracle's likelihood to the optimizer
