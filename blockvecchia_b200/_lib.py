@@ -53,6 +53,8 @@ EXPORTS = {
     "bv_knn": (C.c_int, [_D, _D, C.c_int, C.c_int, C.c_int, _I, _D, _D, _I, C.c_int]),
     "bv_knn_subset": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, C.c_int, _I, _D, _D, _D,
                                 C.POINTER(C.c_ubyte), _I, C.c_int]),
+    "bv_knn_ex": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, C.c_int, _I, _D, _D, _D,
+                            C.POINTER(C.c_ubyte), C.c_int, _I, C.c_int]),
     "bv_knn3": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, C.c_int, _I, _D, _D, _D, _I, C.c_int]),
     "bv_layout_build": (C.c_int, [_D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                   _I, _I, _D, _D, _D, _D, _D, _I, _I]),
@@ -101,7 +103,7 @@ class BvOpts(C.Structure):
                 ("device", C.c_int), ("on_failure", C.c_int), ("print_iter", C.c_int),
                 ("use_graph", C.c_int), ("schedule", C.c_int), ("mixed_tol", C.c_double),
                 ("shard_count", C.c_int), ("shard_index", C.c_int), ("large_blocks", C.c_int),
-                ("nugget", C.c_int)]
+                ("nugget", C.c_int), ("earth", C.c_int)]
 
 
 class BvStatus(C.Structure):

@@ -4,7 +4,8 @@
 //
 // Flags kept: --kernel --ikernel --kernel_init --vecchia_cs --vecchia_bc
 // --num_loc --knn --perf --seed --xy_path --obs_path --tol --maxiter
-// --omp_threads --permutation --dist_scale --lower_bound --upper_bound.
+// --omp_threads --permutation --dist_scale --lower_bound --upper_bound
+// --earth --t_slots --3D.
 // --perf evaluates once at --ikernel with zero observations on GenerateXYLoc
 // locations and writes the blocks' points and conditioning points to
 // ./log/points_<Ordering>.csv and ./log/neighbors_<Ordering>.csv; otherwise the
@@ -48,7 +49,7 @@ struct Opts {
     // space-time (include/vecchia_helper_data.h:293-302)
     double beta_time = 2.2, nu_time = 0.5, sep = 0.5, aux = 0.0;
     double beta_time_init = 0.01, nu_time_init = 0.01, sep_init = 0.01;
-    int time_flag = 0, t_slots = 0, use_nugget = 0;
+    int time_flag = 0, t_slots = 0, use_nugget = 0, earth = 0;
     int knn = 1, seed = 0, perf = 0, vecchia_cs = 100, vecchia_bc = 200, maxiter = 1000;
     double tol = 1e-5, lower_bound = 0.01, upper_bound = 3.0;
     int omp_threads = 40, device = 0, precision = BV_PREC_FP64, print_opts = 0;
@@ -201,8 +202,10 @@ Opts parse(int argc, char **argv)
             // Not in the reference (its likelihood never reads the nugget):
             // the nugget (fourth --ikernel value) enters the covariance.
             o.use_nugget = atoi(next()) != 0;
-        } else if (a == "--earth") {
-            die("not supported by this build (Euclidean distances only): ", a.c_str());
+        } else if (a == "--earth" && has) {
+            // include/vecchia_helper_data.h:451-454: a flag that needs a
+            // following argument but does not consume it.
+            o.earth = 1;
         } else {
             die("unknown or incomplete option: ", a.c_str());
         }
@@ -210,6 +213,8 @@ Opts parse(int argc, char **argv)
     // src/test_Xvecchia_batch.cpp:107-111
     if (o.time_flag && o.t_slots != 0 && o.num_loc % o.t_slots != 0)
         die("Your number of locations cannot be divided by t_slot!");
+    // src/ckernel.cpp:170-172 (the reference stops at the first covariance).
+    if (o.earth && o.time_flag) die("Great Circle (GC) distance is only valid for 2d");
     return o;
 }
 
@@ -222,12 +227,12 @@ void print_opts(const Opts &o)
            "\"dist_scale\": %.17g, \"omp_threads\": %d, \"precision\": %d, \"xy_path\": \"%s\", "
            "\"obs_path\": \"%s\", \"time_flag\": %d, \"t_slots\": %d, \"beta_time\": %.17g, "
            "\"nu_time\": %.17g, \"sep\": %.17g, \"nugget\": %.17g, \"use_nugget\": %d, "
-           "\"permutation\": \"%s\", \"ordering\": %d}\n",
+           "\"permutation\": \"%s\", \"ordering\": %d, \"earth\": %d}\n",
            o.kernel, o.num_params, o.num_loc, o.sigma, o.beta, o.nu, o.sigma_init, o.beta_init,
            o.nu_init, o.vecchia_cs, o.vecchia_bc, o.knn, o.perf, o.seed, o.tol, o.maxiter,
            o.lower_bound, o.upper_bound, o.dist_scale, o.omp_threads, o.precision,
            o.xy_path.c_str(), o.obs_path.c_str(), o.time_flag, o.t_slots, o.beta_time, o.nu_time, o.sep,
-           o.nugget, o.use_nugget, o.permutation.c_str(), o.ordering);
+           o.nugget, o.use_nugget, o.permutation.c_str(), o.ordering, o.earth);
 }
 
 // include/utils.h:27-87: "x,y" per line ("x,y,z" with time_flag); one
@@ -375,6 +380,9 @@ int main(int argc, char **argv)
     }
     const int n = o.num_loc;
     const bool tf = o.time_flag != 0;
+    // src/test_Xvecchia_batch.cpp:206-209: distance_metric = 1 is set for
+    // locations read from files only (not for the synthetic --perf locations).
+    const int earth = (o.earth && !o.perf) ? 1 : 0;
     std::vector<double> x, y, t3, z;  // t3: third coordinate (time_flag), z: observations
     // Parameter vector: the kernel's (3, or 7 for space-time), then the
     // nugget when --use_nugget (src/test_Xvecchia_batch.cpp:156-235).
@@ -432,10 +440,10 @@ int main(int argc, char **argv)
     std::vector<int> knn((size_t)bc * cs);
     if (cs > 0) {
         if (o.knn) {
-            const int krc = tf ? bv_knn3(xn.data(), yn.data(), tn.data(), n, bc, cs, acc.data(), cx.data(),
-                                         cy.data(), ct.data(), knn.data(), o.device)
-                               : bv_knn(xn.data(), yn.data(), n, bc, cs, acc.data(), cx.data(), cy.data(),
-                                        knn.data(), o.device);
+            const int krc = bv_knn_ex(xn.data(), yn.data(), tf ? tn.data() : nullptr, n, bc, cs,
+                                      acc.data(), cx.data(), cy.data(), tf ? ct.data() : nullptr,
+                                      nullptr, earth ? BV_METRIC_EARTH : BV_METRIC_EUCLIDEAN,
+                                      knn.data(), o.device);
             if (krc) die(bv_last_error());
         } else {
             // src/test_Xvecchia_batch.cpp:391-404: the cs points before each block.
@@ -472,6 +480,7 @@ int main(int argc, char **argv)
     bv_default_opts(&bo);
     bo.kernel = o.kernel;
     bo.nugget = o.use_nugget;
+    bo.earth = earth;
     bo.dist_scale = o.dist_scale;
     bo.device = o.device;
     bo.precision = o.precision;

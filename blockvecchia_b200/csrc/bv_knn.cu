@@ -65,18 +65,42 @@ struct KnnArgs {
     int nlist;
 };
 
-// The argument of the key's final square root for candidate p (kZ: 3-D
-// locations; the 2-D kernels are separate instantiations).
-template <bool kZ>
+// Key geometries, each a separate instantiation: plane (2-D), 3-D (the
+// time_flag key), and the great-circle key of distance_metric = 1 (--earth,
+// include/nearest_neighbor.h:93-96: distanceEarth(centroid, point); z and cz
+// then carry cos(latitude) of the points and centroids, from the host).
+enum KnnGeo : int { kGeoPlane = 0, kGeo3D = 1, kGeoEarth = 2 };
+
+// The argument of the key's final square root for candidate p.
+template <int kGeo>
 __device__ __forceinline__ double knn_prekey(const KnnArgs &a, int p, double cx, double cy, double cz)
 {
+    if constexpr (kGeo == kGeoEarth) {
+        // distanceEarth up to its square root: lat1 = centroid, lat2 = point.
+        const double pi = 3.141592653589793;
+        const double lat1r = __ddiv_rn(__dmul_rn(cx, pi), 180.0);
+        const double lon1r = __ddiv_rn(__dmul_rn(cy, pi), 180.0);
+        const double lat2r = __ddiv_rn(__dmul_rn(__ldg(a.x + p), pi), 180.0);
+        const double lon2r = __ddiv_rn(__dmul_rn(__ldg(a.y + p), pi), 180.0);
+        const double u = sin(__dmul_rn(__dsub_rn(lat2r, lat1r), 0.5));
+        const double v = sin(__dmul_rn(__dsub_rn(lon2r, lon1r), 0.5));
+        return __fma_rn(u, u, __dmul_rn(__dmul_rn(__dmul_rn(cz, __ldg(a.z + p)), v), v));
+    }
     const double dx = __ldg(a.x + p) - cx;
     const double dy = __ldg(a.y + p) - cy;
     const double s = __fma_rn(dx, dx, __dmul_rn(dy, dy));
-    if constexpr (!kZ) return s;
+    if constexpr (kGeo == kGeoPlane) return s;
     const double d = __dsqrt_rn(s);
     const double dz = cz - __ldg(a.z + p);
     return __fma_rn(d, d, __dmul_rn(dz, dz));
+}
+
+// The key (a distance) from its pre-key.
+template <int kGeo>
+__device__ __forceinline__ double knn_dist(double s)
+{
+    if constexpr (kGeo == kGeoEarth) return __dmul_rn(12742.0, asin(__dsqrt_rn(s)));
+    return __dsqrt_rn(s);
 }
 
 __device__ __forceinline__ unsigned lanemask_lt()
@@ -171,16 +195,18 @@ __device__ int warp_compact(KnnWarpSmem &w, int n, unsigned long long lim)
     return count;
 }
 
-// Upper end of the squared-distance window whose square roots can equal
-// sqrt(s): sqrt halves relative spacing, so 2^-49 relative is ample.
+// Upper end of the pre-key window whose keys can equal key(s): sqrt halves
+// relative spacing, so 2^-49 relative is ample; the great-circle key adds
+// asin's few-ulp error and its scaling, covered by 2^-40.
+template <int kGeo>
 __device__ __forceinline__ unsigned long long window_hi(unsigned long long skey)
 {
     const double s = __longlong_as_double((long long)skey);
-    const double hi = s * (1.0 + 0x1p-49) + 0x1p-1070;
+    const double hi = s * (1.0 + (kGeo == kGeoEarth ? 0x1p-40 : 0x1p-49)) + 0x1p-1070;
     return (unsigned long long)__double_as_longlong(hi);
 }
 
-template <bool kZ>
+template <int kGeo>
 __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
 {
     extern __shared__ __align__(16) unsigned char knn_smem[];
@@ -202,7 +228,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
             if (i < 1) break;
         }
         const int P = a.acc[i];
-        const double cx = a.cx[i], cy = a.cy[i], cz = kZ ? a.cz[i] : 0.0;
+        const double cx = a.cx[i], cy = a.cy[i], cz = (kGeo != kGeoPlane) ? a.cz[i] : 0.0;
         int *out = a.out + (size_t)i * k;
         if (P < k) {
             if (lane == 0) atomicCAS(a.error, 0, i + 1);
@@ -222,7 +248,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
                 keep[u] = false;
                 key[u] = 0ull;
                 if (p < P) {
-                    const double s = knn_prekey<kZ>(a, p, cx, cy, cz);
+                    const double s = knn_prekey<kGeo>(a, p, cx, cy, cz);
                     key[u] = (unsigned long long)__double_as_longlong(s);
                     keep[u] = key[u] <= lim;
                 }
@@ -240,7 +266,7 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
             if (count > kKnnCap - 128) {
                 __syncwarp();
                 const unsigned long long kth = warp_kth(w, count, k);
-                lim = window_hi(kth);
+                lim = window_hi<kGeo>(kth);
                 count = warp_compact(w, count, lim);
                 if (count > kKnnCap - 128) {
                     overflow = true;
@@ -256,8 +282,19 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
 
         // 2. Exact k-th key; S = members whose distance equals or beats it.
         const unsigned long long kth = warp_kth(w, count, k);
-        count = warp_compact(w, count, window_hi(kth));
-        const double dk = __dsqrt_rn(__longlong_as_double((long long)kth));
+        count = warp_compact(w, count, window_hi<kGeo>(kth));
+        double dk = knn_dist<kGeo>(__longlong_as_double((long long)kth));
+        if constexpr (kGeo == kGeoEarth) {
+            // The great-circle key need not be monotone in its pre-key to the
+            // last bit (device asin): the k-th smallest key itself, over the
+            // window's members (all keys are non-negative, so their bit
+            // patterns order as the values do).
+            for (int j = lane; j < count; j += 32)
+                w.key[j] = (unsigned long long)__double_as_longlong(
+                    knn_dist<kGeo>(__longlong_as_double((long long)w.key[j])));
+            __syncwarp();
+            dk = __longlong_as_double((long long)warp_kth(w, count, k));
+        }
         {
             int m = 0;
             for (int base = 0; base < count; base += 32) {
@@ -266,7 +303,8 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(KnnArgs a)
                 int id = 0;
                 bool keep = false;
                 if (j < count) {
-                    d = __dsqrt_rn(__longlong_as_double((long long)w.key[j]));
+                    const double kj = __longlong_as_double((long long)w.key[j]);
+                    d = (kGeo == kGeoEarth) ? kj : knn_dist<kGeo>(kj);  // earth: already keys
                     id = w.idx[j];
                     keep = d <= dk;
                 }
@@ -335,14 +373,14 @@ struct KnnHeavyScratch {
     int *pos;
 };
 
-template <bool kZ>
+template <int kGeo>
 __device__ __forceinline__ unsigned long long knn_skey(const KnnArgs &a, int p, double cx, double cy,
                                                        double cz)
 {
-    return (unsigned long long)__double_as_longlong(knn_prekey<kZ>(a, p, cx, cy, cz));
+    return (unsigned long long)__double_as_longlong(knn_prekey<kGeo>(a, p, cx, cy, cz));
 }
 
-template <bool kZ>
+template <int kGeo>
 __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int nheavy, KnnHeavyScratch scr,
                                                                   size_t stride)
 {
@@ -358,7 +396,7 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
     for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
         const int i = a.heavy[h];
         const int P = a.acc[i];
-        const double cx = a.cx[i], cy = a.cy[i], cz = kZ ? a.cz[i] : 0.0;
+        const double cx = a.cx[i], cy = a.cy[i], cz = (kGeo != kGeoPlane) ? a.cz[i] : 0.0;
         int *out = a.out + (size_t)i * k;
         // 1. Exact k-th smallest squared distance, MSB-first radix select.
         if (tid == 0) {
@@ -371,7 +409,7 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
             __syncthreads();
             const unsigned long long prefix = s_prefix;
             for (int p = tid; p < P; p += kHeavyThreads) {
-                const unsigned long long key = knn_skey<kZ>(a, p, cx, cy, cz);
+                const unsigned long long key = knn_skey<kGeo>(a, p, cx, cy, cz);
                 if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255ull], 1u);
             }
             __syncthreads();
@@ -393,14 +431,14 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
         }
         const unsigned long long kth = s_prefix;
         // 2. S = candidates whose distance equals or beats the k-th.
-        const unsigned long long hi = window_hi(kth);
-        const double dk = __dsqrt_rn(__longlong_as_double((long long)kth));
+        const unsigned long long hi = window_hi<kGeo>(kth);
+        const double dk = knn_dist<kGeo>(__longlong_as_double((long long)kth));
         if (tid == 0) s_count = 0;
         __syncthreads();
         for (int p = tid; p < P; p += kHeavyThreads) {
-            const unsigned long long key = knn_skey<kZ>(a, p, cx, cy, cz);
+            const unsigned long long key = knn_skey<kGeo>(a, p, cx, cy, cz);
             if (key <= hi) {
-                const double d = __dsqrt_rn(__longlong_as_double((long long)key));
+                const double d = knn_dist<kGeo>(__longlong_as_double((long long)key));
                 if (d <= dk) {
                     const int slot = atomicAdd(&s_count, 1);
                     sc.key[slot] = (unsigned long long)__double_as_longlong(d);
@@ -466,12 +504,22 @@ __global__ void __launch_bounds__(kHeavyThreads) knn_heavy_kernel(KnnArgs a, int
 
 int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, int bc, int cs,
                const int *d_acc, const double *cx, const double *cy, const double *cz, int *d_knn,
-               cudaStream_t s, const unsigned char *mask)
+               cudaStream_t s, const unsigned char *mask, int earth)
 {
     if (d_z && !cz) {
         set_error("bv_knn: 3-D locations need the centroids' third coordinate");
         return BV_E_INVALID;
     }
+    if (earth && !d_z) {
+        set_error("bv_knn: the great-circle key needs cos(latitude) of points and centroids");
+        return BV_E_INVALID;
+    }
+    const int geo = earth ? kGeoEarth : (d_z ? kGeo3D : kGeoPlane);
+    void (*const kern)(KnnArgs) = geo == kGeoEarth ? knn_kernel<kGeoEarth>
+                                                   : (geo == kGeo3D ? knn_kernel<kGeo3D> : knn_kernel<kGeoPlane>);
+    void (*const heavy)(KnnArgs, int, KnnHeavyScratch, size_t) =
+        geo == kGeoEarth ? knn_heavy_kernel<kGeoEarth>
+                         : (geo == kGeo3D ? knn_heavy_kernel<kGeo3D> : knn_heavy_kernel<kGeoPlane>);
     if (cs <= 0) return BV_OK;
     if (cs > kKnnMaxCs) {
         set_error("bv_knn: cs=%d exceeds the supported maximum %d", cs, kKnnMaxCs);
@@ -539,24 +587,20 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
         ka.list = mask ? d_list : nullptr;
         ka.nlist = (int)list.size();
         const size_t smem = sizeof(KnnWarpSmem) * kKnnWarps;
-        if ((e = cudaFuncSetAttribute(d_z ? knn_kernel<true> : knn_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem))) {
+        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) {
             fail(e, "attribute");
             break;
         }
         int dev = 0, sms = 0, occ = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, d_z ? knn_kernel<true> : knn_kernel<false>, kKnnWarps * 32, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kKnnWarps * 32, smem);
         if (occ < 1) occ = 1;
         int grid = sms * occ;
         const int nsel = mask ? (int)list.size() : bc;
         const int need = (nsel + kKnnWarps - 1) / kKnnWarps;
         if (grid > need) grid = need > 0 ? need : 1;
-        if (d_z)
-            knn_kernel<true><<<grid, kKnnWarps * 32, smem, s>>>(ka);
-        else
-            knn_kernel<false><<<grid, kKnnWarps * 32, smem, s>>>(ka);
+        kern<<<grid, kKnnWarps * 32, smem, s>>>(ka);
         if ((e = cudaGetLastError())) {
             fail(e, "launch");
             break;
@@ -586,10 +630,7 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
                 fail(e, "cudaMalloc (tie scratch)");
                 break;
             }
-            if (d_z)
-                knn_heavy_kernel<true><<<g, kHeavyThreads, 0, s>>>(ka, nheavy, sc, (size_t)n);
-            else
-                knn_heavy_kernel<false><<<g, kHeavyThreads, 0, s>>>(ka, nheavy, sc, (size_t)n);
+            heavy<<<g, kHeavyThreads, 0, s>>>(ka, nheavy, sc, (size_t)n);
             if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(s))) {
                 fail(e, "tie pass");
                 break;
@@ -608,13 +649,29 @@ int knn_device(const double *d_x, const double *d_y, const double *d_z, int n, i
 
 static int knn_host(const double *x, const double *y, const double *z, int n, int bc, int cs,
                     const int *batchNumAccum, const double *cx, const double *cy, const double *cz,
-                    int *knn_idx, int device, const unsigned char *mask = nullptr)
+                    int *knn_idx, int device, const unsigned char *mask = nullptr, int earth = 0)
 {
     using namespace bv;
     if (!x || !y || !batchNumAccum || !cx || !cy || !knn_idx || n <= 0 || bc <= 0 || cs < 0 ||
         (z && !cz)) {
         set_error("bv_knn: invalid argument");
         return BV_E_INVALID;
+    }
+    if (earth && z) {
+        // src/ckernel.cpp:170-172: "Great Circle (GC) distance is only valid for 2d".
+        set_error("bv_knn: the great-circle distance is defined for 2-D locations only");
+        return BV_E_INVALID;
+    }
+    // The great-circle key reads cos(latitude) of every point and centroid,
+    // computed here with the host's libm as the reference computes it.
+    std::vector<double> zc, czc;
+    if (earth) {
+        zc.resize(n);
+        czc.resize(bc);
+        for (int p = 0; p < n; ++p) zc[p] = earth_cos_lat(x[p]);
+        for (int b = 0; b < bc; ++b) czc[b] = earth_cos_lat(cx[b]);
+        z = zc.data();
+        cz = czc.data();
     }
     if (batchNumAccum[0] != 0 || batchNumAccum[bc] > n) {
         set_error("bv_knn: batchNumAccum must start at 0 and stay within n");
@@ -650,7 +707,7 @@ static int knn_host(const double *x, const double *y, const double *z, int n, in
             rc = BV_E_CUDA;
             break;
         }
-        rc = knn_device(d_x, d_y, d_z, n, bc, cs, d_acc, cx, cy, cz, d_knn, s, mask);
+        rc = knn_device(d_x, d_y, d_z, n, bc, cs, d_acc, cx, cy, cz, d_knn, s, mask, earth);
         if (rc) break;
         // Block 0 and the selected blocks' sets back to the caller (the
         // others' entries stay as the caller had them).
@@ -711,4 +768,17 @@ extern "C" int bv_knn3(const double *x, const double *y, const double *z, int n,
         return BV_E_INVALID;
     }
     return knn_host(x, y, z, n, bc, cs, batchNumAccum, cx, cy, cz, knn_idx, device);
+}
+
+extern "C" int bv_knn_ex(const double *x, const double *y, const double *z, int n, int bc, int cs,
+                         const int *batchNumAccum, const double *cx, const double *cy,
+                         const double *cz, const unsigned char *mask, int metric, int *knn_idx,
+                         int device)
+{
+    if (metric != BV_METRIC_EUCLIDEAN && metric != BV_METRIC_EARTH) {
+        bv::set_error("bv_knn_ex: unknown distance metric %d", metric);
+        return BV_E_INVALID;
+    }
+    return knn_host(x, y, z, n, bc, cs, batchNumAccum, cx, cy, cz, knn_idx, device, mask,
+                    metric == BV_METRIC_EARTH);
 }

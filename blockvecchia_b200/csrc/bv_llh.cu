@@ -252,6 +252,7 @@ extern "C" void bv_default_opts(bv_opts *o)
     o->shard_index = 0;
     o->large_blocks = BV_LARGE_AUTO;
     o->nugget = 0;
+    o->earth = 0;
 }
 
 // Cost rank (largest first, ties by index) shared by the schedule and the
@@ -667,7 +668,20 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
         handle_free(h);
         return BV_E_INVALID;
     }
-    h->nz = L->z ? 1 : 0;
+    if (h->opts.earth && (L->z || h->opts.kernel == 4)) {
+        // src/ckernel.cpp:170-172: "Great Circle (GC) distance is only valid for 2d".
+        set_error("bv_create: the great-circle distance (earth) is defined for 2-D locations only");
+        handle_free(h);
+        return BV_E_INVALID;
+    }
+    if (h->opts.earth && h->opts.precision == BV_PREC_MIXED) {
+        set_error("bv_create: the mixed-precision path evaluates Euclidean distances only");
+        handle_free(h);
+        return BV_E_INVALID;
+    }
+    // Great-circle layouts run the 3-D kernel instantiations, whose third
+    // coordinate then carries cos(latitude) of every point.
+    h->nz = (L->z || h->opts.earth) ? 1 : 0;
     h->n = L->n;
     h->bc = L->bc;
     h->cs = L->cs;
@@ -720,9 +734,19 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
     BV_CUDA_H(cudaMemcpy(h->d_x, L->x, n * sizeof(double), cudaMemcpyHostToDevice));
     BV_CUDA_H(cudaMemcpy(h->d_y, L->y, n * sizeof(double), cudaMemcpyHostToDevice));
     BV_CUDA_H(cudaMemcpy(h->d_obs, L->obs, n * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<double> ccos;  // centroids' cos(latitude), for the great-circle key
     if (L->z) {
         BV_CUDA_H(cudaMalloc(&h->d_z, n * sizeof(double)));
         BV_CUDA_H(cudaMemcpy(h->d_z, L->z, n * sizeof(double), cudaMemcpyHostToDevice));
+    } else if (h->opts.earth) {
+        std::vector<double> c(n);
+        for (size_t p = 0; p < n; ++p) c[p] = earth_cos_lat(L->x[p]);
+        BV_CUDA_H(cudaMalloc(&h->d_z, n * sizeof(double)));
+        BV_CUDA_H(cudaMemcpy(h->d_z, c.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+        if (L->cx) {
+            ccos.resize(bc);
+            for (size_t b = 0; b < bc; ++b) ccos[b] = earth_cos_lat(L->cx[b]);
+        }
     }
     BV_CUDA_H(cudaMemcpy(h->d_acc, L->batchNumAccum, (bc + 1) * sizeof(int), cudaMemcpyHostToDevice));
     if (h->owned > 0)
@@ -744,7 +768,8 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
                 BV_CUDA_H(cudaMemsetAsync(h->d_knn, 0, bc * cs * sizeof(int), h->stream));
             }
             BV_TRY_H(knn_device(h->d_x, h->d_y, h->d_z, h->n, h->bc, h->cs, h->d_acc, L->cx, L->cy,
-                                L->cz, h->d_knn, h->stream, mine.empty() ? nullptr : mine.data()));
+                                h->opts.earth ? ccos.data() : L->cz, h->d_knn, h->stream,
+                                mine.empty() ? nullptr : mine.data(), h->opts.earth));
             BV_CUDA_H(cudaStreamSynchronize(h->stream));
         }
     }
@@ -794,7 +819,7 @@ static int fill_params(bv_handle *h, const double *theta)
     }
     MaternParams &p = *h->h_mp;
     p.nugget = tau2;
-    p.model = st ? kModelSpaceTime : (h->nz ? kModel3D : kModel2D);
+    p.model = st ? kModelSpaceTime : (h->opts.earth ? kModelEarth : (h->nz ? kModel3D : kModel2D));
     p.st_range_t = p.st_pow = p.st_half = p.st_outer = 0.0;
     if (st) {
         // src/ckernel.cpp:1439-1443 (theta[3..6]).

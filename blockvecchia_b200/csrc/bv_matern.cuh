@@ -23,7 +23,7 @@
 namespace bv {
 
 enum NuKind : int { kNuGeneral = 0, kNuHalf = 1, kNuThreeHalves = 2, kNuFiveHalves = 3 };
-enum Model : int { kModel2D = 0, kModel3D = 1, kModelSpaceTime = 2 };
+enum Model : int { kModel2D = 0, kModel3D = 1, kModelSpaceTime = 2, kModelEarth = 3 };
 
 // Parameters of one evaluation (host-computed scalars).
 struct MaternParams {
@@ -39,7 +39,10 @@ struct MaternParams {
     double nugget;      // tau^2 added to the diagonal of Sigma11 and Sigma22 (0: none,
                         // the reference's likelihood, which never reads theta[3])
     // Locations with a third coordinate (the reference's time_flag):
-    int model;          // kModel2D, kModel3D (core_dcmg with z_flag = 1) or kModelSpaceTime
+    int model;          // kModel2D, kModel3D (core_dcmg with z_flag = 1), kModelSpaceTime,
+                        // or kModelEarth (core_dcmg with distance_metric = 1: x, y are
+                        // latitude, longitude in degrees; the third coordinate carries
+                        // cos(latitude in radians), computed on the host)
     double st_range_t;  // space-time: theta[3]
     double st_pow;      // 2 * theta[4]
     double st_half;     // theta[5] / 2
@@ -322,11 +325,34 @@ __device__ __forceinline__ double matern(double x1, double y1, double x2, double
 //     r = dist / range, g = |dz|^(2 theta[4]) / theta[3] + 1,
 //     C = r == 0 ? sigma2 / g^(theta[5] + theta[6])
 //               : Matern(r / g^(theta[5] / 2)) / g^(theta[5] + theta[6]).
+// distanceEarth (src/ckernel.cpp:145-154): the haversine great-circle
+// distance in km, 2 * 6371 * asin(sqrt(u*u + cos(lat1) cos(lat2) v*v)), u and
+// v the sines of half the latitude and longitude differences, radians =
+// degrees * PI / 180 (PI = 3.141592653589793) rounded as the host rounds it;
+// c1, c2 = cos(lat1), cos(lat2) from the host's libm, and the sum contracted
+// as the reference build contracts it.  The device sin and asin may differ
+// from the host's in the last bit.
+__device__ __forceinline__ double earth_dist(double lat1d, double lon1d, double c1, double lat2d,
+                                             double lon2d, double c2)
+{
+    const double pi = 3.141592653589793;
+    const double lat1r = __ddiv_rn(__dmul_rn(lat1d, pi), 180.0);
+    const double lon1r = __ddiv_rn(__dmul_rn(lon1d, pi), 180.0);
+    const double lat2r = __ddiv_rn(__dmul_rn(lat2d, pi), 180.0);
+    const double lon2r = __ddiv_rn(__dmul_rn(lon2d, pi), 180.0);
+    const double u = sin(__dmul_rn(__dsub_rn(lat2r, lat1r), 0.5));
+    const double v = sin(__dmul_rn(__dsub_rn(lon2r, lon1r), 0.5));
+    const double s = __fma_rn(u, u, __dmul_rn(__dmul_rn(__dmul_rn(c1, c2), v), v));
+    return __dmul_rn(12742.0, asin(__dsqrt_rn(s)));
+}
+
 __device__ __forceinline__ double cov_xyz(double x1, double y1, double z1, double x2, double y2,
                                           double z2, const MaternParams &p)
 {
     const double dx = x2 - x1, dy = y2 - y1, dz = z2 - z1;
-    const double dist = __dsqrt_rn(__fma_rn(dz, dz, __fma_rn(dx, dx, __dmul_rn(dy, dy))));
+    const double dist = (p.model == kModelEarth)
+                            ? earth_dist(x1, y1, z1, x2, y2, z2)
+                            : __dsqrt_rn(__fma_rn(dz, dz, __fma_rn(dx, dx, __dmul_rn(dy, dy))));
     double r = div_by_recip(dist, p.range, p.inv_range);
     if (p.model != kModelSpaceTime) {
         if (!p.scale_is_one) r = div_by_recip(r, p.dist_scale, p.inv_ds);

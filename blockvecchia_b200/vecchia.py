@@ -176,27 +176,24 @@ def order_centroids(x, y, z=None, ordering="random"):
     return (x, y) if z is None else (x, y, z)
 
 
-def knn(layout: Layout, device: int = 0, mask=None) -> np.ndarray:
+def knn(layout: Layout, device: int = 0, mask=None, earth: bool = False) -> np.ndarray:
     """Conditioning sets on the device (findNearestPoints semantics; the
-    time_flag key when the layout has a third coordinate).  mask (bool per
-    block, e.g. shard_blocks): only those blocks' sets are selected; the
-    other entries are zero."""
+    time_flag key when the layout has a third coordinate; the great-circle
+    key of --earth with earth=True, x latitude and y longitude in degrees).
+    mask (bool per block, e.g. shard_blocks): only those blocks' sets are
+    selected; the other entries are zero."""
     L = layout.normalized()
     out = np.zeros(L.bc * L.cs, dtype=np.int32)
+    nd = C.POINTER(C.c_double)()
+    m = None
     if mask is not None:
         m = np.ascontiguousarray(np.asarray(mask, dtype=bool).astype(np.uint8))
-        nd = C.POINTER(C.c_double)()
-        check(lib().bv_knn_subset(dp(L.x), dp(L.y), dp(L.z) if L.z is not None else nd, L.n, L.bc,
-                                  L.cs, ip(L.batchNumAccum), dp(L.cx), dp(L.cy),
-                                  dp(L.cz) if L.cz is not None else nd,
-                                  m.ctypes.data_as(C.POINTER(C.c_ubyte)), ip(out), int(device)))
-        return out
-    if L.z is not None:
-        check(lib().bv_knn3(dp(L.x), dp(L.y), dp(L.z), L.n, L.bc, L.cs, ip(L.batchNumAccum),
-                            dp(L.cx), dp(L.cy), dp(L.cz), ip(out), int(device)))
-        return out
-    check(lib().bv_knn(dp(L.x), dp(L.y), L.n, L.bc, L.cs, ip(L.batchNumAccum), dp(L.cx), dp(L.cy),
-                       ip(out), int(device)))
+    check(lib().bv_knn_ex(dp(L.x), dp(L.y), dp(L.z) if L.z is not None else nd, L.n, L.bc, L.cs,
+                          ip(L.batchNumAccum), dp(L.cx), dp(L.cy),
+                          dp(L.cz) if L.cz is not None else nd,
+                          m.ctypes.data_as(C.POINTER(C.c_ubyte)) if m is not None
+                          else C.POINTER(C.c_ubyte)(),
+                          1 if earth else 0, ip(out), int(device)))
     return out
 
 
@@ -214,7 +211,7 @@ class LlhData:
                  dist_scale: float = 1.0, device: int = 0, on_failure: str = "neginf",
                  print_iter: bool = False, use_graph: bool = True, schedule: str = "auto",
                  mixed_tol: float = 1e-8, shard_count: int = 1, shard_index: int = 0,
-                 large_blocks: str = "auto", nugget: bool = False):
+                 large_blocks: str = "auto", nugget: bool = False, earth: bool = False):
         L = layout.normalized()
         self.layout = L
         o = _lib.BvOpts()
@@ -232,6 +229,7 @@ class LlhData:
         o.shard_index = int(shard_index)
         o.large_blocks = _LARGE[large_blocks]
         o.nugget = int(bool(nugget))
+        o.earth = int(bool(earth))
         null_i = C.POINTER(C.c_int)()
         null_d = C.POINTER(C.c_double)()
         self._l = _lib.BvLayout(L.n, L.bc, L.cs, ip(L.batchNum), ip(L.batchNumAccum), dp(L.x),

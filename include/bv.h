@@ -123,7 +123,19 @@ typedef struct {
                           tau^2 >= 0 is added to the diagonal of Sigma11 and
                           Sigma22 (a point with itself), and bv_llh needs
                           n >= 4 parameters.                                  */
+    int earth;         /* 0 (default): Euclidean distances.  1: the
+                          reference's --earth (distance_metric = 1): x is the
+                          latitude and y the longitude in degrees, distances
+                          are great-circle km by the haversine formula
+                          (src/ckernel.cpp:145-154) in the covariance and in
+                          the conditioning-set key when the handle selects
+                          the sets.  2-D Matern kernels (1-3) and FP64 only,
+                          as the reference allows it for 2-D locations only. */
 } bv_opts;
+
+/* Distance metrics of bv_knn_ex (the reference's distance_metric). */
+#define BV_METRIC_EUCLIDEAN 0
+#define BV_METRIC_EARTH     1
 
 typedef struct {
     int blocks;          /* blocks evaluated                                 */
@@ -147,7 +159,7 @@ typedef struct {
 typedef struct bv_handle bv_handle;
 
 /* Fill *o with the defaults (FP64, Matern, dist_scale 1, device 0,
- * BV_FAIL_NEGINF, no printing, graphs on, persistent schedule). */
+ * BV_FAIL_NEGINF, no printing, graphs on, BV_SCHED_AUTO, Euclidean). */
 void bv_default_opts(bv_opts *o);
 
 /* Create a handle: validates the layout, copies it to the device once
@@ -307,6 +319,19 @@ int bv_knn(const double *x, const double *y, int n, int bc, int cs,
 int bv_knn3(const double *x, const double *y, const double *z, int n, int bc, int cs,
             const int *batchNumAccum, const double *cx, const double *cy,
             const double *cz, int *knn_idx, int device);
+
+/* Conditioning sets with every option: z/cz (3-D locations) may be NULL,
+ * mask (may be NULL) selects blocks as bv_knn_subset does, and metric is
+ * BV_METRIC_EUCLIDEAN or BV_METRIC_EARTH (findNearestPoints with
+ * distance_metric = 1, include/nearest_neighbor.h:93-96: great-circle km
+ * from the centroid, x latitude and y longitude in degrees; 2-D only).  The
+ * great-circle key uses the device's sin and asin, which may differ from the
+ * host libm's in the last bit: two candidates whose distances agree to a few
+ * ulps may then be ordered differently from the reference. */
+int bv_knn_ex(const double *x, const double *y, const double *z, int n, int bc, int cs,
+              const int *batchNumAccum, const double *cx, const double *cy,
+              const double *cz, const unsigned char *mask, int metric, int *knn_idx,
+              int device);
 
 /* Conditioning sets of a subset of the blocks (one rank's shard, mask from
  * bv_shard_blocks): blocks b >= 1 with mask[b] != 0 get their sets (and

@@ -199,6 +199,42 @@ void bvo_matern(double *A, int m, int n,
     }
 }
 
+/* distanceEarth (src/ckernel.cpp:145-154, include/nearest_neighbor.h:64-74):
+ * great-circle distance in km between (latitude, longitude) pairs in degrees
+ * by the haversine formula, deg2rad(d) = d * PI / 180, PI = 3.141592653589793;
+ * the reference build contracts u*u + cos(lat1)*cos(lat2)*v*v into
+ * fma(u, u, ((cos(lat1)*cos(lat2))*v)*v). */
+double bvo_earth_dist(double lat1d, double lon1d, double lat2d, double lon2d)
+{
+    const double pi = 3.141592653589793;
+    double lat1r = lat1d * pi / 180, lon1r = lon1d * pi / 180;
+    double lat2r = lat2d * pi / 180, lon2r = lon2d * pi / 180;
+    double u = sin((lat2r - lat1r) / 2);
+    double v = sin((lon2r - lon1r) / 2);
+    double c = cos(lat1r) * cos(lat2r);
+    return 2.0 * 6371.0 * asin(sqrt(fma(u, u, (c * v) * v)));
+}
+
+/* core_dcmg with distance_metric = 1 (--earth, 2-D only): x = latitude,
+ * y = longitude in degrees, distances in km. */
+void bvo_matern_earth(double *A, int m, int n, const double *x1, const double *y1,
+                      const double *x2, const double *y2, const double *theta,
+                      double dist_scale)
+{
+    double sigma_square = theta[0];
+    double con = pow(2.0, theta[2] - 1.0) * tgamma(theta[2]);
+    con = 1.0 / con;
+    con = sigma_square * con;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < n; ++j) {
+            double expr = bvo_earth_dist(x1[i], y1[i], x2[j], y2[j]) / theta[1];
+            expr /= dist_scale;
+            A[i + (size_t)j * m] = (expr == 0)
+                                       ? sigma_square
+                                       : con * pow(expr, theta[2]) * bvo_besselk(theta[2], expr);
+        }
+}
+
 /* core_dcmg with z_flag = 1 (the --3D / time_flag distance,
  * src/ckernel.cpp:165-186 with the third coordinate):
  * sqrt(pow(dx,2)+pow(dy,2)+pow(dz,2)), which the reference build contracts to
@@ -416,6 +452,64 @@ int bvo_knn_block3_fast(const double *x, const double *y, const double *z,
     return k;
 }
 
+/* bvo_knn_block_fast with findNearestPoints' distance_metric = 1 key
+ * (include/nearest_neighbor.h:93-96): distanceEarth(centroid, point). */
+int bvo_knn_block_earth_fast(const double *x, const double *y, int prefix,
+                             double cx, double cy, int k, int *out_idx)
+{
+    if (prefix <= 0 || k <= 0) return 0;
+    if (k > prefix) k = prefix;
+    double *dist = (double *)malloc(sizeof(double) * (size_t)prefix);
+    double *tmp = (double *)malloc(sizeof(double) * (size_t)prefix);
+    for (int p = 0; p < prefix; ++p) {
+        dist[p] = bvo_earth_dist(cx, cy, x[p], y[p]);
+        tmp[p] = dist[p];
+    }
+    double dk = bvo_select_kth(tmp, prefix, k - 1);
+    int m = 0;
+    for (int p = 0; p < prefix; ++p)
+        if (dist[p] <= dk) tmp[m++] = (double)p;
+    int *sidx = (int *)malloc(sizeof(int) * (size_t)m);
+    int *pos = (int *)malloc(sizeof(int) * (size_t)m);
+    for (int e = 0; e < m; ++e) {
+        sidx[e] = (int)tmp[e];
+        pos[e] = sidx[e];
+    }
+    for (int t = 0; t < k; ++t) {
+        int best = -1, occ = -1;
+        for (int e = 0; e < m; ++e) {
+            if (pos[e] < 0) continue;
+            if (best < 0 || dist[sidx[e]] < dist[sidx[best]] ||
+                (dist[sidx[e]] == dist[sidx[best]] && pos[e] < pos[best]))
+                best = e;
+            if (pos[e] == t) occ = e;
+        }
+        out_idx[t] = sidx[best];
+        if (occ >= 0 && occ != best) pos[occ] = pos[best];
+        pos[best] = -1;
+    }
+    free(dist);
+    free(tmp);
+    free(sidx);
+    free(pos);
+    return k;
+}
+
+void bvo_knn_all_earth_fast(const double *x, const double *y, int bc, int cs,
+                            const int *batchNumAccum, const double *cx,
+                            const double *cy, int *knn_idx, int threads)
+{
+    for (int t = 0; t < cs; ++t) knn_idx[t] = t;
+#ifdef _OPENMP
+    int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+#endif
+    for (int i = 1; i < bc; ++i)
+        bvo_knn_block_earth_fast(x, y, batchNumAccum[i], cx[i], cy[i], cs,
+                                 knn_idx + (size_t)i * cs);
+    (void)threads;
+}
+
 void bvo_knn_all_fast(const double *x, const double *y, int bc, int cs,
                       const int *batchNumAccum, const double *cx,
                       const double *cy, int *knn_idx, int threads)
@@ -520,7 +614,9 @@ static void bvo_cov(const bvo_problem *p, const double *theta, double *A, int m,
                     const double *x1, const double *y1, const double *z1,
                     const double *x2, const double *y2, const double *z2)
 {
-    if (!p->z)
+    if (p->earth)
+        bvo_matern_earth(A, m, n, x1, y1, x2, y2, theta, p->dist_scale);
+    else if (!p->z)
         bvo_matern(A, m, n, x1, y1, x2, y2, theta, p->dist_scale);
     else if (p->spacetime)
         bvo_matern_st(A, m, n, x1, y1, z1, x2, y2, z2, theta);

@@ -87,6 +87,19 @@ void bvo_knn_all_fast(const double *x, const double *y, int bc, int cs,
                       const int *batchNumAccum, const double *cx,
                       const double *cy, int *knn_idx, int threads);
 
+/* --earth (distance_metric = 1): distanceEarth in km for (latitude,
+ * longitude) in degrees (src/ckernel.cpp:145-154), core_dcmg with it, and
+ * findNearestPoints with it (include/nearest_neighbor.h:93-96). */
+double bvo_earth_dist(double lat1d, double lon1d, double lat2d, double lon2d);
+void bvo_matern_earth(double *A, int m, int n, const double *x1, const double *y1,
+                      const double *x2, const double *y2, const double *theta,
+                      double dist_scale);
+int bvo_knn_block_earth_fast(const double *x, const double *y, int prefix,
+                             double cx, double cy, int k, int *out_idx);
+void bvo_knn_all_earth_fast(const double *x, const double *y, int bc, int cs,
+                            const int *batchNumAccum, const double *cx,
+                            const double *cy, int *knn_idx, int threads);
+
 /* The problem one log-likelihood evaluation reads (the llh_data fields of
  * include/vecchia_helper_data.h:69-146 that the FP64 Matern path uses). */
 typedef struct {
@@ -103,6 +116,8 @@ typedef struct {
                                  0 = the reference's likelihood (no nugget)  */
     const double *z;          /* [n] third coordinate (time_flag), or NULL  */
     int spacetime;            /* 1: core_dcmg_spacetime_matern, theta[7]     */
+    int earth;                /* 1: distance_metric = 1 (--earth): x, y are
+                                 latitude, longitude in degrees (2-D only)   */
 } bvo_problem;
 
 /* Per-block result of the restated likelihood. */

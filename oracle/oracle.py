@@ -48,7 +48,7 @@ class Problem(C.Structure):
                 ("batchNum", _I), ("batchNumAccum", _I),
                 ("x", _D), ("y", _D), ("obs", _D), ("knn_idx", _I),
                 ("dist_scale", C.c_double), ("nugget", C.c_double),
-                ("z", _D), ("spacetime", C.c_int)]
+                ("z", _D), ("spacetime", C.c_int), ("earth", C.c_int)]
 
 
 _lib = None
@@ -69,6 +69,11 @@ def lib():
         L.bvo_knn_block.argtypes = [_D, _D, C.c_int, C.c_double, C.c_double, C.c_int, _I]
         L.bvo_knn_all.argtypes = [_D, _D, C.c_int, C.c_int, _I, _D, _D, _I]
         L.bvo_knn_all_fast.argtypes = [_D, _D, C.c_int, C.c_int, _I, _D, _D, _I, C.c_int]
+        L.bvo_earth_dist.restype = C.c_double
+        L.bvo_earth_dist.argtypes = [C.c_double] * 4
+        L.bvo_matern_earth.argtypes = [_D, C.c_int, C.c_int, _D, _D, _D, _D, _D, C.c_double]
+        L.bvo_knn_block_earth_fast.argtypes = [_D, _D, C.c_int, C.c_double, C.c_double, C.c_int, _I]
+        L.bvo_knn_all_earth_fast.argtypes = [_D, _D, C.c_int, C.c_int, _I, _D, _D, _I, C.c_int]
         L.bvo_matern3.argtypes = [_D, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, _D, C.c_double]
         L.bvo_matern_st.argtypes = [_D, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, _D]
         L.bvo_knn_block3_fast.restype = C.c_int
@@ -111,6 +116,9 @@ def ref():
         L.ref_layout_from_clusters3.restype = C.c_int
         L.ref_layout_from_clusters3.argtypes = [_D, _D, _D, _D, C.c_int, C.c_int, _I, _D, _D, _D,
                                                 C.c_int, _I, _I, _D, _D, _D, _D, _D, _D, _D, _I, _I]
+        L.ref_core_dcmg_earth.argtypes = [_D, C.c_int, C.c_int, _D, _D, _D, _D, _D, C.c_double]
+        L.ref_find_nearest_earth.argtypes = [_D, _D, C.c_int, C.c_int, C.c_double, C.c_double,
+                                             C.c_int, _I]
         L.ref_order_centroids.argtypes = [C.c_int, C.c_int, _D, _D, _D]
         L.ref_layout_from_clusters_ord.restype = C.c_int
         L.ref_layout_from_clusters_ord.argtypes = [_D, _D, _D, _D, C.c_int, C.c_int, _I, _D, _D, _D,
@@ -250,7 +258,7 @@ class OracleProblem:
     """Holds numpy arrays alive behind a bvo_problem."""
 
     def __init__(self, batchNum, batchNumAccum, x, y, obs, knn_idx, cs, dist_scale=1.0, nugget=0.0,
-                 z=None, spacetime=False):
+                 z=None, spacetime=False, earth=False):
         self.batchNum = np.ascontiguousarray(batchNum, dtype=np.int32)
         self.batchNumAccum = np.ascontiguousarray(batchNumAccum, dtype=np.int32)
         self.x = np.ascontiguousarray(x, dtype=np.float64)
@@ -266,6 +274,7 @@ class OracleProblem:
         if self.z is not None:
             self.p.z = _dp(self.z)
             self.p.spacetime = int(bool(spacetime))
+        self.p.earth = int(bool(earth))
 
 
 def llh(prob: OracleProblem, theta, threads: int = 0, per_block: bool = False):
@@ -443,3 +452,41 @@ def ref_layout_from_clusters_ord(x, y, obs, labels, cx, cy, cs, ordering, z=None
     if tf:
         out.update(z=zn, cz=bcz[:bc].copy())
     return out
+
+
+def matern_earth(x1, y1, x2, y2, theta, dist_scale=1.0):
+    """core_dcmg with distance_metric = 1 (--earth): x latitude, y longitude
+    in degrees, great-circle distances in km."""
+    x1, y1, x2, y2 = (_c(a) for a in (x1, y1, x2, y2))
+    th = _c(theta)
+    A = np.zeros((len(x1), len(x2)), order="F")
+    lib().bvo_matern_earth(A.ctypes.data_as(_D), len(x1), len(x2), _dp(x1), _dp(y1), _dp(x2), _dp(y2),
+                           _dp(th), float(dist_scale))
+    return A
+
+
+def knn_all_earth_fast(x, y, cs, batchNumAccum, cx, cy, threads=0):
+    """Every block's conditioning set with the great-circle key."""
+    x, y, cx, cy = (_c(a) for a in (x, y, cx, cy))
+    acc = np.ascontiguousarray(batchNumAccum, dtype=np.int32)
+    bc = len(acc) - 1
+    out = np.zeros(bc * cs, dtype=np.int32)
+    lib().bvo_knn_all_earth_fast(_dp(x), _dp(y), bc, cs, _ip(acc), _dp(cx), _dp(cy), _ip(out),
+                                 int(threads))
+    return out
+
+
+def ref_core_dcmg_earth(x1, y1, x2, y2, theta, dist_scale=1.0):
+    x1, y1, x2, y2 = (_c(a) for a in (x1, y1, x2, y2))
+    th = _c(theta)
+    A = np.zeros((len(x1), len(x2)), order="F")
+    ref().ref_core_dcmg_earth(A.ctypes.data_as(_D), len(x1), len(x2), _dp(x1), _dp(y1), _dp(x2),
+                              _dp(y2), _dp(th), float(dist_scale))
+    return A
+
+
+def ref_find_nearest_earth(x, y, prefix, cx, cy, k):
+    out = np.zeros(k, dtype=np.int32)
+    ref().ref_find_nearest_earth(_dp(_c(x)), _dp(_c(y)), len(x), int(prefix), float(cx), float(cy),
+                                 int(k), _ip(out))
+    return out[:min(k, prefix)]

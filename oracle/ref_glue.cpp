@@ -61,6 +61,35 @@ void ref_core_dcmg(double *A, int m, int n, double *x1, double *y1,
     core_dcmg(A, m, n, &l1, &l2, theta, 0, 0, dist_scale);
 }
 
+/* core_dcmg with distance_metric = 1 (--earth), 2-D. */
+void ref_core_dcmg_earth(double *A, int m, int n, double *x1, double *y1,
+                         double *x2, double *y2, const double *theta,
+                         double dist_scale)
+{
+    location l1 = {x1, y1, nullptr};
+    location l2 = {x2, y2, nullptr};
+    core_dcmg(A, m, n, &l1, &l2, theta, 1, 0, dist_scale);
+}
+
+/* findNearestPoints with distance_metric = 1 (see ref_find_nearest). */
+void ref_find_nearest_earth(const double *x, const double *y, int n, int prefix,
+                            double cx, double cy, int k, int *out_idx)
+{
+    std::vector<double> obs(n), xs(x, x + n), ys(y, y + n);
+    for (int p = 0; p < n; ++p) obs[p] = (double)p;
+    std::vector<double> cond_obs((size_t)2 * k), cond_x((size_t)2 * k),
+        cond_y((size_t)2 * k);
+    location con = {cond_x.data(), cond_y.data(), nullptr};
+    double cxv[2] = {cx, cx}, cyv[2] = {cy, cy};
+    location cent = {cxv, cyv, nullptr};
+    int fcc = 1;
+    location lnew = {xs.data(), ys.data(), nullptr};
+    findNearestPoints(cond_obs.data(), &con, &cent, &fcc, obs.data(), &lnew, 0,
+                      prefix, k, 1, 1, false);
+    int kk = k < prefix ? k : prefix;
+    for (int t = 0; t < kk; ++t) out_idx[t] = (int)cond_obs[(size_t)kk + t];
+}
+
 /* findNearestPoints (include/nearest_neighbor.h:76-148) for block i_block,
  * with observations set to the point index so that the gathered
  * "observations" are the selected indices. */

@@ -51,7 +51,8 @@ def test_question_mark_keeps_value(exe):
 
 
 @pytest.mark.parametrize("bad", [["--tol", "0"], ["--maxiter", "-3"], ["--upper_bound", "200"],
-                                 ["--permutation", "zigzag"], ["--earth", "1"], ["--kernel", "foo"],
+                                 ["--permutation", "zigzag"], ["--earth", "1"], ["--earth", "--3D", "1"],
+                                 ["--kernel", "foo"],
                                  ["--kernel", "univariate_matern_spacetime_stationary", "--t_slots", "3",
                                   "--num_loc", "1000", "--perf", "1"]])
 def test_rejected(exe, bad):
@@ -77,3 +78,11 @@ def test_permutation_flag(exe, name, code):
     """--permutation (include/vecchia_helper_data.h:456-476)."""
     o = _opts(exe, "--permutation", name)
     assert o["permutation"] == name and o["ordering"] == code
+
+
+def test_earth_flag(exe):
+    """--earth (include/vecchia_helper_data.h:451-454) sets the great-circle
+    metric and does not consume the next argument ("--earth 1" leaves "1" as
+    an unrecognised option, as in the reference)."""
+    o = _opts(exe, "--earth", "--num_loc", "5000")
+    assert o["earth"] == 1 and o["num_loc"] == 5000

@@ -124,3 +124,31 @@ def test_fit_c1_matches_oracle_fit(exe, bvlib, oracle, tmp_path):
     print({"device": th.tolist(), "oracle": ref_th.tolist(), "llk": llk, "oracle_llk": ref_llk})
     assert np.all(np.abs(th - ref_th) <= 1e-3 * np.abs(ref_th)), (th, ref_th)
     assert abs(llk - ref_llk) <= 1e-8 * abs(ref_llk), (llk, ref_llk)
+
+
+def test_earth_one_evaluation_matches_oracle(exe, bvlib, oracle, tmp_path):
+    """--earth on latitude/longitude files with --dist_scale: the first
+    evaluation (at --kernel_init) against the oracle's great-circle
+    likelihood on the same layout and conditioning sets."""
+    n, bc, cs = 4000, 300, 50
+    rng = np.random.default_rng(3)
+    lat, lon = rng.uniform(-50, 50, n), rng.uniform(-120, 120, n)
+    z = rng.standard_normal(n)
+    np.savetxt(tmp_path / "xy.csv", np.stack([lat, lon], 1), delimiter=",", fmt="%.17g")
+    np.savetxt(tmp_path / "z.csv", z, fmt="%.17g")
+    r = subprocess.run([exe, "--num_loc", str(n), "--vecchia_bc", str(bc), "--vecchia_cs", str(cs),
+                        "--xy_path", "xy.csv", "--obs_path", "z.csv", "--kernel_init", "1.0:0.7:0.5",
+                        "--dist_scale", "1000", "--earth", "--maxiter", "1", "--seed", "0"],
+                       capture_output=True, text=True, timeout=600, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    m = re.findall(r"Model Parameters \(Variance, range, smoothness\): \(([-\d.e]+), ([-\d.e]+), "
+                   r"([-\d.e]+)\) -> Loglik: ([-\d.eE+]+)", r.stdout)
+    assert m, r.stdout
+    llk = float(m[0][3])
+    L = bvlib.build_layout(lat, lon, z, bc, cs, seed=0, epochs=50)
+    knn = oracle.knn_all_earth_fast(L.x, L.y, cs, L.batchNumAccum, L.cx, L.cy)
+    P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, knn, cs,
+                             dist_scale=1000.0, earth=True)
+    ref = oracle.llh(P, (1.0, 0.7, 0.5))
+    # The CLI prints the log-likelihood with 6 decimals.
+    assert abs(llk - ref) <= max(1e-10 * abs(ref), 1e-6), (llk, ref)

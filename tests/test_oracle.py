@@ -263,3 +263,56 @@ def test_generate_xyt_and_3d_layout_pins(ref, bvlib):
     assert bc == L.bc and np.array_equal(bn[:bc], L.batchNum)
     for a, b in [(xn, L.x), (yn, L.y), (zn, L.z), (on, L.obs), (bcx[:bc], L.cx), (bcz[:bc], L.cz)]:
         assert np.array_equal(a, b)
+
+
+# ------------------------------------------------------ great-circle metric
+
+def test_earth_golden_bitexact(oracle):
+    """--earth (distance_metric = 1): the oracle's haversine covariance and
+    conditioning sets equal the reference's (fixtures from its own code)."""
+    g = golden("earth.npz")
+    lat, lon = g["lat"], g["lon"]
+    for t in range(2):
+        A = oracle.matern_earth(lat[:60], lon[:60], lat[60:140], lon[60:140], g[f"theta_{t}"])
+        assert np.array_equal(A, g[f"cov_{t}"]), t
+    for s in range(6):
+        prefix, cx, cy, k = g[f"knn_{s}_args"]
+        out = np.zeros(int(k), dtype=np.int32)
+        oracle.lib().bvo_knn_block_earth_fast(oracle._dp(oracle._c(lat)), oracle._dp(oracle._c(lon)),
+                                              int(prefix), float(cx), float(cy), int(k),
+                                              oracle._ip(out))
+        assert np.array_equal(out, g[f"knn_{s}"]), s
+
+
+def test_earth_live_pins_against_reference(ref):
+    rng = np.random.default_rng(11)
+    lat, lon = rng.uniform(-80, 80, 500), rng.uniform(-179, 179, 500)
+    for th in [(1.0, 700.0, 0.5), (1.0, 2000.0, 2.5), (2.0, 300.0, 0.9)]:
+        assert np.array_equal(ref.matern_earth(lat, lon, lat[:50], lon[:50], th, 3.0),
+                              ref.ref_core_dcmg_earth(lat, lon, lat[:50], lon[:50], th, 3.0))
+    acc = np.array([0, 100, 180, 333, 500], dtype=np.int32)
+    cx, cy = rng.uniform(-80, 80, 4), rng.uniform(-179, 179, 4)
+    got = ref.knn_all_earth_fast(lat, lon, 90, acc, cx, cy)
+    for i in range(1, 4):
+        assert np.array_equal(got[i * 90:(i + 1) * 90],
+                              ref.ref_find_nearest_earth(lat, lon, int(acc[i]), cx[i], cy[i], 90))
+
+
+def test_llh_exact_earth(oracle):
+    """Two blocks, the second conditioned on all of the first: the exact
+    Gaussian log-density under the great-circle covariance."""
+    scipy_stats = pytest.importorskip("scipy.stats")
+    rng = np.random.default_rng(4)
+    cs, bs1 = 40, 11
+    n = cs + bs1
+    lat, lon = rng.uniform(-40, 40, n), rng.uniform(-90, 90, n)
+    z = rng.standard_normal(n)
+    bn = np.array([cs, bs1], dtype=np.int32)
+    acc = np.array([0, cs, n], dtype=np.int32)
+    knn = np.concatenate([np.arange(cs), rng.permutation(cs)]).astype(np.int32)
+    P = oracle.OracleProblem(bn, acc, lat, lon, z, knn, cs, dist_scale=1000.0, earth=True)
+    for th in [(1.5, 1.2, 0.5), (0.9, 0.8, 1.5)]:
+        Sigma = oracle.matern_earth(lat, lon, lat, lon, th, 1000.0)
+        exact = scipy_stats.multivariate_normal(mean=np.zeros(n), cov=Sigma).logpdf(z)
+        v = oracle.llh(P, th)
+        assert abs(v - exact) <= 1e-10 * abs(exact), (th, v, exact)
