@@ -103,14 +103,15 @@ class BvOpts(C.Structure):
                 ("device", C.c_int), ("on_failure", C.c_int), ("print_iter", C.c_int),
                 ("use_graph", C.c_int), ("schedule", C.c_int), ("mixed_tol", C.c_double),
                 ("shard_count", C.c_int), ("shard_index", C.c_int), ("large_blocks", C.c_int),
-                ("nugget", C.c_int), ("earth", C.c_int)]
+                ("nugget", C.c_int), ("earth", C.c_int), ("tune", C.c_int)]
 
 
 class BvStatus(C.Structure):
     _fields_ = [("blocks", C.c_int), ("cond_fail", C.c_int), ("schur_fail", C.c_int),
                 ("fp32_fallback", C.c_int), ("nonfinite", C.c_int), ("flags_or", C.c_uint),
                 ("llk", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double),
-                ("failed", C.c_int), ("launches", C.c_int), ("streamed_blocks", C.c_int)]
+                ("failed", C.c_int), ("launches", C.c_int), ("streamed_blocks", C.c_int),
+                ("streamed_threads", C.c_int), ("tune_ms", C.c_double * 3)]
 
 
 class BvJobOpts(C.Structure):

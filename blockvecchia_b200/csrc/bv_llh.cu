@@ -168,6 +168,11 @@ struct bv_handle {
     double *d_slab_lean = nullptr;  // per-CTA slabs of the multi-CTA streamed launch
     int lean_max_m = 0;             // blocks with M <= this run the multi-CTA streamed kernel
     int streamed_blocks = 0;        // of the owned blocks, how many that is
+    // The streamed launch's order positions and largest M, its CTA size
+    // (kLeanVariants index; -1: from the table), and the tuner's record.
+    int lean_begin = 0, lean_end = 0, lean_m = 0, lean_choice = -1, lean_threads = 0;
+    bool tuned = false;
+    double tune_ms[3] = {0.0, 0.0, 0.0};
     MaternParams *d_mp = nullptr;
     EvalResult *d_res = nullptr;
     MixedWork mixed;  // mixed-precision scratch (bv_llh_mixed.cuh)
@@ -253,6 +258,7 @@ extern "C" void bv_default_opts(bv_opts *o)
     o->large_blocks = BV_LARGE_AUTO;
     o->nugget = 0;
     o->earth = 0;
+    o->tune = 0;
 }
 
 // Cost rank (largest first, ties by index) shared by the schedule and the
@@ -391,7 +397,11 @@ static int order_m(const bv_handle *h, int t)
 // largest block has M = max_m.
 static int plan_lean_launch(bv_handle *h, const cudaDeviceProp &prop, int begin, int end, int max_m)
 {
-    const LeanVariant &v = kLeanVariants[lean_variant(max_m)];
+    const LeanVariant &v = kLeanVariants[h->lean_choice >= 0 ? h->lean_choice : lean_variant(max_m)];
+    h->lean_begin = begin;
+    h->lean_end = end;
+    h->lean_m = max_m;
+    h->lean_threads = v.threads;
     void (*const kern)(LlhArgs) = h->nz ? v.kernel3 : v.kernel;
     cudaFuncAttributes fa;
     BV_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
@@ -533,6 +543,8 @@ static cudaError_t record_timing(cudaEvent_t ev, cudaStream_t s)
     return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal)
                                                : cudaEventRecord(ev, s);
 }
+
+static int capture_graph(bv_handle *h);
 
 static int enqueue_eval(bv_handle *h, cudaStream_t s)
 {
@@ -779,20 +791,7 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
         for (int t = 0; t < h->owned; ++t) max_bs = std::max(max_bs, h->batchNum[h->order[t]]);
         BV_TRY_H(mixed_create(h->mixed, h->device, h->bc, h->cs, max_bs, h->order.data(), h->owned));
     }
-    if (h->opts.use_graph) {
-        BV_CUDA_H(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-        int erc = enqueue_eval(h, h->stream);
-        cudaGraph_t g = nullptr;
-        cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
-        if (erc || ce != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            if (!erc) set_error("graph capture: %s", cudaGetErrorString(ce));
-            handle_free(h);
-            return erc ? erc : BV_E_CUDA;
-        }
-        h->graph = g;
-        BV_CUDA_H(cudaGraphInstantiate(&h->gexec, h->graph, 0));
-    }
+    if (h->opts.use_graph) BV_TRY_H(capture_graph(h));
 #undef BV_TRY_H
 #undef BV_CUDA_H
     *out = h;
@@ -852,11 +851,79 @@ static int fill_params(bv_handle *h, const double *theta)
     return BV_OK;
 }
 
+// One evaluation captured into the handle's graph (replacing any earlier).
+static int capture_graph(bv_handle *h)
+{
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->gexec = nullptr;
+    h->graph = nullptr;
+    BV_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int erc = enqueue_eval(h, h->stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+    if (erc || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (!erc) set_error("graph capture: %s", cudaGetErrorString(ce));
+        return erc ? erc : BV_E_CUDA;
+    }
+    h->graph = g;
+    BV_CUDA_TRY(cudaGraphInstantiate(&h->gexec, h->graph, 0));
+    return BV_OK;
+}
+
+// The streamed launch (always the last one planned) again, with CTA size vi.
+static int replan_lean(bv_handle *h, int vi)
+{
+    cudaDeviceProp prop;
+    BV_CUDA_TRY(cudaGetDeviceProperties(&prop, h->device));
+    h->launches.pop_back();
+    cudaFree(h->d_slab_lean);
+    h->d_slab_lean = nullptr;
+    h->lean_choice = vi;
+    return plan_lean_launch(h, prop, h->lean_begin, h->lean_end, h->lean_m);
+}
+
+// bv_opts.tune: on the first evaluation, time the streamed kernel at every
+// CTA size (twice each, the faster kept) and keep the fastest.  The sizes
+// give the same bits, so the evaluation's value does not depend on it.
+static int tune_lean(bv_handle *h)
+{
+    h->tuned = true;
+    int best = h->lean_choice >= 0 ? h->lean_choice : lean_variant(h->lean_m);
+    double best_ms = 1e300;
+    for (int vi = 0; vi < (int)(sizeof(kLeanVariants) / sizeof(kLeanVariants[0])); ++vi) {
+        int rc = replan_lean(h, vi);
+        if (rc) return rc;
+        double t = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {
+            rc = enqueue_eval(h, h->stream);
+            if (rc) return rc;
+            BV_CUDA_TRY(cudaStreamSynchronize(h->stream));
+            float kms = 0.f;
+            BV_CUDA_TRY(cudaEventElapsedTime(&kms, h->evk0, h->evk1));
+            t = std::min(t, (double)kms);
+        }
+        h->tune_ms[vi] = t;
+        if (t < best_ms) {
+            best_ms = t;
+            best = vi;
+        }
+    }
+    int rc = replan_lean(h, best);
+    if (rc) return rc;
+    return h->opts.use_graph ? capture_graph(h) : BV_OK;
+}
+
 static int eval_locked(bv_handle *h, const double *theta, double *llk)
 {
     int rc = fill_params(h, theta);
     if (rc) return rc;
     BV_CUDA_TRY(cudaSetDevice(h->device));
+    if (h->opts.tune && !h->tuned && h->streamed_blocks > 0 && h->opts.precision == BV_PREC_FP64) {
+        rc = tune_lean(h);
+        if (rc) return rc;
+    }
     BV_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
     if (h->gexec) {
         BV_CUDA_TRY(cudaGraphLaunch(h->gexec, h->stream));
@@ -882,6 +949,8 @@ static int eval_locked(bv_handle *h, const double *theta, double *llk)
     // mixed pass, FP64 fallback pass and the reduction.
     s.launches = h->opts.precision == BV_PREC_MIXED ? 5 : (int)h->launches.size() + 1;
     s.streamed_blocks = h->opts.precision == BV_PREC_MIXED ? 0 : h->streamed_blocks;
+    s.streamed_threads = s.streamed_blocks > 0 ? h->lean_threads : 0;
+    for (int i = 0; i < 3; ++i) s.tune_ms[i] = h->tune_ms[i];
     s.llk = r.llk;
     s.device_ms = ms;
     s.kernel_ms = kms;

@@ -211,7 +211,8 @@ class LlhData:
                  dist_scale: float = 1.0, device: int = 0, on_failure: str = "neginf",
                  print_iter: bool = False, use_graph: bool = True, schedule: str = "auto",
                  mixed_tol: float = 1e-8, shard_count: int = 1, shard_index: int = 0,
-                 large_blocks: str = "auto", nugget: bool = False, earth: bool = False):
+                 large_blocks: str = "auto", nugget: bool = False, earth: bool = False,
+                 tune: bool = False):
         L = layout.normalized()
         self.layout = L
         o = _lib.BvOpts()
@@ -230,6 +231,7 @@ class LlhData:
         o.large_blocks = _LARGE[large_blocks]
         o.nugget = int(bool(nugget))
         o.earth = int(bool(earth))
+        o.tune = int(bool(tune))
         null_i = C.POINTER(C.c_int)()
         null_d = C.POINTER(C.c_double)()
         self._l = _lib.BvLayout(L.n, L.bc, L.cs, ip(L.batchNum), ip(L.batchNumAccum), dp(L.x),
@@ -301,7 +303,9 @@ class LlhData:
     def status(self) -> dict:
         s = _lib.BvStatus()
         check(lib().bv_get_status(self._h, C.byref(s)))
-        return {f: getattr(s, f) for f, _ in s._fields_}
+        out = {f: getattr(s, f) for f, _ in s._fields_}
+        out["tune_ms"] = list(out["tune_ms"])
+        return out
 
     @property
     def iterations(self) -> int:

@@ -328,3 +328,23 @@ def test_nugget_served_and_mixed(bvlib):
     with bvlib.LlhData(L, nugget=True, precision="mixed") as M:
         vm = M(th)
     assert abs(vm - v) <= 1e-8 * abs(v)
+
+
+def test_tuner_picks_fastest_and_keeps_bits(bvlib, oracle):
+    """bv_opts.tune: the first evaluation times the streamed kernel at 96,
+    128 and 192 threads per CTA and keeps the fastest; every size gives the
+    same bits, so tuned and untuned handles agree exactly."""
+    L = _gen(bvlib, 8000, 500, 100)
+    th = (1.0, 0.1, 1.5)
+    with bvlib.LlhData(L) as D:
+        v0 = D(th)
+        t0 = D.status()["streamed_threads"]
+    with bvlib.LlhData(L, tune=True) as D:
+        v1 = D(th)
+        st = D.status()
+        v2 = D(th)
+    assert v0 == v1 == v2
+    assert t0 in (96, 128, 192)
+    ms = st["tune_ms"]
+    assert all(m > 0 for m in ms), ms
+    assert st["streamed_threads"] == (96, 128, 192)[int(np.argmin(ms))]
