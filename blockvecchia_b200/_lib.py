@@ -111,7 +111,8 @@ class BvStatus(C.Structure):
                 ("fp32_fallback", C.c_int), ("nonfinite", C.c_int), ("flags_or", C.c_uint),
                 ("llk", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double),
                 ("failed", C.c_int), ("launches", C.c_int), ("streamed_blocks", C.c_int),
-                ("streamed_threads", C.c_int), ("tune_ms", C.c_double * 3)]
+                ("streamed_threads", C.c_int), ("streamed_variant", C.c_int),
+                ("tune_ms", C.c_double * 6)]
 
 
 class BvJobOpts(C.Structure):

@@ -62,7 +62,7 @@ static void (*const llh_fp64_big_kernel3)(LlhArgs) = llh_fp64_kernel_t<true, tru
 // The streamed (left-looking, panels through L2) path run by small CTAs,
 // several per SM, so that the pivot chains of several blocks overlap on one
 // SM: NT threads per CTA, RC rows per streamed chunk, MINB CTAs per SM.
-template <int NT, int RC, int MINB, int NS, bool kXYZ3>
+template <int NT, int RC, int MINB, int NS, bool kXYZ3, bool kBulk>
 __global__ void __launch_bounds__(NT, MINB) llh_lean_kernel_t(LlhArgs a)
 {
     extern __shared__ __align__(128) double smem[];
@@ -86,9 +86,8 @@ __global__ void __launch_bounds__(NT, MINB) llh_lean_kernel_t(LlhArgs a)
                 a.block_status[b] = a.status_or;
             }
         } else {
-            process_block_big<NT, RC, LeanShared, NS, kXYZ3>(a, mp, b,
-                                                             reinterpret_cast<unsigned char *>(smem),
-                                                             slab, sh);
+            process_block_big<NT, RC, LeanShared, NS, kXYZ3, kBulk>(
+                a, mp, b, reinterpret_cast<unsigned char *>(smem), slab, sh);
         }
         __syncthreads();
     }
@@ -98,31 +97,36 @@ struct LeanVariant {
     void (*kernel)(LlhArgs);   // 2-D locations
     void (*kernel3)(LlhArgs);  // with a third coordinate
     int threads, rc, ns;
+    bool bulk;  // the whole matrix generated into the slab before the factorization
 };
-#define BV_LEAN(NT, RC, MINB, NS) \
-    {llh_lean_kernel_t<NT, RC, MINB, NS, false>, llh_lean_kernel_t<NT, RC, MINB, NS, true>, NT, RC, NS}
+#define BV_LEAN(NT, RC, MINB, NS, BULK)                                                              \
+    {llh_lean_kernel_t<NT, RC, MINB, NS, false, BULK>, llh_lean_kernel_t<NT, RC, MINB, NS, true, BULK>, \
+     NT, RC, NS, BULK}
 // The left-looking update reads the earlier panels straight from the slab
 // (no staging), so the CTAs can be small and several blocks share an SM.
-// Kernel ms, n = 200k uniform, bc = 20k, nu = 1.5 (first column: the
-// persistent kernel; then 96-thread CTAs x5 per SM, 128 x3, 192 x2):
-//   cs =  40 (M <=  74):  2.54 / 0.88 / 1.01 / 1.36
-//   cs =  80 (M <= 114):  4.48 / 2.37 / 2.27 / 2.66
-//   cs = 120 (M <= 154):  6.88 / 5.46 / 4.61 / 5.06
-//   cs = 160 (M <= 194):  9.99 / 11.6 / 8.21 / 8.39
-//   cs = 200 (M <= 234): 13.62 / 21.2 / 13.38 / 13.18
-//   cs = 240 (M <= 274): 26.26 / 38.2 / 23.68 / 19.40
-//   cs = 300 (M <= 334): 41.08 / 65.7 / 39.14 / 32.27
-// and at the headline shape (n = 1M, cs = 200, nu = 2.5): 68.0 / - / 65.6
-// / 65.7.  Staged variants (chunks copied to shared memory by bulk copies,
-// 2-4 in flight, 256- and 128-thread CTAs) measured 70-122 ms there.  All
-// give the same bits (the per-element operations do not depend on the CTA
-// size).
+// Kernel ms, n = 200k uniform, bc = 20k, nu = 1.5 (the persistent kernel;
+// then 96-thread CTAs x5 per SM, 128 x3, 192 x2 generating panel by panel,
+// and 128 x3, 192 x2 generating the whole matrix first):
+//   cs =  40 (M <=  74):  2.54 /  0.80 /  0.98 /  1.33 /  1.17 /  1.55
+//   cs =  80 (M <= 114):  4.48 /  2.03 /  2.21 /  2.54 /  2.52 /  3.07
+//   cs = 120 (M <= 154):  6.88 /  4.17 /  4.34 /  4.66 /  4.42 /  5.14
+//   cs = 160 (M <= 194): 10.00 /  8.88 /  7.30 /  7.59 /  7.11 /  7.82
+//   cs = 200 (M <= 234): 13.64 / 14.79 / 12.07 / 11.83 / 12.42 / 11.65
+//   cs = 240 (M <= 274): 26.16 / 28.68 / 21.42 / 17.15 / 20.00 / 16.85
+//   cs = 300 (M <= 334): 40.97 / 47.90 / 35.57 / 28.33 / 35.37 / 28.83
+// and at the headline shape (n = 1M, cs = 200, nu = 2.5): 68.0 / 73.3 /
+// 59.8 / 58.9 / 61.9 / 58.1.  All give the same bits (the per-element
+// operations do not depend on the CTA size or the generation mode), so
+// bv_opts.tune may pick any of them.
 static const LeanVariant kLeanVariants[] = {
-    BV_LEAN(96, 64, 5, 0),
-    BV_LEAN(128, 64, 3, 0),
-    BV_LEAN(192, 64, 2, 0),
+    BV_LEAN(96, 64, 5, 0, false),
+    BV_LEAN(128, 64, 3, 0, false),
+    BV_LEAN(192, 64, 2, 0, false),
+    BV_LEAN(128, 64, 3, 0, true),
+    BV_LEAN(192, 64, 2, 0, true),
 };
-static int lean_variant(int max_m) { return max_m <= 96 ? 0 : (max_m <= 234 ? 1 : 2); }
+constexpr int kNumLean = (int)(sizeof(kLeanVariants) / sizeof(kLeanVariants[0]));
+static int lean_variant(int max_m) { return max_m <= 160 ? 0 : (max_m <= 200 ? 3 : 4); }
 
 static thread_local char g_err[1024] = "";
 
@@ -170,9 +174,9 @@ struct bv_handle {
     int streamed_blocks = 0;        // of the owned blocks, how many that is
     // The streamed launch's order positions and largest M, its CTA size
     // (kLeanVariants index; -1: from the table), and the tuner's record.
-    int lean_begin = 0, lean_end = 0, lean_m = 0, lean_choice = -1, lean_threads = 0;
+    int lean_begin = 0, lean_end = 0, lean_m = 0, lean_choice = -1, lean_threads = 0, lean_vi = -1;
     bool tuned = false;
-    double tune_ms[3] = {0.0, 0.0, 0.0};
+    double tune_ms[kNumLean] = {};
     MaternParams *d_mp = nullptr;
     EvalResult *d_res = nullptr;
     MixedWork mixed;  // mixed-precision scratch (bv_llh_mixed.cuh)
@@ -397,7 +401,9 @@ static int order_m(const bv_handle *h, int t)
 // largest block has M = max_m.
 static int plan_lean_launch(bv_handle *h, const cudaDeviceProp &prop, int begin, int end, int max_m)
 {
-    const LeanVariant &v = kLeanVariants[h->lean_choice >= 0 ? h->lean_choice : lean_variant(max_m)];
+    const int vi = h->lean_choice >= 0 ? h->lean_choice : lean_variant(max_m);
+    const LeanVariant &v = kLeanVariants[vi];
+    h->lean_vi = vi;
     h->lean_begin = begin;
     h->lean_end = end;
     h->lean_m = max_m;
@@ -892,7 +898,7 @@ static int tune_lean(bv_handle *h)
     h->tuned = true;
     int best = h->lean_choice >= 0 ? h->lean_choice : lean_variant(h->lean_m);
     double best_ms = 1e300;
-    for (int vi = 0; vi < (int)(sizeof(kLeanVariants) / sizeof(kLeanVariants[0])); ++vi) {
+    for (int vi = 0; vi < kNumLean; ++vi) {
         int rc = replan_lean(h, vi);
         if (rc) return rc;
         double t = 1e300;
@@ -950,7 +956,8 @@ static int eval_locked(bv_handle *h, const double *theta, double *llk)
     s.launches = h->opts.precision == BV_PREC_MIXED ? 5 : (int)h->launches.size() + 1;
     s.streamed_blocks = h->opts.precision == BV_PREC_MIXED ? 0 : h->streamed_blocks;
     s.streamed_threads = s.streamed_blocks > 0 ? h->lean_threads : 0;
-    for (int i = 0; i < 3; ++i) s.tune_ms[i] = h->tune_ms[i];
+    s.streamed_variant = s.streamed_blocks > 0 ? h->lean_vi : -1;
+    for (int i = 0; i < kNumLean; ++i) s.tune_ms[i] = h->tune_ms[i];
     s.llk = r.llk;
     s.device_ms = ms;
     s.kernel_ms = kms;

@@ -204,106 +204,133 @@ __device__ __forceinline__ void panel_update_tiles(double *dst, int dst_r0, cons
 
 // The left-looking update of panel p+1 without staging: nxt rows [n0, Mp)
 // (local row = i - n0) take panels q = 0..p-1 read straight from this CTA's
-// slab (L2), each panel's rank-16 product formed from zero and subtracted on
-// its own, in q order -- per element the same operations in the same order
-// as the staged update, so the same bits.  Warps [w0, w0 + nw) own 8-row
-// tiles (tile t on warp t mod nw) and keep up to kDT of them in registers
-// across all q, so the warps never wait for one another; the next panel's
-// fragments are loaded while the current one is applied.
-constexpr int kDT = 4;
+// slab (L2).  Warps [w0, w0 + nw) own 8-row tiles (tile t on warp t mod nw)
+// and keep kDT of them in registers across all q, so the warps never wait
+// for one another; the next panel's fragments are loaded while the current
+// one is applied.  The tiles are the DMMA accumulators themselves: with B
+// negated, D = (-B)^T A + D subtracts each panel's products in place, 2 kDT
+// independent accumulation chains per warp.  Per element the operations and
+// their order do not depend on the CTA size or the tile count.  A lane's
+// DMMA steps 2h and 2h+1 use the adjacent columns k = 8h + 2 c4 + {0, 1},
+// one 16-byte load for both (the same columns in A and B, so each step
+// still sums four k-products).  kDT = 2 measured fastest (C3 shape: 59.1 ms
+// at 2, 63.4 at 3, 69.9 at 4; with 3 or more the live fragments crowd the
+// registers).
+constexpr int kDT = 2;
 
-__device__ __forceinline__ void load_frags(const double *slab, int Mp, int q, int n0, int i0, int ntile,
-                                           int nw, int r8, int c4, double (&bf)[4][2],
-                                           double (&af)[kDT][4])
+__device__ __forceinline__ double2 ldcg2(const double *p)
 {
-    const double *pq = slab + big_panel_base(q, Mp);
-    const int q0 = q * kNB;
+    return __ldcg(reinterpret_cast<const double2 *>(p));
+}
+
+template <int NTILE>
+__device__ __forceinline__ void load_frags(const double *pq, int q0, int Mp, int n0, int i0, int nw,
+                                           int r8, int c4, double2 (&bf)[2][2], double2 (&af)[NTILE][2])
+{
 #pragma unroll
-    for (int kk = 0; kk < 4; ++kk)
+    for (int h = 0; h < 2; ++h) {
 #pragma unroll
         for (int nj = 0; nj < 2; ++nj) {
-            const int r = n0 + 8 * nj + r8, k = 4 * kk + c4;
-            bf[kk][nj] = (r < Mp) ? __ldcg(pq + (size_t)(r - q0) * 16 + swz(r, k)) : 0.0;
+            const int r = n0 + 8 * nj + r8;
+            bf[h][nj] = (r < Mp) ? ldcg2(pq + (size_t)(r - q0) * 16 + swz(r, 8 * h + 2 * c4))
+                                 : make_double2(0.0, 0.0);
         }
 #pragma unroll
-    for (int m = 0; m < kDT; ++m) {
-        const int ia = i0 + 8 * nw * m + r8;
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk)
-            af[m][kk] = (m < ntile && ia < Mp) ? __ldcg(pq + (size_t)(ia - q0) * 16 + swz(ia, 4 * kk + c4))
-                                               : 0.0;
+        for (int m = 0; m < NTILE; ++m) {
+            const int ia = i0 + 8 * nw * m + r8;
+            af[m][h] = (ia < Mp) ? ldcg2(pq + (size_t)(ia - q0) * 16 + swz(ia, 8 * h + 2 * c4))
+                                 : make_double2(0.0, 0.0);
+        }
     }
 }
 
+template <int NTILE, bool kRaw>
+__device__ __forceinline__ void direct_tiles(double *nxt, int n0, const double *slab, int Mp, int p,
+                                             int i0, int nw, int r8, int c4)
+{
+    // Panel p+1 before the update: generated into nxt, or (kRaw) still in
+    // the slab where the whole matrix was generated.
+    const double *src = kRaw ? slab + big_panel_base(p + 1, Mp) : nxt;
+    double d[NTILE][2][2];
+#pragma unroll
+    for (int m = 0; m < NTILE; ++m) {
+        const int ia = i0 + 8 * nw * m + r8;
+#pragma unroll
+        for (int nj = 0; nj < 2; ++nj)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int o = (ia - n0) * 16 + swz(ia, 8 * nj + 2 * c4 + e);
+                d[m][nj][e] = (ia < Mp) ? (kRaw ? __ldcg(src + o) : src[o]) : 0.0;
+            }
+    }
+    double2 bf[2][2], af[NTILE][2], bn[2][2], an[NTILE][2];
+    if (p > 0) load_frags<NTILE>(slab + big_panel_base(0, Mp), 0, Mp, n0, i0, nw, r8, c4, bf, af);
+    for (int q = 0; q < p; ++q) {
+        if (q + 1 < p)
+            load_frags<NTILE>(slab + big_panel_base(q + 1, Mp), (q + 1) * kNB, Mp, n0, i0, nw, r8, c4,
+                              bn, an);
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const int h = kk >> 1;
+            double b[2];
+#pragma unroll
+            for (int nj = 0; nj < 2; ++nj) b[nj] = -((kk & 1) ? bf[h][nj].y : bf[h][nj].x);
+#pragma unroll
+            for (int m = 0; m < NTILE; ++m) {
+                const double a = (kk & 1) ? af[m][h].y : af[m][h].x;
+#pragma unroll
+                for (int nj = 0; nj < 2; ++nj) dmma_8x8x4(d[m][nj][0], d[m][nj][1], a, b[nj]);
+            }
+        }
+        if (q + 1 < p) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+#pragma unroll
+                for (int nj = 0; nj < 2; ++nj) bf[h][nj] = bn[h][nj];
+#pragma unroll
+                for (int m = 0; m < NTILE; ++m) af[m][h] = an[m][h];
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < NTILE; ++m) {
+        const int ia = i0 + 8 * nw * m + r8;
+        if (ia < Mp) {
+#pragma unroll
+            for (int nj = 0; nj < 2; ++nj)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) nxt[(ia - n0) * 16 + swz(ia, 8 * nj + 2 * c4 + e)] = d[m][nj][e];
+        }
+    }
+}
+
+// kRaw: panel p+1 is taken from the slab (the whole matrix generated there
+// first) and written to nxt updated, also when there is nothing to apply.
+template <bool kRaw>
 __device__ __forceinline__ void panel_update_direct(double *nxt, int n0, const double *slab, int Mp, int p,
                                                     int w0, int nw)
 {
     const int warp = (threadIdx.x >> 5) - w0, lane = threadIdx.x & 31;
-    if (warp < 0 || warp >= nw || p == 0) return;
+    if (warp < 0 || warp >= nw || (!kRaw && p == 0)) return;
     const int r8 = lane >> 2, c4 = lane & 3;
     const int ntiles = (Mp - n0 + 7) >> 3;
-    for (int t0 = warp; t0 < ntiles; t0 += nw * kDT) {
-        const int ntile = min(kDT, (ntiles - t0 + nw - 1) / nw);  // tiles t0, t0 + nw, ...
-        const int i0 = n0 + 8 * t0;
-        double d[kDT][2][2];
-#pragma unroll
-        for (int m = 0; m < kDT; ++m) {
-            const int ia = i0 + 8 * nw * m + r8;
-#pragma unroll
-            for (int nj = 0; nj < 2; ++nj)
-#pragma unroll
-                for (int e = 0; e < 2; ++e)
-                    d[m][nj][e] = (m < ntile && ia < Mp) ? nxt[(ia - n0) * 16 + swz(ia, 8 * nj + 2 * c4 + e)] : 0.0;
-        }
-        double bf[4][2], af[kDT][4], bn[4][2], an[kDT][4];
-        load_frags(slab, Mp, 0, n0, i0, ntile, nw, r8, c4, bf, af);
-        for (int q = 0; q < p; ++q) {
-            if (q + 1 < p) load_frags(slab, Mp, q + 1, n0, i0, ntile, nw, r8, c4, bn, an);
-#pragma unroll
-            for (int m = 0; m < kDT; ++m) {
-                if (m < ntile) {
-                    double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-#pragma unroll
-                    for (int kk = 0; kk < 4; ++kk)
-#pragma unroll
-                        for (int nj = 0; nj < 2; ++nj) dmma_8x8x4(acc[nj][0], acc[nj][1], af[m][kk], bf[kk][nj]);
-#pragma unroll
-                    for (int nj = 0; nj < 2; ++nj)
-#pragma unroll
-                        for (int e = 0; e < 2; ++e) d[m][nj][e] -= acc[nj][e];
-                }
-            }
-            if (q + 1 < p) {
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-#pragma unroll
-                    for (int nj = 0; nj < 2; ++nj) bf[kk][nj] = bn[kk][nj];
-#pragma unroll
-                    for (int m = 0; m < kDT; ++m) af[m][kk] = an[m][kk];
-                }
-            }
-        }
-#pragma unroll
-        for (int m = 0; m < kDT; ++m) {
-            const int ia = i0 + 8 * nw * m + r8;
-            if (m < ntile && ia < Mp) {
-#pragma unroll
-                for (int nj = 0; nj < 2; ++nj)
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) nxt[(ia - n0) * 16 + swz(ia, 8 * nj + 2 * c4 + e)] = d[m][nj][e];
-            }
-        }
-    }
+    // Groups of kDT tiles per warp, computed whole: the tiles of a group
+    // beyond the panel's rows hold zeros and are not stored (one code path
+    // keeps the accumulation chains of all kDT tiles interleaved).
+    for (int t0 = warp; t0 < ntiles; t0 += nw * kDT)
+        direct_tiles<kDT, kRaw>(nxt, n0, slab, Mp, p, n0 + 8 * t0, nw, r8, c4);
 }
 
 // One block by the streamed path, run by a CTA of NT threads (warp 0
 // factors, the other NT/32 - 1 warps generate and update), with RC rows per
 // streamed chunk and NS chunks in flight (NS = 0: no staging, the warps read
-// the slab directly, panel_update_direct).  smem: the dynamic area
+// the slab directly, panel_update_direct; with kBulk the whole matrix is
+// generated into the slab first).  smem: the dynamic area
 // (big_layout(M, RC, nz, NS).total bytes); slab: this CTA's global slab
 // (big_slab_doubles(M) doubles).  Every element's operations and their
-// order are the same for every NT, RC and NS.
-template <int NT, int RC, typename SH, int NS = kBigStages, bool kXYZ3 = false>
+// order are the same for every NT, RC, NS > 0 and kBulk; the direct update
+// (NS = 0) accumulates in place and rounds differently from the staged one.
+template <int NT, int RC, typename SH, int NS = kBigStages, bool kXYZ3 = false, bool kBulk = false>
 static __device__ __noinline__ void process_block_big(const LlhArgs &a, const MaternParams &mp, int b,
                                                       unsigned char *smem, double *slab, SH &sh)
 {
@@ -339,11 +366,29 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         fence_mbar_init();
     }
     __syncthreads();
-    // Panel 0 into Pcur.
-    for (int e = tid; e < Mp * 16; e += kT) {
-        const int r = e >> 4, c = e & 15;
-        const double v = (c < M && r >= c) ? big_entry<kXYZ3>(X, Y, Z, T, M, r, c, mp) : 0.0;
-        cur[r * 16 + swz(r, c)] = v;
+    if constexpr (NS == 0 && kBulk) {
+        // Every panel's entries straight into the slab, by all warps (the
+        // update warps then take panel p+1 from there): the generation runs
+        // at the CTA's full width instead of beside warp 0's pivot chain.
+        for (int q = 0; q < P; ++q) {
+            const int q0 = q * kNB, kbq = min(kNB, M - q0);
+            double *pg = slab + big_panel_base(q, Mp);
+            for (int e = tid; e < (Mp - q0) * 16; e += kT) {
+                const int r = q0 + (e >> 4), c = e & 15, j = q0 + c;
+                pg[(r - q0) * 16 + swz(r, c)] =
+                    (c < kbq && r >= j) ? big_entry<kXYZ3>(X, Y, Z, T, M, r, j, mp) : 0.0;
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < Mp * 8; e += kT)
+            reinterpret_cast<double2 *>(cur)[e] = __ldcg(reinterpret_cast<const double2 *>(slab) + e);
+    } else {
+        // Panel 0 into cur.
+        for (int e = tid; e < Mp * 16; e += kT) {
+            const int r = e >> 4, c = e & 15;
+            const double v = (c < M && r >= c) ? big_entry<kXYZ3>(X, Y, Z, T, M, r, c, mp) : 0.0;
+            cur[r * 16 + swz(r, c)] = v;
+        }
     }
     __syncthreads();
 
@@ -377,17 +422,20 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
             }
             if (lane == 0) st |= fst;
         } else if (kb1 > 0) {
-            // Panel p+1: generate, then apply panels 0..p-1 from the slab.
             const int nrows = Mp - n0;
-            for (int e = tid - 32; e < nrows * 16; e += kT - 32) {
-                const int r = n0 + (e >> 4), c = e & 15;
-                const int j = n0 + c;
-                const double v = (c < kb1 && r >= j) ? big_entry<kXYZ3>(X, Y, Z, T, M, r, j, mp) : 0.0;
-                nxt[(r - n0) * 16 + swz(r, c)] = v;
+            if constexpr (NS != 0 || !kBulk) {
+                // Panel p+1: generate, then apply panels 0..p-1 from the slab.
+                for (int e = tid - 32; e < nrows * 16; e += kT - 32) {
+                    const int r = n0 + (e >> 4), c = e & 15;
+                    const int j = n0 + c;
+                    const double v =
+                        (c < kb1 && r >= j) ? big_entry<kXYZ3>(X, Y, Z, T, M, r, j, mp) : 0.0;
+                    nxt[(r - n0) * 16 + swz(r, c)] = v;
+                }
+                update_warps_sync<NT>();
             }
-            update_warps_sync<NT>();
             if constexpr (NS == 0) {
-                panel_update_direct(nxt, n0, slab, Mp, p, 1, kW - 1);
+                panel_update_direct<kBulk>(nxt, n0, slab, Mp, p, 1, kW - 1);
             } else {
             const int nchunk = (nrows + RC - 1) / RC;
             const int items = nchunk * p;       // (chunk, q), q fastest

@@ -131,13 +131,12 @@ typedef struct {
                           the conditioning-set key when the handle selects
                           the sets.  2-D Matern kernels (1-3) and FP64 only,
                           as the reference allows it for 2-D locations only. */
-    int tune;          /* 0 (default): the streamed kernel's CTA size from
-                          a measured table (96, 128 or 192 threads by the
-                          launch's largest block).  1: the first evaluation
-                          times every CTA size on this layout and the handle
-                          keeps the fastest (all sizes give the same bits, so
-                          results do not depend on the choice);
-                          bv_get_status reports the times.              */
+    int tune;          /* 0 (default): the streamed kernel's variant from a
+                          measured table by the launch's largest block.  1:
+                          the first evaluation times every variant on this
+                          layout and the handle keeps the fastest (all give
+                          the same bits, so results do not depend on the
+                          choice); bv_get_status reports the times.        */
 } bv_opts;
 
 /* Distance metrics of bv_knn_ex (the reference's distance_metric). */
@@ -162,9 +161,12 @@ typedef struct {
                             kernel (the rest on the persistent kernel);
                             0 for the mixed path                             */
     int streamed_threads; /* threads per CTA of that kernel (0: none)       */
-    double tune_ms[3];   /* with bv_opts.tune: the streamed kernel's time at
-                            96, 128 and 192 threads per CTA on the first
-                            evaluation (0 where not timed)                   */
+    int streamed_variant; /* its variant, an index into tune_ms             */
+    double tune_ms[6];   /* with bv_opts.tune: the streamed kernel's time on
+                            the first evaluation per variant: 96, 128 and 192
+                            threads per CTA generating panel by panel, then
+                            128 and 192 generating the whole matrix first (0
+                            where not timed; entry 5 unused)                 */
 } bv_status;
 
 typedef struct bv_handle bv_handle;

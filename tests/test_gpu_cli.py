@@ -137,7 +137,7 @@ def test_earth_one_evaluation_matches_oracle(exe, bvlib, oracle, tmp_path):
     np.savetxt(tmp_path / "xy.csv", np.stack([lat, lon], 1), delimiter=",", fmt="%.17g")
     np.savetxt(tmp_path / "z.csv", z, fmt="%.17g")
     r = subprocess.run([exe, "--num_loc", str(n), "--vecchia_bc", str(bc), "--vecchia_cs", str(cs),
-                        "--xy_path", "xy.csv", "--obs_path", "z.csv", "--kernel_init", "1.0:0.7:0.5",
+                        "--xy_path", "xy.csv", "--obs_path", "z.csv", "--kernel_init", "1.0:0.2:0.5",
                         "--dist_scale", "1000", "--earth", "--maxiter", "1", "--seed", "0"],
                        capture_output=True, text=True, timeout=600, cwd=tmp_path)
     assert r.returncode == 0, r.stdout + r.stderr
@@ -149,6 +149,6 @@ def test_earth_one_evaluation_matches_oracle(exe, bvlib, oracle, tmp_path):
     knn = oracle.knn_all_earth_fast(L.x, L.y, cs, L.batchNumAccum, L.cx, L.cy)
     P = oracle.OracleProblem(L.batchNum, L.batchNumAccum, L.x, L.y, L.obs, knn, cs,
                              dist_scale=1000.0, earth=True)
-    ref = oracle.llh(P, (1.0, 0.7, 0.5))
+    ref = oracle.llh(P, (1.0, 0.2, 0.5))
     # The CLI prints the log-likelihood with 6 decimals.
     assert abs(llk - ref) <= max(1e-10 * abs(ref), 1e-6), (llk, ref)

@@ -68,7 +68,8 @@ def test_blocks_beyond_shared_memory_fall_back(bvlib, oracle):
     evaluated by the FP64 kernel."""
     L = _gen(bvlib, 3000, 200, 300)
     th = (1.0, 0.1, 0.5)
-    with bvlib.LlhData(L) as D:
+    # The fallback runs the persistent kernel.
+    with bvlib.LlhData(L, schedule="persistent") as D:
         v64 = D(th)
     with bvlib.LlhData(L, precision="mixed") as M:
         vm = M(th)
