@@ -104,29 +104,35 @@ struct LeanVariant {
      NT, RC, NS, BULK}
 // The left-looking update reads the earlier panels straight from the slab
 // (no staging), so the CTAs can be small and several blocks share an SM.
-// Kernel ms, n = 200k uniform, bc = 20k, nu = 1.5 (the persistent kernel;
-// then 96-thread CTAs x5 per SM, 128 x3, 192 x2 generating panel by panel,
-// and 128 x3, 192 x2 generating the whole matrix first):
-//   cs =  40 (M <=  74):  2.54 /  0.80 /  0.98 /  1.33 /  1.17 /  1.55
-//   cs =  80 (M <= 114):  4.48 /  2.03 /  2.21 /  2.54 /  2.52 /  3.07
-//   cs = 120 (M <= 154):  6.88 /  4.17 /  4.34 /  4.66 /  4.42 /  5.14
-//   cs = 160 (M <= 194): 10.00 /  8.88 /  7.30 /  7.59 /  7.11 /  7.82
-//   cs = 200 (M <= 234): 13.64 / 14.79 / 12.07 / 11.83 / 12.42 / 11.65
-//   cs = 240 (M <= 274): 26.16 / 28.68 / 21.42 / 17.15 / 20.00 / 16.85
-//   cs = 300 (M <= 334): 40.97 / 47.90 / 35.57 / 28.33 / 35.37 / 28.83
-// and at the headline shape (n = 1M, cs = 200, nu = 2.5): 68.0 / 73.3 /
-// 59.8 / 58.9 / 61.9 / 58.1.  All give the same bits (the per-element
-// operations do not depend on the CTA size or the generation mode), so
-// bv_opts.tune may pick any of them.
+// Kernel ms, n = 200k uniform, bc = 20k, nu = 1.5: the persistent kernel;
+// then 96-thread CTAs x5 per SM, 160 x3 and 256 x2 generating panel by panel
+// (the first three variants; the whole-matrix generation, the last three,
+// wins only where the generation is expensive: general nu):
+//   cs =  40 (M <=  74):  2.54 /  0.80 /  1.00 /  1.35
+//   cs =  80 (M <= 114):  4.48 /  2.02 /  2.16 /  2.58
+//   cs = 120 (M <= 154):  6.88 /  4.13 /  4.01 /  4.40
+//   cs = 160 (M <= 194): 10.00 /  8.89 /  6.62 /  7.04
+//   cs = 200 (M <= 234): 13.70 / 14.79 / 10.73 / 10.78
+//   cs = 240 (M <= 274): 26.23 / 28.65 / 18.41 / 15.43
+//   cs = 300 (M <= 334): 40.94 / 47.85 / 30.23 / 25.35
+// At the headline shape (n = 1M, cs = 200, nu = 2.5, largest M 240):
+// 68.0 / 73.3 / 53.2 / 53.5; at the general-nu stress shape (2M points,
+// cs = 300, nu = 0.8) 256 x2 generating the whole matrix first, 526 ms,
+// against 537 panel by panel.  Larger CTAs spill (288 or 320 threads x2)
+// or run one block per SM (512 x1); smaller ones (128, 192) lost
+// everywhere.  All give the same bits (the per-element operations do not
+// depend on the CTA size or the generation mode), so bv_opts.tune may pick
+// any of them.
 static const LeanVariant kLeanVariants[] = {
     BV_LEAN(96, 64, 5, 0, false),
-    BV_LEAN(128, 64, 3, 0, false),
-    BV_LEAN(192, 64, 2, 0, false),
-    BV_LEAN(128, 64, 3, 0, true),
-    BV_LEAN(192, 64, 2, 0, true),
+    BV_LEAN(160, 64, 3, 0, false),
+    BV_LEAN(256, 64, 2, 0, false),
+    BV_LEAN(96, 64, 5, 0, true),
+    BV_LEAN(160, 64, 3, 0, true),
+    BV_LEAN(256, 64, 2, 0, true),
 };
 constexpr int kNumLean = (int)(sizeof(kLeanVariants) / sizeof(kLeanVariants[0]));
-static int lean_variant(int max_m) { return max_m <= 160 ? 0 : (max_m <= 200 ? 3 : 4); }
+static int lean_variant(int max_m) { return max_m <= 120 ? 0 : (max_m <= 250 ? 1 : 2); }
 
 static thread_local char g_err[1024] = "";
 
@@ -172,6 +178,7 @@ struct bv_handle {
     double *d_slab_lean = nullptr;  // per-CTA slabs of the multi-CTA streamed launch
     int lean_max_m = 0;             // blocks with M <= this run the multi-CTA streamed kernel
     int streamed_blocks = 0;        // of the owned blocks, how many that is
+    bool mixed_lean = false;        // mixed path: the FP64 pass runs the streamed kernel (last launch)
     // The streamed launch's order positions and largest M, its CTA size
     // (kLeanVariants index; -1: from the table), and the tuner's record.
     int lean_begin = 0, lean_end = 0, lean_m = 0, lean_choice = -1, lean_threads = 0, lean_vi = -1;
@@ -456,9 +463,9 @@ static int plan_launches(bv_handle *h)
     }
     const int sched = h->opts.schedule;
     // The multi-CTA streamed kernel takes every block whose panels fit its
-    // shared memory (by default and under BV_SCHED_STREAMED); the mixed
-    // path's FP64 fallback and BV_SCHED_PERSISTENT / BUCKETED keep the
-    // persistent kernel.
+    // shared memory (by default and under BV_SCHED_STREAMED; for the mixed
+    // path's FP64 pass, when every block fits); BV_SCHED_PERSISTENT /
+    // BUCKETED keep the persistent kernel.
     int lean_limit = 0;
     {
         int optin = 0;
@@ -535,6 +542,16 @@ static int plan_launches(bv_handle *h)
         const int rc = plan_lean_launch(h, prop, split, h->owned, order_m(h, split));
         if (rc) return rc;
     }
+    // Mixed precision: the FP64 pass over the blocks the mixed kernel hands
+    // back runs the streamed kernel too when every block fits it (the list
+    // is only known on the device, so the launch covers all positions).
+    h->mixed_lean = false;
+    if (h->opts.precision == BV_PREC_MIXED && (sched == BV_SCHED_STREAMED || sched == BV_SCHED_AUTO) &&
+        h->owned > 0 && h->max_m <= lean_limit) {
+        const int rc = plan_lean_launch(h, prop, 0, h->owned, h->max_m);
+        if (rc) return rc;
+        h->mixed_lean = true;
+    }
     BV_CUDA_TRY(cudaMalloc(&h->d_counters, sizeof(unsigned) * std::max<size_t>(1, h->launches.size())));
     return BV_OK;
 }
@@ -602,7 +619,17 @@ static int enqueue_eval(bv_handle *h, cudaStream_t s)
         ma.log2pi = std::log(2 * 3.141592653589793);
         int rc = mixed_enqueue(h->mixed, ma, s);
         if (rc) return rc;
-        if (h->owned > 0) {
+        if (h->owned > 0 && h->mixed_lean) {
+            const size_t l = h->launches.size() - 1;
+            const bv_handle::Launch &ln = h->launches[l];
+            LlhArgs a = fp64_args(h->d_counters + l, h->mixed.fallback_list, 0, h->owned);
+            a.task_count = h->mixed.fallback_count;
+            a.status_or = BV_ST_FP32_FALLBACK;
+            a.gslab = ln.slab;
+            a.gslab_stride = ln.slab_stride;
+            ln.kernel<<<ln.grid, ln.threads, ln.smem, s>>>(a);
+            BV_CUDA_TRY(cudaGetLastError());
+        } else if (h->owned > 0) {
             LlhArgs a = fp64_args(h->d_counters, h->mixed.fallback_list, 0, h->owned);
             a.task_count = h->mixed.fallback_count;
             a.status_or = BV_ST_FP32_FALLBACK;

@@ -163,10 +163,10 @@ typedef struct {
     int streamed_threads; /* threads per CTA of that kernel (0: none)       */
     int streamed_variant; /* its variant, an index into tune_ms             */
     double tune_ms[6];   /* with bv_opts.tune: the streamed kernel's time on
-                            the first evaluation per variant: 96, 128 and 192
+                            the first evaluation per variant: 96, 160 and 256
                             threads per CTA generating panel by panel, then
-                            128 and 192 generating the whole matrix first (0
-                            where not timed; entry 5 unused)                 */
+                            the same sizes generating the whole matrix first
+                            (0 where not timed)                              */
 } bv_status;
 
 typedef struct bv_handle bv_handle;

@@ -47,8 +47,8 @@ def test_ill_conditioned_falls_back_to_fp64(bvlib):
     beyond 1/eps32); the fallback reproduces the FP64 path exactly."""
     L = _gen(bvlib, 6000, 600, 80)
     th = (1.0, 0.05, 2.5)
-    # The fallback pass runs the persistent kernel.
-    with bvlib.LlhData(L, schedule="persistent") as D:
+    # The fallback pass runs the FP64 handle's streamed kernel.
+    with bvlib.LlhData(L) as D:
         v64 = D(th)
         b64 = D.block_llk()
     with bvlib.LlhData(L, precision="mixed", on_failure="continue") as M:
@@ -68,14 +68,16 @@ def test_blocks_beyond_shared_memory_fall_back(bvlib, oracle):
     evaluated by the FP64 kernel."""
     L = _gen(bvlib, 3000, 200, 300)
     th = (1.0, 0.1, 0.5)
-    # The fallback runs the persistent kernel.
-    with bvlib.LlhData(L, schedule="persistent") as D:
-        v64 = D(th)
-    with bvlib.LlhData(L, precision="mixed") as M:
-        vm = M(th)
-        st = M.status()
-    assert st["fp32_fallback"] == L.bc
-    assert vm == v64
+    # The fallback runs the FP64 handle's streamed kernel, or with the
+    # persistent schedule the persistent one.
+    for sched in ("auto", "persistent"):
+        with bvlib.LlhData(L, schedule=sched) as D:
+            v64 = D(th)
+        with bvlib.LlhData(L, precision="mixed", schedule=sched) as M:
+            vm = M(th)
+            st = M.status()
+        assert st["fp32_fallback"] == L.bc
+        assert vm == v64, sched
 
 
 def test_mixed_deterministic_graph_and_stream(bvlib):
