@@ -155,6 +155,37 @@ __device__ __forceinline__ double big_entry(const double *X, const double *Y, co
     return (i == j && mp.nugget != 0.0) ? c + mp.nugget : c;
 }
 
+// Column c of a 16-column panel starting at row and column q0, rows
+// [r_begin, Mp) step `rstep`, into dst (local row r - dst_r0, swizzled): the
+// column point is read once and kept in registers; entries above the
+// diagonal and columns beyond the matrix (c >= kbq) are zeros.  The same
+// entries as big_entry.
+template <bool kXYZ3>
+__device__ __forceinline__ void gen_column(double *dst, int dst_r0, const double *X, const double *Y,
+                                           const double *Z, const double *T, int M, int Mp, int q0, int kbq,
+                                           int c, int r_begin, int rstep, const MaternParams &mp)
+{
+    const int j = q0 + c;
+    if (c >= kbq) {
+        for (int r = r_begin; r < Mp; r += rstep) dst[(r - dst_r0) * 16 + swz(r, c)] = 0.0;
+        return;
+    }
+    const double xj = X[j], yj = Y[j], tj = kXYZ3 ? T[j] : 0.0, zj = Z[j];
+    for (int r = r_begin; r < Mp; r += rstep) {
+        double v = 0.0;
+        if (r >= M) {
+            v = zj;
+        } else if (r >= j) {
+            if constexpr (kXYZ3)
+                v = cov_xyz(X[r], Y[r], T[r], xj, yj, tj, mp);
+            else
+                v = matern(X[r], Y[r], xj, yj, mp);
+            if (r == j && mp.nugget != 0.0) v += mp.nugget;
+        }
+        dst[(r - dst_r0) * 16 + swz(r, c)] = v;
+    }
+}
+
 // Rank-16 update of a panel held in shared memory, dst rows [d0, d1) (panel
 // local rows relative to dst_r0) and 16 columns:
 //     dst(i, n) -= sum_k A(i, k) * B(n, k)
@@ -334,6 +365,7 @@ template <int NT, int RC, typename SH, int NS = kBigStages, bool kXYZ3 = false, 
 static __device__ __noinline__ void process_block_big(const LlhArgs &a, const MaternParams &mp, int b,
                                                       unsigned char *smem, double *slab, SH &sh)
 {
+    static_assert(NT % 32 == 0 && NT > 32, "whole warps, at least one besides the factor warp");
     constexpr int kT = NT, kW = NT / 32;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int off = a.acc[b];
@@ -370,25 +402,15 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         // Every panel's entries straight into the slab, by all warps (the
         // update warps then take panel p+1 from there): the generation runs
         // at the CTA's full width instead of beside warp 0's pivot chain.
-        for (int q = 0; q < P; ++q) {
-            const int q0 = q * kNB, kbq = min(kNB, M - q0);
-            double *pg = slab + big_panel_base(q, Mp);
-            for (int e = tid; e < (Mp - q0) * 16; e += kT) {
-                const int r = q0 + (e >> 4), c = e & 15, j = q0 + c;
-                pg[(r - q0) * 16 + swz(r, c)] =
-                    (c < kbq && r >= j) ? big_entry<kXYZ3>(X, Y, Z, T, M, r, j, mp) : 0.0;
-            }
-        }
+        for (int q = 0; q < P; ++q)
+            gen_column<kXYZ3>(slab + big_panel_base(q, Mp), q * kNB, X, Y, Z, T, M, Mp, q * kNB,
+                              min(kNB, M - q * kNB), tid & 15, q * kNB + (tid >> 4), kT >> 4, mp);
         __syncthreads();
         for (int e = tid; e < Mp * 8; e += kT)
             reinterpret_cast<double2 *>(cur)[e] = __ldcg(reinterpret_cast<const double2 *>(slab) + e);
     } else {
-        // Panel 0 into cur.
-        for (int e = tid; e < Mp * 16; e += kT) {
-            const int r = e >> 4, c = e & 15;
-            const double v = (c < M && r >= c) ? big_entry<kXYZ3>(X, Y, Z, T, M, r, c, mp) : 0.0;
-            cur[r * 16 + swz(r, c)] = v;
-        }
+        // Panel 0 into cur: thread t takes column t mod 16, every (kT/16)-th row.
+        gen_column<kXYZ3>(cur, 0, X, Y, Z, T, M, Mp, 0, min(kNB, M), tid & 15, tid >> 4, kT >> 4, mp);
     }
     __syncthreads();
 
@@ -424,14 +446,11 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         } else if (kb1 > 0) {
             const int nrows = Mp - n0;
             if constexpr (NS != 0 || !kBulk) {
-                // Panel p+1: generate, then apply panels 0..p-1 from the slab.
-                for (int e = tid - 32; e < nrows * 16; e += kT - 32) {
-                    const int r = n0 + (e >> 4), c = e & 15;
-                    const int j = n0 + c;
-                    const double v =
-                        (c < kb1 && r >= j) ? big_entry<kXYZ3>(X, Y, Z, T, M, r, j, mp) : 0.0;
-                    nxt[(r - n0) * 16 + swz(r, c)] = v;
-                }
+                // Panel p+1: generate (update thread u takes column u mod 16,
+                // every ((kT - 32)/16)-th row), then apply panels 0..p-1.
+                const int u = tid - 32;
+                gen_column<kXYZ3>(nxt, n0, X, Y, Z, T, M, Mp, n0, kb1, u & 15, n0 + (u >> 4), (kT - 32) >> 4,
+                                  mp);
                 update_warps_sync<NT>();
             }
             if constexpr (NS == 0) {

@@ -241,7 +241,7 @@ int bv_llh_host(bv_handle *h, const double *x, const double *y,
  * other blocks condition on it, give BV_E_INVALID.  The first call on a
  * device looks up that array's device address (cached per device ordinal;
  * a cudaDeviceReset invalidates it, so do not call this entry point after
- * one), so make that first call before any stream capture.  Every call
+ * one).  Every call
  * shares the array: calls that overlap on the GPU race, so serialise them
  * (one stream, or synchronise).  Runs on `stream` (a cudaStream_t of the
  * current device; NULL = the default stream) and waits for its own work
