@@ -424,18 +424,21 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         const int kb1 = max(0, min(kNB, M - n0));     // its width
         if (warp == 0) {
             // Lagged Crout factorization of the diagonal block (lane r < kb
-            // owns row k0+r; factor_rows, the upper lanes idle).
-            const bool valid = lane < kb;
+            // owns row k0+r; factor_rows).  With a full panel the upper lanes
+            // solve the next 16 rows (k0+16..k0+31, below the diagonal block)
+            // on the same chain, so the substitution phase starts 16 rows on.
+            const bool low = lane < kNB;
             const int row = k0 + lane;
+            const bool valid = low ? lane < kb : (kb == kNB && row < Mp);
             double v[kNB], myinv;
 #pragma unroll
             for (int c = 0; c < kNB; ++c)
-                v[c] = (valid && c < kb && c <= lane) ? cur[lane * 16 + swz(row, c)] : 0.0;
+                v[c] = (valid && c < kb && (!low || c <= lane)) ? cur[lane * 16 + swz(row, c)] : 0.0;
             const unsigned fst = factor_rows(k0, kb, mc, v, myinv);
             if (valid) {
 #pragma unroll
                 for (int c = 0; c < kNB; ++c)
-                    if (c < kb && c <= lane) cur[lane * 16 + swz(row, c)] = v[c];
+                    if (c < kb && (!low || c <= lane)) cur[lane * 16 + swz(row, c)] = v[c];
             }
             if (lane < kNB) {
 #pragma unroll
@@ -512,10 +515,11 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
             }
         }
         __syncthreads();
-        // Rows below the diagonal block: forward substitution against L_kk,
-        // the two operands on step q+1's dependent chain (1 / L_{q+1,q+1} and
+        // Rows below the diagonal block (after the 16 the factor warp solved
+        // for a full panel): forward substitution against L_kk, the two
+        // operands on step q+1's dependent chain (1 / L_{q+1,q+1} and
         // L_{q+2,q+1}) read one step ahead.
-        for (int r = k0 + kb + tid; r < Mp; r += kT) {
+        for (int r = k0 + (kb == kNB ? 2 * kNB : kb) + tid; r < Mp; r += kT) {
             double *row = cur + (r - k0) * 16;
             double w[kNB];
 #pragma unroll
