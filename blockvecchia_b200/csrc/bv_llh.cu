@@ -118,21 +118,27 @@ struct LeanVariant {
 // At the headline shape (n = 1M, cs = 200, nu = 2.5, largest M 240):
 // 68.0 / 73.3 / 53.2 / 53.5; at the general-nu stress shape (2M points,
 // cs = 300, nu = 0.8) 256 x2 generating the whole matrix first, 526 ms,
-// against 537 panel by panel.  Larger CTAs spill (288 or 320 threads x2)
-// or run one block per SM (512 x1); smaller ones (128, 192) lost
-// everywhere.  All give the same bits (the per-element operations do not
+// against 537 panel by panel.  128 x4 (four CTAs while two panels of
+// M <= ~200 fit) is the fastest up to M ~ 170 (cs = 40 / 80 / 120: 0.78 /
+// 1.98 / 3.86).  Larger CTAs spill (288 or 320 threads x2, 192 x3, 160 x4)
+// or run one block per SM (512 x1); 128 x3 and 192 x2 lost everywhere.
+// All give the same bits (the per-element operations do not
 // depend on the CTA size or the generation mode), so bv_opts.tune may pick
 // any of them.
 static const LeanVariant kLeanVariants[] = {
     BV_LEAN(96, 64, 5, 0, false),
     BV_LEAN(160, 64, 3, 0, false),
     BV_LEAN(256, 64, 2, 0, false),
-    BV_LEAN(96, 64, 5, 0, true),
+    BV_LEAN(128, 64, 4, 0, false),
     BV_LEAN(160, 64, 3, 0, true),
     BV_LEAN(256, 64, 2, 0, true),
 };
 constexpr int kNumLean = (int)(sizeof(kLeanVariants) / sizeof(kLeanVariants[0]));
-static int lean_variant(int max_m) { return max_m <= 120 ? 0 : (max_m <= 250 ? 1 : 2); }
+static int lean_variant(int max_m)
+{
+    const int t = lean_table_threads(max_m);
+    return t == 128 ? 3 : (t == 160 ? 1 : 2);  // the panel-by-panel variants
+}
 
 static thread_local char g_err[1024] = "";
 

@@ -121,6 +121,11 @@ inline size_t big_slab_stride(int max_m, int small_m, int big_m, int nz = 0)
 
 __device__ __forceinline__ int swz(int r, int c) { return c ^ ((r & 3) << 2); }
 
+// CTA size of the multi-CTA streamed kernel for a launch whose largest block
+// has M = max_m, from the measured table (the handles and the server use
+// it): 128 threads x 4 CTAs per SM for small blocks, 160 x 3, 256 x 2.
+inline int lean_table_threads(int max_m) { return max_m <= 170 ? 128 : (max_m <= 250 ? 160 : 256); }
+
 // The static shared scratch the streamed path needs (a subset of
 // BlockShared), for kernels that run only this path.
 struct alignas(16) LeanShared {

@@ -7,8 +7,9 @@
 //
 // Batches.  A scheduler thread takes every pending request of the admitted
 // jobs (up to max_batch) as soon as one of `max_inflight` batch slots is free
-// and launches ONE persistent kernel over the blocks of all of them, largest
-// blocks first.  Each slot has its own stream, so a batch launched while
+// and launches the multi-CTA streamed kernel over the blocks of all of them,
+// largest blocks first (blocks beyond its shared memory in a persistent
+// launch before it, as under the handles' default schedule).  Each slot has its own stream, so a batch launched while
 // another runs starts on the SMs that the running batch's CTAs give up at its
 // tail: requests that arrive during a batch overlap with it on the device.
 // The CTA that completes the last block of a request reduces that request's
@@ -16,9 +17,10 @@
 // the next batch's CTAs), and a completion thread per slot hands the results
 // back.
 //
-// Determinism.  Per-block work (process_block) and the per-request reduction
-// (reduce_blocks) are the code of the single-job path, so a result is
-// bit-identical to bv_llh_eval on the same layout, alone or in any mix.
+// Determinism.  Per-block work (process_block_big / run_block) and the
+// per-request reduction (reduce_blocks) are the code of the single-job path,
+// so a result is bit-identical to bv_llh_eval on the same layout under the
+// default schedule, alone or in any mix.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -86,6 +88,71 @@ __global__ void __launch_bounds__(kThreads, 1) llh_fp64_server_kernel(const JobD
         }
     }
 }
+
+// The multi-CTA streamed kernel's server form: the same task list protocol
+// over the blocks whose two panels fit in shared memory (the rest run the
+// kernel above), NT threads per CTA, MINB CTAs per SM, one global slab per
+// CTA.  Per block the code of the handles' default path (process_block_big,
+// panel-by-panel generation), so a request's blocks give the bits a handle
+// created with the default schedule gives.
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) llh_lean_server_kernel(const JobDesc *descs, const int2 *tasks,
+                                                                   int ntasks, unsigned *counter,
+                                                                   double *slab0, size_t slab_stride)
+{
+    // Only LeanShared as static shared memory, as the handles' kernel, so the
+    // two route a block by the same shared-memory limit.  The "last block of
+    // its request" flag travels in sh.red, unused between blocks.
+    extern __shared__ __align__(128) double smem[];
+    __shared__ LeanShared sh;
+    const int tid = threadIdx.x;
+    double *slab = slab0 + (size_t)blockIdx.x * slab_stride;
+    for (;;) {
+        if (tid == 0) {
+            sh.task = (int)atomicAdd(counter, 1u);
+            sh.status = 0u;
+        }
+        __syncthreads();
+        const int t = sh.task;
+        if (t >= ntasks) break;
+        const int2 tk = tasks[t];
+        const JobDesc &d = descs[tk.x];
+        const LlhArgs a = d.a;
+        const int b = tk.y;
+        if (a.acc[b + 1] == a.acc[b]) {  // empty block: contributes -(0 + 0 + 0) / 2
+            if (tid == 0) {
+                a.block_llk[b] = -0.0;
+                a.block_status[b] = a.status_or;
+            }
+        } else {
+            const MaternParams mp = d.mp;
+            process_block_big<NT, 64, LeanShared, 0, false, false>(a, mp, b,
+                                                                   reinterpret_cast<unsigned char *>(smem),
+                                                                   slab, sh);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            const unsigned prev = atomicAdd(d.done, 1u);
+            sh.red[0][0] = (prev + 1u == (unsigned)a.bc) ? 1.0 : 0.0;
+        }
+        __syncthreads();
+        if (sh.red[0][0] != 0.0) {
+            __threadfence();
+            reduce_blocks(a.block_llk, a.block_status, a.bc, d.out, smem);
+        }
+    }
+}
+
+struct LeanServerVariant {
+    void (*kernel)(const JobDesc *, const int2 *, int, unsigned *, double *, size_t);
+    int threads;
+};
+static const LeanServerVariant kLeanServer[] = {
+    {llh_lean_server_kernel<128, 4>, 128},
+    {llh_lean_server_kernel<160, 3>, 160},
+    {llh_lean_server_kernel<256, 2>, 256},
+};
 
 }  // namespace bv
 
@@ -174,6 +241,8 @@ struct bv_server {
         double *slab = nullptr;
         size_t slab_stride = 0;
         int slab_max_m = 0;
+        double *lean_slab = nullptr;  // the streamed kernel's per-CTA slabs
+        size_t lean_bytes = 0;
         // pinned host staging
         int2 *h_tasks = nullptr;
         size_t cap_h_tasks = 0;
@@ -207,6 +276,8 @@ struct bv_server {
     int big_max_m = 0;
     size_t smem_bytes = 0;
     int grid = 0;
+    int lean_limit = 0;  // blocks up to this M run the streamed kernel
+    int sms = 0;
     cudaStream_t upload = nullptr;
 };
 
@@ -309,6 +380,31 @@ bool can_release(bv_server *S)
     return false;
 }
 
+// The streamed server kernel's launch for blocks up to M = max_m: variant
+// from the handles' table, shared memory, the full grid (CTAs resident per
+// SM x SMs) and the per-CTA slab stride.
+struct LeanLaunch {
+    const LeanServerVariant *v = nullptr;
+    size_t smem = 0, stride = 0;
+    int grid = 0;
+};
+
+bool lean_launch_for(const bv_server *S, int max_m, LeanLaunch &ll)
+{
+    const int t = lean_table_threads(max_m);
+    ll.v = &kLeanServer[t == 128 ? 0 : (t == 160 ? 1 : 2)];
+    ll.smem = std::max<size_t>(big_layout(max_m, 64, 0, 0).total, kReduceScratchBytes);
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ll.v->kernel, ll.v->threads, ll.smem) != cudaSuccess ||
+        occ < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    ll.grid = S->sms * occ;
+    ll.stride = (big_slab_doubles(max_m) + 31) & ~(size_t)31;
+    return true;
+}
+
 // Build the batch's descriptors and tasks in the slot and launch it.
 // Called by the scheduler without the lock; `jobs[r]` stay alive and
 // unchanged while their requests are in flight.
@@ -317,28 +413,82 @@ bool launch_batch(bv_server *S, bv_server::Slot &sl, const std::vector<Job *> &j
 {
     const int R = (int)jobs.size();
     size_t total = 0;
-    int max_m = 1;
     bool any_big = false;
     for (const Job *j : jobs) {
         total += j->bc;
-        max_m = std::max(max_m, j->max_m);
         any_big = any_big || j->big;
     }
     cudaStream_t s = sl.s;
     bool ok = grow_async(sl.bllk, sl.cap_bllk, total, s) && grow_async(sl.bst, sl.cap_bst, total, s) &&
               grow_async(sl.tasks, sl.cap_tasks, total, s) && grow_pinned(sl.h_tasks, sl.cap_h_tasks, total);
-    if (ok && max_m > S->smem_cap_m && max_m > sl.slab_max_m) {
+    if (!ok) {
+        sl.err = "out of memory for the batch buffers";
+        return false;
+    }
+    // Tasks: merge the jobs' runs of equal M, largest M first.  Blocks above
+    // the streamed kernel's limit (the first n_pers tasks) run the persistent
+    // kernel, the others the streamed kernel, as under the handles' default
+    // schedule.
+    size_t n_pers = 0;
+    int pers_max_m = 0, lean_max_m = 0;
+    {
+        std::vector<size_t> run(R, 0);
+        size_t w = 0;
+        for (;;) {
+            int best = -1;
+            for (int r = 0; r < R; ++r)
+                if (run[r] < jobs[r]->m_value.size() &&
+                    (best < 0 || jobs[r]->m_value[run[r]] > jobs[best]->m_value[run[best]]))
+                    best = r;
+            if (best < 0) break;
+            const int m = jobs[best]->m_value[run[best]];
+            for (int r = best; r < R; ++r) {
+                const Job &j = *jobs[r];
+                if (run[r] < j.m_value.size() && j.m_value[run[r]] == m) {
+                    const int b0 = j.m_start[run[r]];
+                    const int b1 = (run[r] + 1 < j.m_start.size()) ? j.m_start[run[r] + 1] : j.bc;
+                    for (int p = b0; p < b1; ++p) sl.h_tasks[w++] = make_int2(r, j.sorted[p]);
+                    run[r]++;
+                }
+            }
+            if (m > S->lean_limit) {
+                n_pers = w;
+                pers_max_m = std::max(pers_max_m, m);
+            } else {
+                lean_max_m = std::max(lean_max_m, m);
+            }
+        }
+        total = w;
+    }
+    // Slabs: the persistent kernel's (blocks beyond shared memory) and the
+    // streamed kernel's per-CTA slabs.
+    if (n_pers > 0 && pers_max_m > S->smem_cap_m && pers_max_m > sl.slab_max_m) {
         if (sl.slab) cudaFreeAsync(sl.slab, s);
         // Covers both a streamed-path job and any job whose large blocks take
         // the slab path.
-        sl.slab_stride = std::max(big_slab_stride(max_m, S->smem_cap_m, S->big_max_m),
-                                  (block_doubles(max_m) + 31) & ~(size_t)31);
+        sl.slab_stride = std::max(big_slab_stride(pers_max_m, S->smem_cap_m, S->big_max_m),
+                                  (block_doubles(pers_max_m) + 31) & ~(size_t)31);
         ok = cudaMallocAsync(reinterpret_cast<void **>(&sl.slab), sl.slab_stride * 8 * S->grid, s) ==
              cudaSuccess;
-        sl.slab_max_m = ok ? max_m : 0;
+        sl.slab_max_m = ok ? pers_max_m : 0;
         if (!ok) {
             cudaGetLastError();
             sl.slab = nullptr;
+        }
+    }
+    LeanLaunch ll;
+    if (ok && total > n_pers) {
+        ok = lean_launch_for(S, lean_max_m, ll);
+        ll.grid = std::max(1, std::min<int>(ll.grid, (int)(total - n_pers)));
+        const size_t bytes = ll.stride * 8 * (size_t)ll.grid;
+        if (ok && bytes > sl.lean_bytes) {
+            if (sl.lean_slab) cudaFreeAsync(sl.lean_slab, s);
+            ok = cudaMallocAsync(reinterpret_cast<void **>(&sl.lean_slab), bytes, s) == cudaSuccess;
+            sl.lean_bytes = ok ? bytes : 0;
+            if (!ok) {
+                cudaGetLastError();
+                sl.lean_slab = nullptr;
+            }
         }
     }
     if (!ok) {
@@ -376,39 +526,19 @@ bool launch_batch(bv_server *S, bv_server::Slot &sl, const std::vector<Job *> &j
         d.out = sl.res + r;
         off += j.bc;
     }
-    // Tasks: merge the jobs' runs of equal M, largest M first.
-    {
-        std::vector<size_t> run(R, 0);
-        size_t w = 0;
-        for (;;) {
-            int best = -1;
-            for (int r = 0; r < R; ++r)
-                if (run[r] < jobs[r]->m_value.size() &&
-                    (best < 0 || jobs[r]->m_value[run[r]] > jobs[best]->m_value[run[best]]))
-                    best = r;
-            if (best < 0) break;
-            const int m = jobs[best]->m_value[run[best]];
-            for (int r = best; r < R; ++r) {
-                const Job &j = *jobs[r];
-                if (run[r] < j.m_value.size() && j.m_value[run[r]] == m) {
-                    const int b0 = j.m_start[run[r]];
-                    const int b1 = (run[r] + 1 < j.m_start.size()) ? j.m_start[run[r] + 1] : j.bc;
-                    for (int p = b0; p < b1; ++p) sl.h_tasks[w++] = make_int2(r, j.sorted[p]);
-                    run[r]++;
-                }
-            }
-        }
-        total = w;
-    }
-    ok = cudaMemsetAsync(sl.counters, 0, (1 + R) * sizeof(unsigned), s) == cudaSuccess &&
+    ok = cudaMemsetAsync(sl.counters, 0, (2 + R) * sizeof(unsigned), s) == cudaSuccess &&
          cudaMemcpyAsync(sl.desc, sl.h_desc, R * sizeof(JobDesc), cudaMemcpyHostToDevice, s) == cudaSuccess &&
          cudaMemcpyAsync(sl.tasks, sl.h_tasks, total * sizeof(int2), cudaMemcpyHostToDevice, s) == cudaSuccess;
-    if (ok) {
-        const int grid = std::max(1, std::min<int>(S->grid, (int)total));
+    if (ok && n_pers > 0) {
+        const int grid = std::max(1, std::min<int>(S->grid, (int)n_pers));
         // The streamed large-block path is compiled in only when a block needs it.
         auto kern = any_big ? llh_fp64_server_kernel<true> : llh_fp64_server_kernel<false>;
-        kern<<<grid, kThreads, S->smem_bytes, s>>>(sl.desc, sl.tasks, (int)total,
-                                                                     sl.counters);
+        kern<<<grid, kThreads, S->smem_bytes, s>>>(sl.desc, sl.tasks, (int)n_pers, sl.counters);
+        ok = cudaGetLastError() == cudaSuccess;
+    }
+    if (ok && ll.v) {
+        ll.v->kernel<<<ll.grid, ll.v->threads, ll.smem, s>>>(sl.desc, sl.tasks + n_pers, (int)(total - n_pers),
+                                                             sl.counters + 1 + R, sl.lean_slab, ll.stride);
         ok = cudaGetLastError() == cudaSuccess;
     }
     ok = ok && cudaMemcpyAsync(sl.h_res, sl.res, R * sizeof(EvalResult), cudaMemcpyDeviceToHost, s) ==
@@ -562,6 +692,7 @@ void destroy_slot(bv_server::Slot &sl)
     cudaFree(sl.res);
     cudaFree(sl.counters);
     cudaFree(sl.slab);
+    cudaFree(sl.lean_slab);
     cudaFreeHost(sl.h_tasks);
     cudaFreeHost(sl.h_desc);
     cudaFreeHost(sl.h_res);
@@ -634,6 +765,16 @@ extern "C" int bv_server_create(const bv_server_opts *opts, bv_server **out)
     BV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, llh_fp64_server_kernel<true>, kThreads,
                                                               S->smem_bytes));
     S->grid = prop.multiProcessorCount * std::max(1, occ);
+    S->sms = prop.multiProcessorCount;
+    // The streamed kernel: the handles' limit, and its shared memory allowed.
+    {
+        cudaFuncAttributes fl;
+        BV_CUDA_TRY(cudaFuncGetAttributes(&fl, kLeanServer[2].kernel));
+        const size_t avail = (size_t)optin - fl.sharedSizeBytes;
+        S->lean_limit = big_max_m_for_bytes(avail, 64, 0, 0);
+        for (const LeanServerVariant &v : kLeanServer)
+            BV_CUDA_TRY(cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)avail));
+    }
     BV_CUDA_TRY(cudaStreamCreateWithFlags(&S->upload, cudaStreamNonBlocking));
     for (int k = 0; k < S->opts.max_inflight; ++k) {
         std::unique_ptr<bv_server::Slot> sl(new bv_server::Slot());
@@ -642,9 +783,21 @@ extern "C" int bv_server_create(const bv_server_opts *opts, bv_server **out)
         BV_CUDA_TRY(cudaStreamCreateWithFlags(&sl->s, cudaStreamNonBlocking));
         BV_CUDA_TRY(cudaMalloc(&sl->desc, R * sizeof(JobDesc)));
         BV_CUDA_TRY(cudaMalloc(&sl->res, R * sizeof(EvalResult)));
-        BV_CUDA_TRY(cudaMalloc(&sl->counters, (1 + R) * sizeof(unsigned)));
+        BV_CUDA_TRY(cudaMalloc(&sl->counters, (2 + R) * sizeof(unsigned)));
         BV_CUDA_TRY(cudaHostAlloc(&sl->h_desc, R * sizeof(JobDesc), cudaHostAllocDefault));
         BV_CUDA_TRY(cudaHostAlloc(&sl->h_res, R * sizeof(EvalResult), cudaHostAllocDefault));
+        // Streamed-kernel slabs for blocks up to M = 350 (cs = 300 with
+        // blocks of 50) at every table point, so that batches of such jobs
+        // allocate nothing; larger batches grow them.
+        size_t pre = 0;
+        for (int m : {170, 250, std::min(350, S->lean_limit)}) {
+            LeanLaunch ll;
+            if (lean_launch_for(S.get(), m, ll)) pre = std::max(pre, ll.stride * 8 * (size_t)ll.grid);
+        }
+        if (pre > 0) {
+            BV_CUDA_TRY(cudaMalloc(&sl->lean_slab, pre));
+            sl->lean_bytes = pre;
+        }
         S->slots.push_back(std::move(sl));
     }
     bv_server *raw = S.release();

@@ -2,9 +2,10 @@
 
 Many fitting jobs share one device: each job's layout is copied to HBM when it
 fits the budget, and every evaluation request pending at a scheduler tick runs
-in one persistent launch over the blocks of all requests.  A result is
-bit-identical to `LlhData(layout)(theta)` for the same layout, whether its job
-runs alone or among others.
+in one batch over the blocks of all requests (the multi-CTA streamed kernel for
+blocks whose panels fit in shared memory, the persistent kernel beyond, as the
+default schedule).  A result is bit-identical to `LlhData(layout)(theta)` for
+the same layout, whether its job runs alone or among others.
 
     srv = Server(device=0)
     job = srv.open_job(layout)

@@ -163,10 +163,11 @@ typedef struct {
     int streamed_threads; /* threads per CTA of that kernel (0: none)       */
     int streamed_variant; /* its variant, an index into tune_ms             */
     double tune_ms[6];   /* with bv_opts.tune: the streamed kernel's time on
-                            the first evaluation per variant: 96, 160 and 256
-                            threads per CTA generating panel by panel, then
-                            the same sizes generating the whole matrix first
-                            (0 where not timed)                              */
+                            the first evaluation per variant: 96 x 5 CTAs per
+                            SM, 160 x 3, 256 x 2 and 128 x 4 threads per CTA
+                            generating panel by panel, then 160 x 3 and
+                            256 x 2 generating the whole matrix first (0
+                            where not timed)                                 */
 } bv_status;
 
 typedef struct bv_handle bv_handle;
@@ -260,11 +261,12 @@ int bv_llh_noalloc(const double *x, const double *y, const double *obs,
  * dataset per process).  Jobs are copied to HBM while their footprint
  * (locations, observations, offsets, conditioning indices) fits the budget;
  * the others wait in FIFO order and are admitted as jobs close.  A scheduler
- * thread batches every pending request of the admitted jobs into one
- * persistent launch over all their blocks; requests arriving meanwhile join
- * the next batch, which starts on the SMs the running batch releases.  Each
- * result is bit-identical to bv_llh_eval on the same layout, alone or in a
- * mix. */
+ * thread batches every pending request of the admitted jobs into one launch
+ * over all their blocks (the multi-CTA streamed kernel; blocks beyond its
+ * shared memory in a persistent launch before it); requests arriving
+ * meanwhile join the next batch, which starts on the SMs the running batch
+ * releases.  Each result is bit-identical to bv_llh_eval on the same layout
+ * under the default schedule, alone or in a mix. */
 typedef struct bv_server bv_server;
 typedef struct {
     int device;

@@ -232,14 +232,17 @@ def test_large_blocks(bvlib, oracle, n, bc, cs, theta, path):
 
 
 def test_large_blocks_deterministic_and_served(bvlib):
-    """The streamed path (chosen automatically: more than one wave of large
-    blocks) is deterministic and the server gives the same bits."""
+    """Large blocks (cs = 300): the persistent kernel's streamed path (chosen
+    automatically: more than one wave of large blocks) and the default
+    streamed kernel are each deterministic, graph or not, and the server
+    gives the default schedule's bits."""
     L = _gen(bvlib, 8000, 400, 300, seed=2)
     th = (1.0, 0.08, 1.5)
-    with bvlib.LlhData(L, on_failure="continue", schedule="persistent") as D, \
-            bvlib.LlhData(L, on_failure="continue", use_graph=False, schedule="persistent") as E:
-        v = [D(th) for _ in range(2)] + [E(th)]
-    assert v[0] == v[1] == v[2]
+    for sched in ("persistent", "auto"):
+        with bvlib.LlhData(L, on_failure="continue", schedule=sched) as D, \
+                bvlib.LlhData(L, on_failure="continue", use_graph=False, schedule=sched) as E:
+            v = [D(th) for _ in range(2)] + [E(th)]
+        assert v[0] == v[1] == v[2], sched
     with bvlib.Server(on_failure="continue") as srv:
         j = srv.open_job(L)
         assert srv.evaluate(j, th) == v[0]
@@ -320,7 +323,7 @@ def test_nugget_served_and_mixed(bvlib):
     path with a nugget stays within its 1e-8 accuracy bound."""
     L = _gen(bvlib, 3000, 200, 100)
     th = (1.0, 0.1, 0.5, 0.05)
-    with bvlib.LlhData(L, nugget=True, schedule="persistent") as D:
+    with bvlib.LlhData(L, nugget=True) as D:
         v = D(th)
     with bvlib.Server() as srv:
         j = srv.open_job(L, nugget=True)
@@ -332,8 +335,8 @@ def test_nugget_served_and_mixed(bvlib):
 
 def test_tuner_picks_fastest_and_keeps_bits(bvlib, oracle):
     """bv_opts.tune: the first evaluation times the streamed kernel's
-    variants (96, 160 and 256 threads per CTA; panel-by-panel or whole-matrix
-    generation) and keeps the fastest; every variant gives the same bits, so
+    variants (96, 128, 160 and 256 threads per CTA; panel-by-panel or
+    whole-matrix generation) and keeps the fastest; every variant gives the same bits, so
     tuned and untuned handles agree exactly."""
     L = _gen(bvlib, 8000, 500, 100)
     th = (1.0, 0.1, 1.5)
@@ -345,8 +348,8 @@ def test_tuner_picks_fastest_and_keeps_bits(bvlib, oracle):
         st = D.status()
         v2 = D(th)
     assert v0 == v1 == v2
-    assert t0 in (96, 160, 256)
+    assert t0 in (128, 160, 256)
     ms = st["tune_ms"]
     assert all(m > 0 for m in ms), ms
     assert st["streamed_variant"] == int(np.argmin(ms))
-    assert st["streamed_threads"] == (96, 160, 256, 96, 160, 256)[int(np.argmin(ms))]
+    assert st["streamed_threads"] == (96, 160, 256, 128, 160, 256)[int(np.argmin(ms))]

@@ -1,8 +1,10 @@
 """Continuous-batching server (bv_server_*): each request's result equals the
-single-job evaluation of the same layout on the persistent kernel (the
-server's per-block algorithm) bit for bit, whether the job runs alone or
-mixed with other jobs; HBM admission holds jobs back until they fit; and the
-oracle agrees with the served results to the FP64 parity bound."""
+single-job evaluation of the same layout under the default schedule bit for
+bit (the server runs the same per-block code: the streamed kernel for
+blocks whose panels fit in shared memory, the persistent kernel beyond),
+whether the job runs alone or mixed with other jobs; HBM admission holds
+jobs back until they fit; and the oracle agrees with the served results to
+the FP64 parity bound."""
 import threading
 
 import numpy as np
@@ -21,15 +23,30 @@ def _gen(bv, n, bc, cs, seed):
     return L
 
 
+def _big_block_layout(bv, seed):
+    """cs = 300 with one block of 550 points (M = 850, beyond the streamed
+    kernel's shared memory: the persistent kernel's global-slab path)."""
+    rng = np.random.default_rng(seed)
+    cs = 300
+    bn = np.array([320, 40, 550, 25, 60, 1, 90], dtype=np.int32)
+    acc = np.concatenate([[0], np.cumsum(bn)]).astype(np.int32)
+    n = int(acc[-1])
+    knn = np.zeros(len(bn) * cs, dtype=np.int32)
+    knn[:cs] = np.arange(cs)
+    for b in range(1, len(bn)):
+        knn[b * cs:(b + 1) * cs] = rng.choice(acc[b], cs, replace=False)
+    return bv.Layout(bn, acc, rng.random(n), rng.random(n), rng.standard_normal(n), cs, knn_idx=knn)
+
+
 @pytest.fixture(scope="module")
 def jobs(bvlib):
-    # Shared-memory blocks, a cs=250 job whose blocks take the global slab,
-    # and a classic-Vecchia job of many small blocks.
+    # Streamed-kernel blocks at three sizes, a classic-Vecchia job of many
+    # small blocks, and a job with a block beyond the streamed kernel.
     specs = [(4000, 300, 80, 1), (2500, 150, 250, 2), (3000, 1500, 40, 3)]
-    Ls = [_gen(bvlib, *s) for s in specs]
+    Ls = [_gen(bvlib, *s) for s in specs] + [_big_block_layout(bvlib, 4)]
     alone = []
     for L in Ls:
-        with bvlib.LlhData(L, schedule="persistent") as D:
+        with bvlib.LlhData(L) as D:  # the server's default failure policy too
             alone.append([D(th) for th in THETAS])
     return Ls, alone
 
