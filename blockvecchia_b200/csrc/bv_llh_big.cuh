@@ -28,6 +28,14 @@
 // stays on the diagonal, its column is zeroed below, the block is flagged).
 // Every wait on an mbarrier is bounded; a wait that gives up flags the block
 // BV_ST_DEVICE_TIMEOUT and the remaining waits are skipped.
+//
+// The same function with NS = 0 is the default path for every block whose
+// two panels fit (the multi-CTA streamed kernels llh_lean_kernel_t and
+// llh_lean_server_kernel, 96-256 threads, several CTAs per SM): no staging;
+// the update warps read the earlier panels' fragments straight from the slab
+// into registers and accumulate panel p+1's tiles in place on the DMMA
+// accumulators (panel_update_direct); optionally the whole matrix is
+// generated into the slab first (kBulk).
 #pragma once
 
 #include <stdint.h>
