@@ -40,6 +40,7 @@ _I = C.POINTER(C.c_int)
 # Every function include/bv.h declares, with its ctypes signature.
 EXPORTS = {
     "bv_default_opts": (None, [C.c_void_p]),
+    "bv_abi_sizes": (C.c_int, [C.POINTER(C.c_size_t), C.c_int]),
     "bv_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     "bv_destroy": (None, [C.c_void_p]),
     "bv_llh": (C.c_double, [C.c_uint, _D, _D, C.c_void_p]),

@@ -257,6 +257,15 @@ static void handle_free(bv_handle *h)
     delete h;
 }
 
+extern "C" int bv_abi_sizes(size_t *out, int n)
+{
+    const size_t v[] = {sizeof(bv_layout), sizeof(bv_opts), sizeof(bv_status), sizeof(bv_server_opts),
+                        sizeof(bv_server_stats), sizeof(bv_job_opts)};
+    int k = 0;
+    for (; out && k < n && k < (int)(sizeof(v) / sizeof(v[0])); ++k) out[k] = v[k];
+    return k;
+}
+
 extern "C" void bv_default_opts(bv_opts *o)
 {
     if (!o) return;

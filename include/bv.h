@@ -172,6 +172,11 @@ typedef struct {
 
 typedef struct bv_handle bv_handle;
 
+/* sizeof of the ABI structs in this build, for bindings that restate them
+ * (ctypes, cgo): out[0..5] = bv_layout, bv_opts, bv_status, bv_server_opts,
+ * bv_server_stats, bv_job_opts; returns the number written (<= n). */
+int bv_abi_sizes(size_t *out, int n);
+
 /* Fill *o with the defaults (FP64, Matern, dist_scale 1, device 0,
  * BV_FAIL_NEGINF, no printing, graphs on, BV_SCHED_AUTO, Euclidean). */
 void bv_default_opts(bv_opts *o);

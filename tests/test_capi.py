@@ -57,3 +57,14 @@ def test_server_without_device(bvlib):
         pytest.skip("a CUDA device is present")
     with pytest.raises(bvlib.BvError):
         bvlib.Server()
+
+
+def test_ctypes_structs_match_the_header(bvlib):
+    """The Python binding's restated structs have the C ABI's sizes."""
+    import ctypes as C
+    from blockvecchia_b200 import _lib
+    out = (C.c_size_t * 6)()
+    assert _lib.lib().bv_abi_sizes(out, 6) == 6
+    mine = [C.sizeof(t) for t in (_lib.BvLayout, _lib.BvOpts, _lib.BvStatus, _lib.BvServerOpts,
+                                  _lib.BvServerStats, _lib.BvJobOpts)]
+    assert list(out) == mine
