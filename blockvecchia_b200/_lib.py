@@ -104,7 +104,8 @@ class BvOpts(C.Structure):
                 ("device", C.c_int), ("on_failure", C.c_int), ("print_iter", C.c_int),
                 ("use_graph", C.c_int), ("schedule", C.c_int), ("mixed_tol", C.c_double),
                 ("shard_count", C.c_int), ("shard_index", C.c_int), ("large_blocks", C.c_int),
-                ("nugget", C.c_int), ("earth", C.c_int), ("tune", C.c_int)]
+                ("nugget", C.c_int), ("earth", C.c_int), ("tune", C.c_int),
+                ("mixed_fp32", C.c_int)]
 
 
 class BvStatus(C.Structure):

@@ -52,7 +52,7 @@ struct Opts {
     int time_flag = 0, t_slots = 0, use_nugget = 0, earth = 0;
     int knn = 1, seed = 0, perf = 0, vecchia_cs = 100, vecchia_bc = 200, maxiter = 1000;
     double tol = 1e-5, lower_bound = 0.01, upper_bound = 3.0;
-    int omp_threads = 40, device = 0, precision = BV_PREC_FP64, print_opts = 0;
+    int omp_threads = 40, device = 0, precision = BV_PREC_FP64, mixed_fp32 = 0, print_opts = 0;
     std::string xy_path, obs_path, permutation = "random";
     int ordering = BV_ORDER_RANDOM;
 };
@@ -109,7 +109,7 @@ Opts parse(int argc, char **argv)
                    "  [--xy_path F] [--obs_path F] [--tol k (1e-k)] [--maxiter N] [--omp_threads N]\n"
                    "  [--permutation random|morton|kdtree|hilbert|mmd] [--dist_scale d] [--lower_bound b] [--upper_bound b]\n"
                    "  [--t_slots N] [--3D x] [--use_nugget 0|1]\n"
-                   "  [--precision fp64|mixed] [--device N] [--print-opts]\n"
+                   "  [--precision fp64|mixed|mixed_fp32] [--device N] [--print-opts]\n"
                    "  space-time: --kernel univariate_matern_spacetime_stationary\n"
                    "              --ikernel s2:range:nu:range_t:nu_t:sep\n");
             exit(0);
@@ -186,7 +186,10 @@ Opts parse(int argc, char **argv)
                                     o.permutation.c_str());
         } else if (a == "--precision" && has) {
             const std::string p = next();
-            o.precision = (p == "mixed") ? BV_PREC_MIXED : BV_PREC_FP64;
+            // mixed: FP64 throughout unless forced (bv_opts.mixed_fp32);
+            // mixed_fp32: the FP32 pass wherever its probe accepts blocks.
+            o.precision = (p == "mixed" || p == "mixed_fp32") ? BV_PREC_MIXED : BV_PREC_FP64;
+            o.mixed_fp32 = (p == "mixed_fp32") ? 1 : 0;
         } else if (a == "--device" && has) {
             o.device = atoi(next());
         } else if (a == "--print-opts") {
@@ -227,12 +230,12 @@ void print_opts(const Opts &o)
            "\"dist_scale\": %.17g, \"omp_threads\": %d, \"precision\": %d, \"xy_path\": \"%s\", "
            "\"obs_path\": \"%s\", \"time_flag\": %d, \"t_slots\": %d, \"beta_time\": %.17g, "
            "\"nu_time\": %.17g, \"sep\": %.17g, \"nugget\": %.17g, \"use_nugget\": %d, "
-           "\"permutation\": \"%s\", \"ordering\": %d, \"earth\": %d}\n",
+           "\"permutation\": \"%s\", \"ordering\": %d, \"earth\": %d, \"mixed_fp32\": %d}\n",
            o.kernel, o.num_params, o.num_loc, o.sigma, o.beta, o.nu, o.sigma_init, o.beta_init,
            o.nu_init, o.vecchia_cs, o.vecchia_bc, o.knn, o.perf, o.seed, o.tol, o.maxiter,
            o.lower_bound, o.upper_bound, o.dist_scale, o.omp_threads, o.precision,
            o.xy_path.c_str(), o.obs_path.c_str(), o.time_flag, o.t_slots, o.beta_time, o.nu_time, o.sep,
-           o.nugget, o.use_nugget, o.permutation.c_str(), o.ordering, o.earth);
+           o.nugget, o.use_nugget, o.permutation.c_str(), o.ordering, o.earth, o.mixed_fp32);
 }
 
 // include/utils.h:27-87: "x,y" per line ("x,y,z" with time_flag); one
@@ -484,6 +487,7 @@ int main(int argc, char **argv)
     bo.dist_scale = o.dist_scale;
     bo.device = o.device;
     bo.precision = o.precision;
+    bo.mixed_fp32 = o.mixed_fp32;
     bo.print_iter = o.perf ? 0 : 1;
     bv_handle *h = nullptr;
     if (bv_create(&L, &bo, &h)) die(bv_last_error());

@@ -285,6 +285,7 @@ extern "C" void bv_default_opts(bv_opts *o)
     o->nugget = 0;
     o->earth = 0;
     o->tune = 0;
+    o->mixed_fp32 = 0;
 }
 
 // Cost rank (largest first, ties by index) shared by the schedule and the
@@ -837,7 +838,8 @@ extern "C" int bv_create(const bv_layout *L, const bv_opts *opts, bv_handle **ou
     if (h->opts.precision == BV_PREC_MIXED) {
         int max_bs = 0;
         for (int t = 0; t < h->owned; ++t) max_bs = std::max(max_bs, h->batchNum[h->order[t]]);
-        BV_TRY_H(mixed_create(h->mixed, h->device, h->bc, h->cs, max_bs, h->order.data(), h->owned));
+        BV_TRY_H(mixed_create(h->mixed, h->device, h->bc, h->cs, max_bs, h->order.data(), h->owned,
+                              h->opts.mixed_fp32 != 0));
     }
     if (h->opts.use_graph) BV_TRY_H(capture_graph(h));
 #undef BV_TRY_H
@@ -993,10 +995,19 @@ static int eval_locked(bv_handle *h, const double *theta, double *llk)
     s.nonfinite = r.nonfinite;
     s.flags_or = r.flags_or;
     s.failed = r.failed;
-    // FP64: the fused launches and the reduction; mixed: probe, decision,
-    // mixed pass, FP64 fallback pass and the reduction.
-    s.launches = h->opts.precision == BV_PREC_MIXED ? 5 : (int)h->launches.size() + 1;
-    s.streamed_blocks = h->opts.precision == BV_PREC_MIXED ? 0 : h->streamed_blocks;
+    // FP64: the fused launches and the reduction; mixed: the probe (FP32
+    // pass enabled and something to probe), the decision, the mixed pass
+    // (FP32 pass enabled), the FP64 pass and the reduction.
+    const bool mixed = h->opts.precision == BV_PREC_MIXED;
+    if (!mixed)
+        s.launches = (int)h->launches.size() + 1;
+    else if (h->owned <= 0)
+        s.launches = 1;
+    else
+        s.launches = 3 + (h->mixed.fp32 ? 1 + (h->mixed.nprobe > 0 ? 1 : 0) : 0);
+    // Without the FP32 pass every block takes the FP64 pass, on the streamed
+    // kernel when it covers the layout.
+    s.streamed_blocks = !mixed ? h->streamed_blocks : (!h->mixed.fp32 && h->mixed_lean ? h->owned : 0);
     s.streamed_threads = s.streamed_blocks > 0 ? h->lean_threads : 0;
     s.streamed_variant = s.streamed_blocks > 0 ? h->lean_vi : -1;
     for (int i = 0; i < kNumLean; ++i) s.tune_ms[i] = h->tune_ms[i];

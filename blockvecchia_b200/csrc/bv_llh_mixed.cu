@@ -521,9 +521,11 @@ __global__ void mixed_decide_kernel(const int *order, int owned, int nprobe, con
 
 }  // namespace
 
-int mixed_create(MixedWork &w, int device, int bc, int cs, int max_bs, const int *h_order, int owned)
+int mixed_create(MixedWork &w, int device, int bc, int cs, int max_bs, const int *h_order, int owned,
+                 bool fp32)
 {
     mixed_free(w);
+    w.fp32 = fp32;
     int optin = 0;
     BV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     cudaFuncAttributes fa;
@@ -554,7 +556,9 @@ int mixed_create(MixedWork &w, int device, int bc, int cs, int max_bs, const int
     w.owned = owned;
     std::vector<int> probe;
     // Block 0 (unconditioned) never takes the mixed path: probe its neighbour.
-    for (int t = 0; t < owned; t += kMxProbeStride) {
+    // Without the FP32 pass nothing is probed and the decision sends every
+    // block to the FP64 pass.
+    for (int t = 0; fp32 && t < owned; t += kMxProbeStride) {
         const int u = (h_order[t] == 0 && t + 1 < owned) ? t + 1 : t;
         if (h_order[u] != 0) probe.push_back(h_order[u]);
     }
@@ -600,6 +604,7 @@ int mixed_enqueue(MixedWork &w, const MixedArgs &a0, cudaStream_t st)
     mixed_decide_kernel<<<(w.owned + 255) / 256, 256, 0, st>>>(a.order, w.owned, w.nprobe, w.probe_fail,
                                                                w.skip, w.fallback_list, w.fallback_count);
     BV_CUDA_TRY(cudaGetLastError());
+    if (!w.fp32) return BV_OK;
     // Full pass (returns at once when skipped).
     a.task_end = w.owned;
     a.work_counter = w.counter + 1;

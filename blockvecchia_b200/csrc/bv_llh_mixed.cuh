@@ -107,6 +107,7 @@ constexpr int kMxProbeStride = 64;
 
 struct MixedWork {
     bool active = false;
+    bool fp32 = false;             // run the probe and the FP32 pass (else FP64 throughout)
     int grid = 0;
     size_t smem_bytes = 0;
     int owned = 0, nprobe = 0;
@@ -121,10 +122,13 @@ struct MixedWork {
 
 // Host: plan the launch (shared-memory size for the largest block that fits,
 // grid) and allocate the fallback list.  Blocks larger than what fits are
-// routed to the fallback by the kernel itself.
-int mixed_create(MixedWork &w, int device, int bc, int cs, int max_bs, const int *h_order, int owned);
-// Enqueue the probe, the decision and the mixed pass (the FP64 fallback pass
-// is enqueued by the caller, over w.fallback_list[0 .. *w.fallback_count)).
+// routed to the fallback by the kernel itself.  fp32 = false: no probe and no
+// FP32 pass; every block goes to the FP64 pass.
+int mixed_create(MixedWork &w, int device, int bc, int cs, int max_bs, const int *h_order, int owned,
+                 bool fp32);
+// Enqueue the probe, the decision and the mixed pass, or without the FP32 pass
+// the decision alone (the FP64 fallback pass is enqueued by the caller, over
+// w.fallback_list[0 .. *w.fallback_count)).
 int mixed_enqueue(MixedWork &w, const MixedArgs &a, cudaStream_t st);
 void mixed_free(MixedWork &w);
 

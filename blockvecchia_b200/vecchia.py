@@ -212,7 +212,7 @@ class LlhData:
                  print_iter: bool = False, use_graph: bool = True, schedule: str = "auto",
                  mixed_tol: float = 1e-8, shard_count: int = 1, shard_index: int = 0,
                  large_blocks: str = "auto", nugget: bool = False, earth: bool = False,
-                 tune: bool = False):
+                 tune: bool = False, mixed_fp32: bool = False):
         L = layout.normalized()
         self.layout = L
         o = _lib.BvOpts()
@@ -232,6 +232,7 @@ class LlhData:
         o.nugget = int(bool(nugget))
         o.earth = int(bool(earth))
         o.tune = int(bool(tune))
+        o.mixed_fp32 = int(bool(mixed_fp32))
         null_i = C.POINTER(C.c_int)()
         null_d = C.POINTER(C.c_double)()
         self._l = _lib.BvLayout(L.n, L.bc, L.cs, ip(L.batchNum), ip(L.batchNumAccum), dp(L.x),

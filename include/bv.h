@@ -137,6 +137,14 @@ typedef struct {
                           layout and the handle keeps the fastest (all give
                           the same bits, so results do not depend on the
                           choice); bv_get_status reports the times.        */
+    int mixed_fp32;    /* BV_PREC_MIXED only.  0 (default): every block on the
+                          FP64 path (its values exactly): on B200 the FP32
+                          factor + FP64 refinement kernel took 4.8-6.3x the
+                          FP64 path's time on every layout where FP32 could
+                          factor the blocks (nu = 0.5), and smoother kernels
+                          fail in FP32.  1: the FP32 pass runs whenever a
+                          probe of every 64th block accepts at least half of
+                          them; blocks it rejects go to the FP64 path.       */
 } bv_opts;
 
 /* Distance metrics of bv_knn_ex (the reference's distance_metric). */

@@ -86,3 +86,13 @@ def test_earth_flag(exe):
     an unrecognised option, as in the reference)."""
     o = _opts(exe, "--earth", "--num_loc", "5000")
     assert o["earth"] == 1 and o["num_loc"] == 5000
+
+
+def test_precision_flag(exe):
+    """--precision mixed keeps FP64 throughout (bv_opts.mixed_fp32 = 0);
+    mixed_fp32 forces the FP32 pass."""
+    assert (_opts(exe)["precision"], _opts(exe)["mixed_fp32"]) == (0, 0)
+    o = _opts(exe, "--precision", "mixed")
+    assert (o["precision"], o["mixed_fp32"]) == (1, 0)
+    o = _opts(exe, "--precision", "mixed_fp32")
+    assert (o["precision"], o["mixed_fp32"]) == (1, 1)

@@ -328,7 +328,7 @@ def test_nugget_served_and_mixed(bvlib):
     with bvlib.Server() as srv:
         j = srv.open_job(L, nugget=True)
         assert srv.evaluate(j, th) == v
-    with bvlib.LlhData(L, nugget=True, precision="mixed") as M:
+    with bvlib.LlhData(L, nugget=True, precision="mixed", mixed_fp32=True) as M:
         vm = M(th)
     assert abs(vm - v) <= 1e-8 * abs(v)
 
