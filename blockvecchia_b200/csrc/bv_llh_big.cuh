@@ -263,8 +263,13 @@ __device__ __forceinline__ void panel_update_tiles(double *dst, int dst_r0, cons
 // registers).
 constexpr int kDT = 2;
 
-// Substitution rows of the factor warp per panel (process_block_big).
-constexpr int kSubstRows0 = 64;
+// Substitution rows of the factor warp per panel (process_block_big): with
+// up to 256 rows below the diagonal block (every panel of M <= ~290) warp 0
+// solves them all while the other warps generate and update the next panel.
+// Kernel ms at the C3 / C2 / C1 shapes: 32 rows 51.0 / 3.89 / 1.91, 64 rows
+// 50.4 / 3.87 / 1.89, 128 rows 49.7 / 3.78 / 1.86, 256 rows 49.2 / 3.77 /
+// 1.84 (rows dealt over the whole CTA after a barrier: 51.2 / 3.84 / 1.92).
+constexpr int kSubstRows0 = 256;
 
 __device__ __forceinline__ double2 ldcg2(const double *p)
 {
@@ -551,8 +556,7 @@ static __device__ __noinline__ void process_block_big(const LlhArgs &a, const Ma
         // operands on step q+1's dependent chain (1 / L_{q+1,q+1} and
         // L_{q+2,q+1}) read one step ahead.  Warp 0, idle for most of the
         // phase before, takes the first kSubstRows0 rows, the other warps the
-        // rest (C3 shape: 50.4 ms against 51.2 with a barrier before the
-        // substitution and its rows dealt over the whole CTA).
+        // rest.
         const int rs0 = k0 + (kb == kNB ? 2 * kNB : kb);
         const int rw0 = min(Mp, rs0 + kSubstRows0);
         const int rbeg = (warp == 0) ? rs0 + lane : rw0 + tid - 32;
