@@ -258,17 +258,18 @@ __device__ __forceinline__ void panel_update_tiles(double *dst, int dst_r0, cons
 // their order do not depend on the CTA size or the tile count.  A lane's
 // DMMA steps 2h and 2h+1 use the adjacent columns k = 8h + 2 c4 + {0, 1},
 // one 16-byte load for both (the same columns in A and B, so each step
-// still sums four k-products).  kDT = 2 measured fastest (C3 shape: 59.1 ms
-// at 2, 63.4 at 3, 69.9 at 4; with 3 or more the live fragments crowd the
-// registers).
+// still sums four k-products).  kDT = 2 measured fastest (n = 1M, cs = 200:
+// 59.1 ms at 2, 63.4 at 3, 69.9 at 4; with 3 or more the live fragments
+// crowd the registers).
 constexpr int kDT = 2;
 
 // Substitution rows of the factor warp per panel (process_block_big): with
 // up to 256 rows below the diagonal block (every panel of M <= ~290) warp 0
 // solves them all while the other warps generate and update the next panel.
-// Kernel ms at the C3 / C2 / C1 shapes: 32 rows 51.0 / 3.89 / 1.91, 64 rows
-// 50.4 / 3.87 / 1.89, 128 rows 49.7 / 3.78 / 1.86, 256 rows 49.2 / 3.77 /
-// 1.84 (rows dealt over the whole CTA after a barrier: 51.2 / 3.84 / 1.92).
+// Kernel ms for n = 1M, cs = 200 / n = 200k, cs = 120 / n = 20k, cs = 300:
+// 32 rows 51.0 / 3.89 / 1.91, 64 rows 50.4 / 3.87 / 1.89, 128 rows 49.7 /
+// 3.78 / 1.86, 256 rows 49.2 / 3.77 / 1.84 (rows dealt over the whole CTA
+// after a barrier: 51.2 / 3.84 / 1.92).
 constexpr int kSubstRows0 = 256;
 
 __device__ __forceinline__ double2 ldcg2(const double *p)
@@ -280,10 +281,10 @@ template <int NTILE>
 __device__ __forceinline__ void load_frags(const double *pq, int q0, int Mp, int n0, int i0, int nw,
                                            int r8, int c4, double2 (&bf)[2][2], double2 (&af)[NTILE][2])
 {
-    // B: the 16 rows n0.. of panel q, read by every tile of the panel, through
-    // L1 (C3 shape: 51.2 against 51.8 ms through L2 only); A: each tile's
-    // own rows, read once per panel, L2 only.  This CTA wrote both before
-    // the last barrier, from this SM.
+    // B: the 16 rows n0.. of panel q, read by every tile of the panel,
+    // through L1 (n = 1M, cs = 200: 51.2 against 51.8 ms through L2 only);
+    // A: each tile's own rows, read once per panel, L2 only.  This CTA wrote
+    // both before the last barrier, from this SM.
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
 #pragma unroll
